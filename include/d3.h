@@ -1,0 +1,142 @@
+/*
+ * d3.h -- C ABI of the B200-native DFT-D3 dispersion engine (libd3.so).
+ *
+ * Drop-in for the C API of LASP-D3 (src/d3.h of that project): the nine entry points
+ * below keep the reference's names, argument types (float I/O, uint16_t elements,
+ * enums passed as int), units and ownership rules, so its Python cffi binding
+ * (src/d3_cffi.py), Fortran iso_c_binding interfaces (src/fortran_d3.f90) and C/C++
+ * callers link against this library unchanged.
+ *
+ * Units and conventions (as the reference):
+ *   coordinates and cell in Angstrom, cell rows are lattice vectors;
+ *   cutoffs in bohr (not converted);
+ *   energy in eV (negative = binding), forces in eV/Angstrom in the caller's atom
+ *   order, stress in eV/Angstrom^3 (already divided by the signed cell volume),
+ *   row-major 3x3.
+ * Threading: a handle must be used from one thread at a time. Work runs on the
+ * current CUDA device.
+ *
+ * Deliberate deviations from the reference, all on error paths:
+ *   - set_atoms with more atoms than the handle capacity prints an error and returns
+ *     (the reference calls exit(), src/d3_buffer.cu:380-383);
+ *   - an element that was not given at init is rejected (the reference silently maps
+ *     it through a re-built element list, src/d3_buffer.cu:389-422);
+ *   - atomic numbers outside the parameter table are rejected at init.
+ */
+#ifndef D3_B200_H
+#define D3_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef float real_t; /* src/d3_types.h:7 */
+
+typedef enum { ZERO_DAMPING = 0, BJ_DAMPING = 1 } damping_type_t; /* src/d3_types.h:16-19 */
+
+typedef enum {
+    PBE = 0,
+    PBE0 = 1,
+    B3LYP = 2,
+    BLYP = 3,
+    BP86 = 4,
+    REVPBE = 5,
+    CUSTOM = 99
+} functional_t; /* src/d3_types.h:21-29 */
+
+typedef void d3_handle_t; /* src/d3.h:9 */
+
+/* ---------------- reference ABI (src/d3.h:36-128) ---------------- */
+
+/* One-shot evaluation without ATM (replaces src/d3.h:36-38, src/d3.cu:236-251). */
+void compute_dispersion_energy(real_t atoms[][3], uint16_t *elements, uint64_t num_atoms, real_t cell[3][3],
+                               real_t cutoff_radius, real_t CN_cutoff_radius, damping_type_t damping_type,
+                               functional_t functional_type, real_t *energy, real_t *force, real_t *stress);
+
+/* Handle for repeated evaluations, two-body + CN only (replaces src/d3.h:60-62). */
+d3_handle_t *init_d3_handle(uint16_t *elements, uint64_t num_elements, uint64_t max_length, real_t cutoff_radius,
+                            real_t coordination_number_cutoff, damping_type_t damping_type,
+                            functional_t functional_type);
+
+/* Handle with the ATM three-body term within atm_cutoff (bohr) (replaces src/d3.h:64-66). */
+d3_handle_t *init_d3_handle_with_atm(uint16_t *elements, uint64_t length_elements, uint64_t max_length,
+                                     real_t cutoff_radius, real_t coordination_number_cutoff, real_t atm_cutoff,
+                                     damping_type_t damping_type, functional_t functional_type);
+
+/* Coordinates [length][3] in Angstrom and atomic numbers (replaces src/d3.h:82). */
+void set_atoms(d3_handle_t *handle, real_t *coords, uint16_t *elements, uint64_t length);
+
+/* Cell, rows = lattice vectors, Angstrom (replaces src/d3.h:90). */
+void set_cell(d3_handle_t *handle, real_t cell[3][3]);
+
+/* Release the handle after synchronising its work (replaces src/d3.h:97). */
+void free_d3_handle(d3_handle_t *handle);
+
+/* Kept for ABI compatibility: every evaluation starts from cleared intermediates
+   (replaces src/d3.h:106). */
+void clear_d3_handle(d3_handle_t *handle);
+
+/* Energy (eV), forces [n][3] (eV/A), stress [9] (eV/A^3) (replaces src/d3.h:115). */
+void compute_dispersion_energy_from_handle(d3_handle_t *handle, real_t *energy, real_t *force, real_t *stress);
+
+/* Same, returning the status word: 0 success; bit 0 neighbour-list overflow (as the
+   reference's COMPUTE_NEIGHBOR_LIST_OVERFLOW); 1 for a NULL handle or an internal error
+   (replaces src/d3.h:127-128, src/d3.cu:130-226). Additional bits of this engine:
+   0x02 non-finite input, 0x04 degenerate cell, 0x08 lattice shift out of range,
+   0x10 CUDA error, 0x20 atoms or cell not set. */
+uint16_t compute_dispersion_energy_from_handle_status(d3_handle_t *handle, real_t *energy, real_t *force,
+                                                      real_t *stress);
+
+/* ---------------- additive extensions (no reference counterpart) ---------------- */
+
+/* Parameter table layout: 5 references / 95 elements (reference default) or the
+   7-reference / 103-element layout of USE_EXTENDED_PARAMETERS. */
+enum { D3_TABLE_5REF = 0, D3_TABLE_7REF = 1 };
+
+/* Handle with double-precision cutoffs and the table layout chosen at run time;
+   rc_atm <= 0 disables ATM. */
+d3_handle_t *d3_init_handle_ex(const uint16_t *elements, uint64_t n_elements, uint64_t max_length, double rc,
+                               double rc_cn, double rc_atm, int damping_type, int functional_type, int table);
+
+/* FP64 input/output path: Angstrom in, eV / eV/A / eV/A^3 out, same conventions. */
+int d3_set_atoms_f64(d3_handle_t *handle, const double *coords, const uint16_t *elements, uint64_t length);
+int d3_set_cell_f64(d3_handle_t *handle, const double cell[9]);
+uint16_t d3_compute_f64(d3_handle_t *handle, double *energy, double *force, double *stress);
+
+/* Options (value 0/1): */
+enum {
+    D3_OPT_ATM_FORCE_SCALED = 1, /* 1: apply the 1/2, 1/6 repeated-index ATM factors to forces too
+                                    (forces = -dE/dx); 0 (default): reference convention */
+    D3_OPT_SMOOTH_CN = 2         /* tanh^3 CN cutoff (reference compile-time SMOOTH_CUTOFF_CN) */
+};
+int d3_set_option(d3_handle_t *handle, int option, int value);
+
+/* Damping parameters for CUSTOM (or to override a functional): s6, s8 and
+   (sr6, sr8) for zero damping or (a1, a2) for BJ damping. */
+int d3_set_functional_params(d3_handle_t *handle, double s6, double s8, double p1, double p2);
+
+/* Enqueue one evaluation on a CUDA stream (cudaStream_t passed as void*, NULL = the
+   handle's stream) with no host synchronisation; results stay on the device at
+   d3_device_results(): [0] energy, [1..3n] forces, [3n+1..3n+9] stress (double, eV
+   units). The neighbour-list capacity must already be sufficient (run one
+   d3_compute_f64 or compute_dispersion_energy_from_handle_status first). */
+uint16_t d3_compute_async(d3_handle_t *handle, void *cuda_stream);
+const double *d3_device_results(d3_handle_t *handle);
+
+/* Last error message of this thread ("" if none). */
+const char *d3_last_error(void);
+
+/* Diagnostics (caller atom order): coordination numbers, dE/dCN (hartree), per-atom
+   energies (hartree, reference sign); ATM half list as rows (apex, j, Tx, Ty, Tz) with
+   the reference's lattice shifts; wrap shifts and bin index of each atom. */
+int d3_debug_atom_arrays(d3_handle_t *handle, double *cn, double *dedcn, double *energy_atoms);
+int64_t d3_debug_atm_pairs(d3_handle_t *handle, int64_t *rows, int64_t cap);
+int d3_debug_bins(d3_handle_t *handle, int64_t *wrap_shift, int64_t *bin_index, int *num_bins);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* D3_B200_H */

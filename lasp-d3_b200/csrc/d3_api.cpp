@@ -1,0 +1,278 @@
+// C ABI of libd3.so: the reference's nine entry points (LASP-D3 src/d3.h:36-128,
+// implemented there in src/d3.cu:14-251) plus additive d3_* extensions, on top of the
+// engine in d3_engine.cu. No exception crosses this boundary.
+#include "../../include/d3.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "d3_engine.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) {
+    g_last_error = msg;
+    fprintf(stderr, "Error: %s\n", msg.c_str());
+}
+
+struct Handle {
+    d3::Engine *engine = nullptr;
+    uint64_t n = 0;
+    std::vector<double> f64_forces;
+};
+
+Handle *H(d3_handle_t *h) { return reinterpret_cast<Handle *>(h); }
+
+// Angstrom -> bohr, float input widened to double (the reference converts in float,
+// src/d3.cu:50-60; the FP64 engine keeps the conversion in double)
+void to_bohr(const float *in, size_t m, std::vector<double> &out) {
+    out.resize(m);
+    for (size_t i = 0; i < m; ++i) out[i] = (double)in[i] * d3::ANG2BOHR;
+}
+
+d3_handle_t *make_handle(const uint16_t *elements, uint64_t n_el, uint64_t max_len, double rc, double rc_cn,
+                         double rc_atm, bool use_atm, int damping, int functional, bool extended) {
+    std::string err;
+    d3::Engine *e = d3::engine_create(elements, n_el, max_len, rc, rc_cn, rc_atm, use_atm, damping, functional,
+                                      extended, err);
+    if (!e) {
+        set_error(err);
+        return nullptr;
+    }
+    Handle *h = new Handle();
+    h->engine = e;
+    return reinterpret_cast<d3_handle_t *>(h);
+}
+
+uint16_t compute_float(Handle *h, real_t *energy, real_t *force, real_t *stress) {
+    const uint64_t n = d3::engine_num_atoms(h->engine);
+    h->f64_forces.resize(3 * n);
+    double e = 0, s[9] = {0};
+    uint16_t st = d3::engine_compute(h->engine, &e, h->f64_forces.data(), s, nullptr, true);
+    if (st & (d3::ST_CUDA_ERROR | d3::ST_NOT_READY)) {
+        set_error(st & d3::ST_NOT_READY ? "atoms or cell not set" : "CUDA error during compute");
+        return st;
+    }
+    if (energy) *energy = (real_t)e;
+    if (force)
+        for (uint64_t i = 0; i < 3 * n; ++i) force[i] = (real_t)h->f64_forces[i];
+    if (stress)
+        for (int i = 0; i < 9; ++i) stress[i] = (real_t)s[i];
+    return st;
+}
+
+} // namespace
+
+extern "C" {
+
+d3_handle_t *init_d3_handle(uint16_t *elements, uint64_t num_elements, uint64_t max_length, real_t cutoff_radius,
+                            real_t coordination_number_cutoff, damping_type_t damping_type,
+                            functional_t functional_type) {
+    return make_handle(elements, num_elements, max_length, cutoff_radius, coordination_number_cutoff, 0.0, false,
+                       (int)damping_type, (int)functional_type, false);
+}
+
+d3_handle_t *init_d3_handle_with_atm(uint16_t *elements, uint64_t length_elements, uint64_t max_length,
+                                     real_t cutoff_radius, real_t coordination_number_cutoff, real_t atm_cutoff,
+                                     damping_type_t damping_type, functional_t functional_type) {
+    return make_handle(elements, length_elements, max_length, cutoff_radius, coordination_number_cutoff, atm_cutoff,
+                       true, (int)damping_type, (int)functional_type, false);
+}
+
+void set_atoms(d3_handle_t *handle, real_t *coords, uint16_t *elements, uint64_t length) {
+    if (!handle) {
+        set_error("handle is NULL in set_atoms");
+        return;
+    }
+    std::vector<double> b;
+    to_bohr(coords, 3 * length, b);
+    std::string err;
+    if (d3::engine_set_atoms(H(handle)->engine, b.data(), elements, length, err)) set_error(err);
+}
+
+void set_cell(d3_handle_t *handle, real_t cell[3][3]) {
+    if (!handle) {
+        set_error("handle is NULL in set_cell");
+        return;
+    }
+    double c[9];
+    float cf[9];
+    const float a2b = 1.0f / 0.52917726f; // the reference's float conversion (src/d3.cu:79-85)
+    for (int i = 0; i < 9; ++i) {
+        c[i] = (double)cell[i / 3][i % 3] * d3::ANG2BOHR;
+        cf[i] = cell[i / 3][i % 3] * a2b;
+    }
+    std::string err;
+    if (d3::engine_set_cell(H(handle)->engine, c, cf, err)) set_error(err);
+}
+
+void free_d3_handle(d3_handle_t *handle) {
+    if (!handle) {
+        set_error("handle is NULL in free_d3_handle");
+        return;
+    }
+    Handle *h = H(handle);
+    d3::engine_destroy(h->engine);
+    delete h;
+}
+
+void clear_d3_handle(d3_handle_t *handle) {
+    if (!handle) set_error("handle is NULL in clear_d3_handle");
+}
+
+uint16_t compute_dispersion_energy_from_handle_status(d3_handle_t *handle, real_t *energy, real_t *force,
+                                                      real_t *stress) {
+    if (!handle) {
+        set_error("handle is NULL in compute_dispersion_energy_from_handle");
+        return 1;
+    }
+    return compute_float(H(handle), energy, force, stress);
+}
+
+void compute_dispersion_energy_from_handle(d3_handle_t *handle, real_t *energy, real_t *force, real_t *stress) {
+    uint16_t st = compute_dispersion_energy_from_handle_status(handle, energy, force, stress);
+    if (st != 0) fprintf(stderr, "Error: compute_dispersion_energy_from_handle failed with status %d\n", st);
+}
+
+void compute_dispersion_energy(real_t atoms[][3], uint16_t *elements, uint64_t num_atoms, real_t cell[3][3],
+                               real_t cutoff_radius, real_t CN_cutoff_radius, damping_type_t damping_type,
+                               functional_t functional_type, real_t *energy, real_t *force, real_t *stress) {
+    // as the reference: a temporary handle without ATM (src/d3.cu:236-251)
+    d3_handle_t *h = init_d3_handle(elements, num_atoms, num_atoms, cutoff_radius, CN_cutoff_radius, damping_type,
+                                    functional_type);
+    if (!h) return;
+    set_atoms(h, (real_t *)atoms, elements, num_atoms);
+    set_cell(h, cell);
+    clear_d3_handle(h);
+    compute_dispersion_energy_from_handle(h, energy, force, stress);
+    free_d3_handle(h);
+}
+
+// ---------------- extensions ----------------
+
+d3_handle_t *d3_init_handle_ex(const uint16_t *elements, uint64_t n_elements, uint64_t max_length, double rc,
+                               double rc_cn, double rc_atm, int damping_type, int functional_type, int table) {
+    return make_handle(elements, n_elements, max_length, rc, rc_cn, rc_atm, rc_atm > 0.0, damping_type,
+                       functional_type, table == D3_TABLE_7REF);
+}
+
+int d3_set_atoms_f64(d3_handle_t *handle, const double *coords, const uint16_t *elements, uint64_t length) {
+    if (!handle) {
+        set_error("handle is NULL in d3_set_atoms_f64");
+        return 1;
+    }
+    std::vector<double> b(3 * length);
+    for (uint64_t i = 0; i < 3 * length; ++i) b[i] = coords[i] * d3::ANG2BOHR;
+    std::string err;
+    if (d3::engine_set_atoms(H(handle)->engine, b.data(), elements, length, err)) {
+        set_error(err);
+        return 1;
+    }
+    return 0;
+}
+
+int d3_set_cell_f64(d3_handle_t *handle, const double cell[9]) {
+    if (!handle) {
+        set_error("handle is NULL in d3_set_cell_f64");
+        return 1;
+    }
+    double c[9];
+    float cf[9];
+    const float a2b = 1.0f / 0.52917726f;
+    for (int i = 0; i < 9; ++i) {
+        c[i] = cell[i] * d3::ANG2BOHR;
+        cf[i] = (float)cell[i] * a2b;
+    }
+    std::string err;
+    if (d3::engine_set_cell(H(handle)->engine, c, cf, err)) {
+        set_error(err);
+        return 1;
+    }
+    return 0;
+}
+
+uint16_t d3_compute_f64(d3_handle_t *handle, double *energy, double *force, double *stress) {
+    if (!handle) {
+        set_error("handle is NULL in d3_compute_f64");
+        return 1;
+    }
+    uint16_t st = d3::engine_compute(H(handle)->engine, energy, force, stress, nullptr, true);
+    if (st & (d3::ST_CUDA_ERROR | d3::ST_NOT_READY))
+        set_error(st & d3::ST_NOT_READY ? "atoms or cell not set" : "CUDA error during compute");
+    return st;
+}
+
+int d3_set_option(d3_handle_t *handle, int option, int value) {
+    if (!handle) {
+        set_error("handle is NULL in d3_set_option");
+        return 1;
+    }
+    d3::Options o = d3::engine_get_options(H(handle)->engine);
+    switch (option) {
+    case D3_OPT_ATM_FORCE_SCALED: o.atm_force_scaled = value != 0; break;
+    case D3_OPT_SMOOTH_CN: o.smooth_cn = value != 0; break;
+    default: set_error("unknown option " + std::to_string(option)); return 1;
+    }
+    d3::engine_set_options(H(handle)->engine, o);
+    return 0;
+}
+
+int d3_set_functional_params(d3_handle_t *handle, double s6, double s8, double p1, double p2) {
+    if (!handle) {
+        set_error("handle is NULL in d3_set_functional_params");
+        return 1;
+    }
+    d3::engine_set_functional_params(H(handle)->engine, d3::FuncParams{s6, s8, p1, p2});
+    return 0;
+}
+
+uint16_t d3_compute_async(d3_handle_t *handle, void *cuda_stream) {
+    if (!handle) {
+        set_error("handle is NULL in d3_compute_async");
+        return 1;
+    }
+    return d3::engine_compute(H(handle)->engine, nullptr, nullptr, nullptr, (cudaStream_t)cuda_stream, false);
+}
+
+const double *d3_device_results(d3_handle_t *handle) {
+    return handle ? d3::engine_device_results(H(handle)->engine) : nullptr;
+}
+
+const char *d3_last_error(void) { return g_last_error.c_str(); }
+
+int d3_debug_atom_arrays(d3_handle_t *handle, double *cn, double *dedcn, double *energy_atoms) {
+    if (!handle) return 1;
+    try {
+        return d3::engine_debug_atom_arrays(H(handle)->engine, cn, dedcn, energy_atoms);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+int64_t d3_debug_atm_pairs(d3_handle_t *handle, int64_t *rows, int64_t cap) {
+    if (!handle) return -1;
+    try {
+        return d3::engine_debug_atm_pairs(H(handle)->engine, rows, cap);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int d3_debug_bins(d3_handle_t *handle, int64_t *wrap_shift, int64_t *bin_index, int *num_bins) {
+    if (!handle) return 1;
+    try {
+        return d3::engine_debug_bins(H(handle)->engine, wrap_shift, bin_index, num_bins);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+} // extern "C"

@@ -1,0 +1,1434 @@
+// B200 D3 dispersion engine: device kernels and host orchestration (FP64 plain path).
+//
+// Replaces the reference's pipeline (LASP-D3 src/d3.cu:130-226):
+//   coordination_number_kernel (src/d3_kernel.cu:582-683)
+//   atm_kernel                 (src/d3_kernel.cu:1199-1509)
+//   two_body_kernel            (src/d3_kernel.cu:997-1197)
+//   three_body_kernel          (src/d3_kernel.cu:1571-1698, the dE/dCN chain rule)
+// with a GPU cell list instead of per-image all-pairs loops, per-atom factorised C6
+// weights instead of per-pair 25-exponential C6, an explicit rc_ATM half neighbour
+// list with triplets enumerated from it, and deterministic per-atom accumulation
+// except for the ATM scatter to neighbour atoms (FP64 atomics).
+//
+// Device layout (HBM):
+//   xs[n]      double4  wrapped position (bohr) + type in .w, binned order
+//   shift[n]   int4     lattice shift removed by wrapping (S, unwrapped = xs + S*h)
+//   orig[n] / sorted_of[n]  binned <-> caller order
+//   bin_start[nbins+1]      CSR of the bin grid (x fastest)
+//   w, dw[n][NR]            normalised Gaussian weights of the C6 reference grid and
+//                           their CN derivative
+//   Y[n][ne][NR]            y_{i,t}[b] = sum_a w_i[a] C6ref[t_i][t][a][b]
+//   per-atom energy / dE/dCN / force / virial partials of each pass
+//   atm_off[n+1], atm_ent[] rc_ATM half list (j <= a in caller order), CSR
+#include "d3_engine.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+
+#include "d3_synth_params.h"
+
+namespace d3 {
+
+#define D3_CUDA(call)                                                                                     \
+    do {                                                                                                  \
+        cudaError_t err__ = (call);                                                                       \
+        if (err__ != cudaSuccess) throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(err__) + \
+                                                           " at " + __FILE__ + ":" + std::to_string(__LINE__)); \
+    } while (0)
+
+constexpr double K1 = 16.0;
+constexpr double K3 = 4.0;
+
+// ------------------------------------------------------------------------------------
+// kernel parameter block (passed by value)
+// ------------------------------------------------------------------------------------
+struct KP {
+    int n;
+    int ne, nref;
+    double h[9], inv[9], vol;
+    int nb[3];
+    int nbins;
+    int box_mode;
+    int half[3];
+    double rc2, rcn2, ratm2, rc_cn;
+    // tables
+    const double *cnref; // [ne][MAX_NREF]
+    const double *c6;    // [ne][ne][nref][nref]
+    const double *r0ab;  // [ne][ne]
+    const double *rcov;  // [ne]
+    const double *r2r4;  // [ne]
+    const double *pairA; // [ne][ne][4]: BJ: A^6, A^8 ; zero: R0
+    double s6, s8, p1, p2;
+    int damping, smooth_cn, atm_force_scaled;
+    // atoms, caller order
+    const double *pos_in;
+    const int *type_in;
+    int *bin_in;
+    int4 *shift_in;
+    double4 *xw_in;
+    // binning
+    int *bin_cnt, *bin_start, *bin_fill, *order;
+    // atoms, binned order
+    double4 *xs;
+    int4 *shift;
+    int *bin_s, *orig, *sorted_of;
+    double *cn, *w, *dw, *Y;
+    double *e2, *g2, *f2, *v2; // two-body: energy, dE/dCN, force[3], virial[6]
+    double *ea, *ga, *fa, *va; // ATM apex share (direct writes)
+    double *eb, *gb, *fb;      // ATM entry share (atomics)
+    double *fc, *vc;           // chain rule: force[3], virial[6]
+    // ATM list
+    int *atm_cnt;
+    long long *atm_off;
+    int2 *atm_ent;
+    long long atm_cap;
+    int *work;
+    // stencils (x = dy, y = dz, z = dxlo, w = dxhi)
+    const int4 *st2;
+    int nst2;
+    const int4 *stc;
+    int nstc;
+    const int4 *sta;
+    int nsta;
+    // outputs
+    double *out; // [0]=E(eV), [1..3n]=F(eV/A), [3n+1..3n+9]=stress(eV/A^3)
+    unsigned int *status;
+};
+
+__device__ __forceinline__ int floordiv(int a, int b) {
+    int q = a / b;
+    if ((a % b != 0) && ((a < 0) != (b < 0))) --q;
+    return q;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Traverse every candidate (j, T) of binned atom i through a row-compressed stencil.
+// All 32 lanes call f(j, T, active) together (converged), so f may use warp votes.
+template <class F>
+__device__ __forceinline__ void traverse(const KP &p, int bin, const int4 *rows, int nrows, F &&f) {
+    const int lane = threadIdx.x & 31;
+    const int nb0 = p.nb[0], nb1 = p.nb[1], nb2 = p.nb[2];
+    const int bx = bin % nb0, by = (bin / nb0) % nb1, bz = bin / (nb0 * nb1);
+    for (int r = 0; r < nrows; ++r) {
+        const int4 row = rows[r];
+        const int yy = by + row.x, zz = bz + row.y;
+        const int Ty = floordiv(yy, nb1), Tz = floordiv(zz, nb2);
+        const int byy = yy - Ty * nb1, bzz = zz - Tz * nb2;
+        const int xlo = bx + row.z, xhi = bx + row.w;
+        const int plo = floordiv(xlo, nb0), phi = floordiv(xhi, nb0);
+        const int rowbase = nb0 * (byy + nb1 * bzz);
+        for (int px = plo; px <= phi; ++px) {
+            const int a = max(xlo, px * nb0) - px * nb0;
+            const int b = min(xhi, px * nb0 + nb0 - 1) - px * nb0;
+            const int jlo = p.bin_start[rowbase + a], jhi = p.bin_start[rowbase + b + 1];
+            for (int base = jlo; base < jhi; base += 32) {
+                const int j = base + lane;
+                f(j, px, Ty, Tz, j < jhi);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ bool in_box(const KP &p, int4 si, int4 sj, int Tx, int Ty, int Tz) {
+    if (!p.box_mode) return true;
+    // reference lattice shift of this image in unwrapped coordinates
+    const int rx = Tx + si.x - sj.x, ry = Ty + si.y - sj.y, rz = Tz + si.z - sj.z;
+    return abs(rx) <= p.half[0] && abs(ry) <= p.half[1] && abs(rz) <= p.half[2];
+}
+
+__device__ __forceinline__ void image_vec(const KP &p, int Tx, int Ty, int Tz, double &sx, double &sy, double &sz) {
+    sx = Tx * p.h[0] + Ty * p.h[3] + Tz * p.h[6];
+    sy = Tx * p.h[1] + Ty * p.h[4] + Tz * p.h[7];
+    sz = Tx * p.h[2] + Ty * p.h[5] + Tz * p.h[8];
+}
+
+// ------------------------------------------------------------------------------------
+// binning: wrap into the cell, bin, GPU counting sort (stable in caller order)
+// ------------------------------------------------------------------------------------
+__global__ void k_bin(KP p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const double x = p.pos_in[3 * i], y = p.pos_in[3 * i + 1], z = p.pos_in[3 * i + 2];
+    int s[3], b[3];
+    bool bad = !(isfinite(x) && isfinite(y) && isfinite(z));
+    for (int k = 0; k < 3; ++k) {
+        double f = x * p.inv[0 * 3 + k] + y * p.inv[1 * 3 + k] + z * p.inv[2 * 3 + k];
+        if (bad || fabs(f) > 1.0e6) {
+            bad = true;
+            f = 0.0;
+        }
+        double fl = floor(f);
+        s[k] = (int)fl;
+        int bk = (int)((f - fl) * p.nb[k]);
+        b[k] = min(max(bk, 0), p.nb[k] - 1);
+    }
+    if (bad) atomicOr(p.status, ST_BAD_INPUT);
+    const int bin = b[0] + p.nb[0] * (b[1] + p.nb[1] * b[2]);
+    double xw = x - (s[0] * p.h[0] + s[1] * p.h[3] + s[2] * p.h[6]);
+    double yw = y - (s[0] * p.h[1] + s[1] * p.h[4] + s[2] * p.h[7]);
+    double zw = z - (s[0] * p.h[2] + s[1] * p.h[5] + s[2] * p.h[8]);
+    if (bad) xw = yw = zw = 0.0;
+    p.bin_in[i] = bin;
+    p.shift_in[i] = make_int4(s[0], s[1], s[2], 0);
+    p.xw_in[i] = make_double4(xw, yw, zw, (double)p.type_in[i]);
+    atomicAdd(&p.bin_cnt[bin], 1);
+}
+
+// exclusive scan of cnt[0..m) into out[0..m] (out[m] = total); one block
+template <typename T, typename S>
+__global__ void k_scan(const S *cnt, T *out, int m) {
+    __shared__ T warp_tot[32];
+    __shared__ T carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int base = 0; base < m; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        T v = (i < m) ? (T)cnt[i] : (T)0;
+        T x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            T t = (lane < nw) ? warp_tot[lane] : (T)0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                T y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            if (lane < nw) warp_tot[lane] = t;
+        }
+        __syncthreads();
+        const T before = carry + (wid > 0 ? warp_tot[wid - 1] : (T)0) + x - v;
+        if (i < m) out[i] = before;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = before + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[m] = carry;
+}
+
+__global__ void k_scatter(KP p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int b = p.bin_in[i];
+    const int slot = p.bin_start[b] + atomicAdd(&p.bin_fill[b], 1);
+    p.order[slot] = i;
+}
+
+// make the in-bin order deterministic: ascending caller index (bins hold few atoms)
+__global__ void k_binsort(KP p) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= p.nbins) return;
+    const int lo = p.bin_start[b], hi = p.bin_start[b + 1];
+    for (int i = lo + 1; i < hi; ++i) {
+        int v = p.order[i], k = i - 1;
+        while (k >= lo && p.order[k] > v) {
+            p.order[k + 1] = p.order[k];
+            --k;
+        }
+        p.order[k + 1] = v;
+    }
+}
+
+__global__ void k_gather(KP p) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= p.n) return;
+    const int i = p.order[s];
+    p.xs[s] = p.xw_in[i];
+    p.shift[s] = p.shift_in[i];
+    p.bin_s[s] = p.bin_in[i];
+    p.orig[s] = i;
+    p.sorted_of[i] = s;
+}
+
+// ------------------------------------------------------------------------------------
+// coordination numbers (src/d3_kernel.cu:544-683): warp per atom
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double cn_term(const KP &p, double r, double rsum, double *dcn_over_r) {
+    const double e = exp(-K1 * (rsum / r - 1.0));
+    const double ope = 1.0 + e;
+    if (p.smooth_cn) {
+        const double t = tanh(p.rc_cn - r);
+        const double sc = t * t * t;
+        const double dsc = -3.0 * t * t * (1.0 - t * t);
+        *dcn_over_r = (-K1) * e * rsum / (r * r * r * ope * ope) * sc + dsc / (ope * r);
+        return sc / ope;
+    }
+    *dcn_over_r = (-K1) * e * rsum / (r * r * r * ope * ope);
+    return 1.0 / ope;
+}
+
+__global__ void k_cn(KP p) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= p.n) return;
+    const double4 xi = p.xs[i];
+    const int4 si = p.shift[i];
+    const double ri = p.rcov[(int)xi.w];
+    double acc = 0.0;
+    traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, bool act) {
+        if (!act) return;
+        if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+        const double4 xj = p.xs[j];
+        double sx, sy, sz;
+        image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+        const double dx = xi.x - (xj.x + sx), dy = xi.y - (xj.y + sy), dz = xi.z - (xj.z + sz);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 <= p.rcn2 && d2 > 0.0) {
+            double dd;
+            acc += cn_term(p, sqrt(d2), ri + p.rcov[(int)xj.w], &dd);
+        }
+    });
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) p.cn[i] = acc;
+}
+
+// ------------------------------------------------------------------------------------
+// per-atom normalised Gaussian weights (src/d3_kernel.cu:709-881, factorised)
+//   L_ab = w_i[a] w_j[b] with the max-shift split per atom, so
+//   C6_ij = w_i^T C w_j / (sum w_i sum w_j) and dC6/dCN_i = dw_i^T C w_j (normalised)
+// ------------------------------------------------------------------------------------
+template <int NR>
+__global__ void k_weights(KP p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    const int t = (int)p.xs[i].w;
+    const double cn = p.cn[i];
+    double w[NR], dw[NR];
+    double mx = -INFINITY;
+#pragma unroll
+    for (int a = 0; a < NR; ++a) {
+        const double cr = p.cnref[t * MAX_NREF + a];
+        if (cr > -1.0) {
+            const double d = cn - cr;
+            mx = fmax(mx, -K3 * d * d);
+        }
+    }
+    double sw = 0.0, sdw = 0.0;
+#pragma unroll
+    for (int a = 0; a < NR; ++a) {
+        const double cr = p.cnref[t * MAX_NREF + a];
+        if (cr > -1.0) {
+            const double d = cn - cr;
+            w[a] = exp(-K3 * d * d - mx);
+            dw[a] = -2.0 * K3 * d * w[a];
+        } else {
+            w[a] = 0.0;
+            dw[a] = 0.0;
+        }
+        sw += w[a];
+        sdw += dw[a];
+    }
+    const double isw = sw > 0.0 ? 1.0 / sw : 0.0;
+    const double ratio = sdw * isw;
+#pragma unroll
+    for (int a = 0; a < NR; ++a) {
+        const double wn = w[a] * isw;
+        p.w[(size_t)i * NR + a] = wn;
+        p.dw[(size_t)i * NR + a] = dw[a] * isw - wn * ratio;
+        w[a] = wn;
+    }
+    for (int tt = 0; tt < p.ne; ++tt) {
+        const double *C = p.c6 + ((size_t)t * p.ne + tt) * NR * NR;
+        double *Yo = p.Y + ((size_t)i * p.ne + tt) * NR;
+#pragma unroll
+        for (int b = 0; b < NR; ++b) {
+            double acc = 0.0;
+#pragma unroll
+            for (int a = 0; a < NR; ++a) acc += w[a] * C[a * NR + b];
+            Yo[b] = acc;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// two-body (src/d3_kernel.cu:902-1197): warp per central atom, every ordered pair
+// ------------------------------------------------------------------------------------
+template <int NR>
+__global__ void k_twobody(KP p) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= p.n) return;
+    const double4 xi = p.xs[i];
+    const int4 si = p.shift[i];
+    const int ti = (int)xi.w;
+    double wi[NR], dwi[NR];
+#pragma unroll
+    for (int a = 0; a < NR; ++a) {
+        wi[a] = p.w[(size_t)i * NR + a];
+        dwi[a] = p.dw[(size_t)i * NR + a];
+    }
+    const double rri = p.r2r4[ti];
+    double e = 0, g = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+    traverse(p, p.bin_s[i], p.st2, p.nst2, [&](int j, int Tx, int Ty, int Tz, bool act) {
+        if (!act) return;
+        if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+        const double4 xj = p.xs[j];
+        double sx, sy, sz;
+        image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+        const double dx = xi.x - (xj.x + sx), dy = xi.y - (xj.y + sy), dz = xi.z - (xj.z + sz);
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 < p.rc2 && r2 > 0.0)) return;
+        const int tj = (int)xj.w;
+        const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
+        double c6 = 0.0, dc6 = 0.0;
+#pragma unroll
+        for (int b = 0; b < NR; ++b) {
+            const double y = yj[b];
+            c6 += y * wi[b];
+            dc6 += y * dwi[b];
+        }
+        const double rr = 3.0 * rri * p.r2r4[tj];
+        const double c8 = c6 * rr, dc8 = dc6 * rr;
+        const double *pa = p.pairA + ((size_t)ti * p.ne + tj) * 4;
+        double E6, E8, G, fs;
+        if (p.damping == 1) {
+            const double r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
+            const double i6 = 1.0 / (r6 + pa[0]), i8 = 1.0 / (r8 + pa[1]);
+            E6 = p.s6 * c6 * i6;
+            E8 = p.s8 * c8 * i8;
+            G = p.s6 * dc6 * i6 + p.s8 * dc8 * i8;
+            fs = -6.0 * p.s6 * c6 * r4 * i6 * i6 - 8.0 * p.s8 * c8 * r6 * i8 * i8;
+        } else {
+            const double r = sqrt(r2), ir = 1.0 / r, ir2 = ir * ir;
+            const double ir6 = ir2 * ir2 * ir2, ir8 = ir6 * ir2;
+            const double R0 = pa[0];
+            const double x6 = p.p1 * R0 * ir, x8 = p.p2 * R0 * ir;
+            const double x6_2 = x6 * x6, x6_4 = x6_2 * x6_2, x6_8 = x6_4 * x6_4, x6_14 = x6_8 * x6_4 * x6_2;
+            const double x8_2 = x8 * x8, x8_4 = x8_2 * x8_2, x8_8 = x8_4 * x8_4, x8_16 = x8_8 * x8_8;
+            const double f6 = 1.0 / (1.0 + 6.0 * x6_14), f8 = 1.0 / (1.0 + 6.0 * x8_16);
+            const double df6 = 84.0 * f6 * f6 * x6_14 * ir, df8 = 96.0 * f8 * f8 * x8_16 * ir;
+            E6 = p.s6 * c6 * f6 * ir6;
+            E8 = p.s8 * c8 * f8 * ir8;
+            G = p.s6 * f6 * dc6 * ir6 + p.s8 * f8 * dc8 * ir8;
+            fs = p.s6 * c6 * (-6.0 * f6 * ir8 + df6 * ir6 * ir) + p.s8 * c8 * (-8.0 * f8 * ir8 * ir2 + df8 * ir8 * ir);
+        }
+        e += 0.5 * (E6 + E8);
+        g += G;
+        fx += fs * dx;
+        fy += fs * dy;
+        fz += fs * dz;
+        vxx += fs * dx * dx;
+        vyy += fs * dy * dy;
+        vzz += fs * dz * dz;
+        vxy += fs * dx * dy;
+        vxz += fs * dx * dz;
+        vyz += fs * dy * dz;
+    });
+    e = warp_sum(e);
+    g = warp_sum(g);
+    fx = warp_sum(fx);
+    fy = warp_sum(fy);
+    fz = warp_sum(fz);
+    vxx = warp_sum(vxx);
+    vyy = warp_sum(vyy);
+    vzz = warp_sum(vzz);
+    vxy = warp_sum(vxy);
+    vxz = warp_sum(vxz);
+    vyz = warp_sum(vyz);
+    if ((threadIdx.x & 31) == 0) {
+        p.e2[i] = e;
+        p.g2[i] = g;
+        p.f2[3 * i] = fx;
+        p.f2[3 * i + 1] = fy;
+        p.f2[3 * i + 2] = fz;
+        const double sc = -1.0 / (2.0 * p.vol);
+        double *v = p.v2 + 6 * (size_t)i;
+        v[0] = vxx * sc;
+        v[1] = vyy * sc;
+        v[2] = vzz * sc;
+        v[3] = vxy * sc;
+        v[4] = vxz * sc;
+        v[5] = vyz * sc;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// ATM half list: for apex a, entries (j, T) with caller index j <= a, every side in
+// [1e-12, rc_ATM^2] (src/d3_kernel.cu:1235-1269). Count pass then fill pass.
+// ------------------------------------------------------------------------------------
+template <bool FILL>
+__global__ void k_atm_list(KP p) {
+    const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (a >= p.n) return;
+    const int lane = threadIdx.x & 31;
+    const double4 xa = p.xs[a];
+    const int4 sa = p.shift[a];
+    const int oa = p.orig[a];
+    long long pos = 0;
+    if (FILL) pos = p.atm_off[a];
+    int count = 0;
+    bool range_err = false;
+    traverse(p, p.bin_s[a], p.sta, p.nsta, [&](int j, int Tx, int Ty, int Tz, bool act) {
+        bool keep = false;
+        if (act && p.orig[j] <= oa && in_box(p, sa, p.shift[j], Tx, Ty, Tz)) {
+            const double4 xj = p.xs[j];
+            double sx, sy, sz;
+            image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+            const double dx = xa.x - (xj.x + sx), dy = xa.y - (xj.y + sy), dz = xa.z - (xj.z + sz);
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            keep = !(d2 > p.ratm2 || d2 < 1e-12);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (FILL) {
+            if (keep) {
+                const long long slot = pos + __popc(m & ((1u << lane) - 1u));
+                if (abs(Tx) > 127 || abs(Ty) > 127 || abs(Tz) > 127) range_err = true;
+                if (slot < p.atm_cap) {
+                    const int packed = (Tx & 0xff) | ((Ty & 0xff) << 8) | ((Tz & 0xff) << 16);
+                    p.atm_ent[slot] = make_int2(j, packed);
+                }
+            }
+            pos += __popc(m);
+        } else {
+            count += __popc(m);
+        }
+    });
+    if (!FILL && lane == 0) p.atm_cnt[a] = count;
+    if (FILL) {
+        if (range_err) atomicOr(p.status, ST_SHIFT_RANGE);
+        if (lane == 0 && pos > p.atm_cap) atomicOr(p.status, ST_LIST_OVERFLOW);
+    }
+}
+
+__device__ __forceinline__ int sext8(int v) { return (v << 24) >> 24; }
+
+// ------------------------------------------------------------------------------------
+// ATM triplets (src/d3_kernel.cu:1199-1509) over the half list of each apex.
+// Persistent CTAs take apexes from a work counter (largest lists first). A thread owns
+// one list entry x and visits every other entry y of the same apex (both orders of
+// each unordered pair), so every accumulation into x is thread-private; the apex's
+// share is halved per visit. Partner entries are staged through shared memory.
+// ------------------------------------------------------------------------------------
+struct Partner {
+    double vx, vy, vz, d2, r, s, lam, g;
+    int j, t, pad0, pad1;
+};
+
+constexpr int ATM_THREADS = 128;
+
+template <int NR>
+__global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
+    extern __shared__ double smem[];
+    const int ne = p.ne;
+    Partner *ptile = reinterpret_cast<Partner *>(smem);
+    double *ytile = reinterpret_cast<double *>(ptile + tile); // [tile][ne][NR]
+    double *yapex = ytile + (size_t)tile * ne * NR;           // [ne][NR] apex Y
+    double *r0s = yapex + ne * NR;                            // [ne][ne]
+    __shared__ int s_item;
+    __shared__ double red[ATM_THREADS / 32][12];
+    const int tid = threadIdx.x;
+    if (p.atm_off[p.n] > p.atm_cap) return; // list overflowed: the host grows it and re-runs
+    for (int k = tid; k < ne * ne; k += blockDim.x) r0s[k] = p.r0ab[k];
+    const double x16c = 4294967296.0 / 43046721.0; // (4/3)^16 = 4^16 / 3^16
+    const double third = 1.0 / 3.0;
+    while (true) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(p.work, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= p.n) break;
+        const int a = p.sorted_of[p.n - 1 - item];
+        const long long e0 = p.atm_off[a];
+        const int m = (int)(p.atm_off[a + 1] - e0);
+        const double4 xa = p.xs[a];
+        const int ta = (int)xa.w;
+        for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
+        double wa[NR], dwa[NR];
+#pragma unroll
+        for (int b = 0; b < NR; ++b) {
+            wa[b] = p.w[(size_t)a * NR + b];
+            dwa[b] = p.dw[(size_t)a * NR + b];
+        }
+        __syncthreads();
+        double ea = 0, ga = 0, fax = 0, fay = 0, faz = 0;
+        double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+        for (int q0 = 0; q0 < m; q0 += blockDim.x) {
+            const int q = q0 + tid;
+            const bool active = q < m;
+            // own entry x
+            double vqx = 0, vqy = 0, vqz = 0, dq = 1, rq = 1, sq = 0, lam_qa = 0, lam_aq = 0, gq = 0;
+            double wq[NR], dwq[NR];
+            int jq = -1, tq = 0;
+            if (active) {
+                const int2 ent = p.atm_ent[e0 + q];
+                jq = ent.x;
+                const int Tx = sext8(ent.y & 0xff), Ty = sext8((ent.y >> 8) & 0xff), Tz = sext8((ent.y >> 16) & 0xff);
+                const double4 xj = p.xs[jq];
+                tq = (int)xj.w;
+                double sx, sy, sz;
+                image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+                vqx = xj.x + sx - xa.x;
+                vqy = xj.y + sy - xa.y;
+                vqz = xj.z + sz - xa.z;
+                dq = vqx * vqx + vqy * vqy + vqz * vqz;
+                rq = sqrt(dq);
+#pragma unroll
+                for (int b = 0; b < NR; ++b) {
+                    wq[b] = p.w[(size_t)jq * NR + b];
+                    dwq[b] = p.dw[(size_t)jq * NR + b];
+                }
+                const double *ya = yapex + tq * NR;        // C6_aq = y_{a,tq} . w_q
+                const double *yq = p.Y + ((size_t)jq * ne + ta) * NR; // dC6/dCN_a = y_{q,ta} . dw_a
+                double c6 = 0, dca = 0, dcq = 0;
+#pragma unroll
+                for (int b = 0; b < NR; ++b) {
+                    c6 += ya[b] * wq[b];
+                    dcq += ya[b] * dwq[b];
+                    dca += yq[b] * dwa[b];
+                }
+                sq = sqrt(c6);
+                lam_aq = c6 > 0 ? dca / c6 : 0.0;
+                lam_qa = c6 > 0 ? dcq / c6 : 0.0;
+                gq = pow(r0s[ta * ne + tq] / rq, 16.0 * third);
+            } else {
+#pragma unroll
+                for (int b = 0; b < NR; ++b) wq[b] = dwq[b] = 0.0;
+            }
+            double eq = 0, gq_acc = 0, fqx = 0, fqy = 0, fqz = 0;
+            for (int p0 = 0; p0 < m; p0 += tile) {
+                const int cnt = min(tile, m - p0);
+                __syncthreads();
+                for (int k = tid; k < cnt; k += blockDim.x) {
+                    const int2 ent = p.atm_ent[e0 + p0 + k];
+                    const int jp = ent.x;
+                    const int Tx = sext8(ent.y & 0xff), Ty = sext8((ent.y >> 8) & 0xff), Tz = sext8((ent.y >> 16) & 0xff);
+                    const double4 xj = p.xs[jp];
+                    const int tp = (int)xj.w;
+                    double sx, sy, sz;
+                    image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+                    Partner pr;
+                    pr.vx = xj.x + sx - xa.x;
+                    pr.vy = xj.y + sy - xa.y;
+                    pr.vz = xj.z + sz - xa.z;
+                    pr.d2 = pr.vx * pr.vx + pr.vy * pr.vy + pr.vz * pr.vz;
+                    pr.r = sqrt(pr.d2);
+                    const double *ya = yapex + tp * NR;
+                    const double *yp = p.Y + ((size_t)jp * ne + ta) * NR;
+                    double c6 = 0, dca = 0;
+#pragma unroll
+                    for (int b = 0; b < NR; ++b) {
+                        c6 += ya[b] * p.w[(size_t)jp * NR + b];
+                        dca += yp[b] * dwa[b];
+                    }
+                    pr.s = sqrt(c6);
+                    pr.lam = c6 > 0 ? dca / c6 : 0.0; // dlnC6_ap/dCN_a
+                    pr.g = pow(r0s[ta * ne + tp] / pr.r, 16.0 * third);
+                    pr.j = jp;
+                    pr.t = tp;
+                    ptile[k] = pr;
+                    for (int u = 0; u < ne * NR; ++u) ytile[(size_t)k * ne * NR + u] = p.Y[(size_t)jp * ne * NR + u];
+                }
+                __syncthreads();
+                if (!active) continue;
+                for (int k = 0; k < cnt; ++k) {
+                    if (p0 + k == q) continue;
+                    const Partner &pr = ptile[k];
+                    const double rx = vqx - pr.vx, ry = vqy - pr.vy, rz = vqz - pr.vz;
+                    const double d3 = rx * rx + ry * ry + rz * rz;
+                    if (d3 > p.ratm2 || d3 < 1e-12) continue;
+                    const double r3 = sqrt(d3);
+                    const double *yp = ytile + ((size_t)k * ne + tq) * NR; // C6_qp = y_{p,tq} . w_q
+                    double c6 = 0, dc6 = 0;
+#pragma unroll
+                    for (int b = 0; b < NR; ++b) {
+                        c6 += yp[b] * wq[b];
+                        dc6 += yp[b] * dwq[b];
+                    }
+                    const double s3 = sqrt(c6);
+                    const double lam_qp = c6 > 0 ? dc6 / c6 : 0.0;
+                    const double g3 = pow(r0s[tq * ne + pr.t] / r3, 16.0 * third);
+                    // weights (reference scale factors, src/d3_kernel.cu:1282-1290)
+                    const bool same = (jq == pr.j), qa = (jq == a), pa = (pr.j == a);
+                    double w, wf;
+                    if (same && qa) {
+                        w = 1.0 / 3.0;
+                        wf = 2.0;
+                    } else if (same) {
+                        w = 1.0;
+                        wf = 2.0;
+                    } else if (qa || pa) {
+                        w = 0.5;
+                        wf = 1.0;
+                    } else {
+                        w = 1.0;
+                        wf = 1.0;
+                    }
+                    if (p.atm_force_scaled) wf = w;
+                    const double d1 = dq, d2 = pr.d2;
+                    const double rsq = d1 * d2 * d3;
+                    const double rprod = rq * pr.r * r3;
+                    const double t1 = d1 + d2 - d3, t2 = d1 - d2 + d3, t3 = -d1 + d2 + d3;
+                    const double cosp = t1 * t2 * t3 / (8.0 * rsq);
+                    const double ir9 = 1.0 / (rsq * rprod);
+                    const double A = (1.0 + 3.0 * cosp) * ir9;
+                    const double dd = 0.375 * ir9 / rsq;
+                    const double dang1 = dd * (d1 * d1 * d1 + d1 * d1 * (d2 + d3) + d1 * (3.0 * d3 * d3 + 2.0 * d3 * d2 + 3.0 * d2 * d2) -
+                                               5.0 * (d3 - d2) * (d3 - d2) * (d3 + d2));
+                    const double dang2 = dd * (d2 * d2 * d2 + d2 * d2 * (d3 + d1) + d2 * (3.0 * d3 * d3 + 2.0 * d3 * d1 + 3.0 * d1 * d1) -
+                                               5.0 * (d3 - d1) * (d3 - d1) * (d3 + d1));
+                    const double dang3 = dd * (d3 * d3 * d3 + d3 * d3 * (d2 + d1) + d3 * (3.0 * d2 * d2 + 2.0 * d2 * d1 + 3.0 * d1 * d1) -
+                                               5.0 * (d2 - d1) * (d2 - d1) * (d2 + d1));
+                    const double x16 = x16c * gq * pr.g * g3;
+                    const double fd = 1.0 / (1.0 + 6.0 * x16);
+                    const double dfd = 32.0 * x16 * fd * fd;
+                    const double C9 = -sq * pr.s * s3;
+                    const double Et = C9 * A * fd;
+                    const double f1 = -C9 * (dang1 * fd - A * dfd) / d1;
+                    const double f2 = -C9 * (dang2 * fd - A * dfd) / d2;
+                    const double f3 = -C9 * (dang3 * fd - A * dfd) / d3;
+                    // own entry (atom x): energy share, dE/dCN_x, force on x
+                    eq += w * Et * third;
+                    gq_acc += w * 0.5 * Et * (lam_qa + lam_qp);
+                    fqx += wf * (f1 * vqx + f3 * rx);
+                    fqy += wf * (f1 * vqy + f3 * ry);
+                    fqz += wf * (f1 * vqz + f3 * rz);
+                    // apex share, halved (each unordered pair is visited twice)
+                    const double wh = 0.5 * w, wfh = 0.5 * wf;
+                    ea += wh * Et * third;
+                    ga += wh * 0.5 * Et * (lam_aq + pr.lam);
+                    fax -= wfh * (f1 * vqx + f2 * pr.vx);
+                    fay -= wfh * (f1 * vqy + f2 * pr.vy);
+                    faz -= wfh * (f1 * vqz + f2 * pr.vz);
+                    vxx += wh * (f1 * vqx * vqx + f2 * pr.vx * pr.vx + f3 * rx * rx);
+                    vyy += wh * (f1 * vqy * vqy + f2 * pr.vy * pr.vy + f3 * ry * ry);
+                    vzz += wh * (f1 * vqz * vqz + f2 * pr.vz * pr.vz + f3 * rz * rz);
+                    vxy += wh * (f1 * vqx * vqy + f2 * pr.vx * pr.vy + f3 * rx * ry);
+                    vxz += wh * (f1 * vqx * vqz + f2 * pr.vx * pr.vz + f3 * rx * rz);
+                    vyz += wh * (f1 * vqy * vqz + f2 * pr.vy * pr.vz + f3 * ry * rz);
+                }
+            }
+            if (active) {
+                atomicAdd(&p.eb[jq], eq);
+                atomicAdd(&p.gb[jq], gq_acc);
+                atomicAdd(&p.fb[3 * jq], fqx);
+                atomicAdd(&p.fb[3 * jq + 1], fqy);
+                atomicAdd(&p.fb[3 * jq + 2], fqz);
+            }
+        }
+        // apex reduction over the CTA (fixed order)
+        double vals[11] = {ea, ga, fax, fay, faz, vxx, vyy, vzz, vxy, vxz, vyz};
+        const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+        for (int k = 0; k < 11; ++k) {
+            const double v = warp_sum(vals[k]);
+            if (lane == 0) red[wid][k] = v;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double tot[11];
+            for (int k = 0; k < 11; ++k) {
+                tot[k] = 0;
+                for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) tot[k] += red[w2][k];
+            }
+            p.ea[a] = tot[0];
+            p.ga[a] = tot[1];
+            p.fa[3 * a] = tot[2];
+            p.fa[3 * a + 1] = tot[3];
+            p.fa[3 * a + 2] = tot[4];
+            const double sc = -1.0 / p.vol;
+            for (int k = 0; k < 6; ++k) p.va[6 * (size_t)a + k] = tot[5 + k] * sc;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// chain rule (src/d3_kernel.cu:1511-1698): F_i += (dE/dCN_i + dE/dCN_j) dCN_ij/dr r_hat
+// ------------------------------------------------------------------------------------
+__global__ void k_chain(KP p, const double *G) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= p.n) return;
+    const double4 xi = p.xs[i];
+    const int4 si = p.shift[i];
+    const double ri = p.rcov[(int)xi.w];
+    const double gi = G[i];
+    double fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+    traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, bool act) {
+        if (!act) return;
+        if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+        const double4 xj = p.xs[j];
+        double sx, sy, sz;
+        image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+        const double dx = xi.x - (xj.x + sx), dy = xi.y - (xj.y + sy), dz = xi.z - (xj.z + sz);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (!(d2 <= p.rcn2 && d2 > 0.0)) return;
+        double dcn;
+        cn_term(p, sqrt(d2), ri + p.rcov[(int)xj.w], &dcn);
+        const double dE = (gi + G[j]) * dcn;
+        fx += dE * dx;
+        fy += dE * dy;
+        fz += dE * dz;
+        vxx += dE * dx * dx;
+        vyy += dE * dy * dy;
+        vzz += dE * dz * dz;
+        vxy += dE * dx * dy;
+        vxz += dE * dx * dz;
+        vyz += dE * dy * dz;
+    });
+    fx = warp_sum(fx);
+    fy = warp_sum(fy);
+    fz = warp_sum(fz);
+    vxx = warp_sum(vxx);
+    vyy = warp_sum(vyy);
+    vzz = warp_sum(vzz);
+    vxy = warp_sum(vxy);
+    vxz = warp_sum(vxz);
+    vyz = warp_sum(vyz);
+    if ((threadIdx.x & 31) == 0) {
+        p.fc[3 * i] = fx;
+        p.fc[3 * i + 1] = fy;
+        p.fc[3 * i + 2] = fz;
+        const double sc = -1.0 / (2.0 * p.vol);
+        double *v = p.vc + 6 * (size_t)i;
+        v[0] = vxx * sc;
+        v[1] = vyy * sc;
+        v[2] = vzz * sc;
+        v[3] = vxy * sc;
+        v[4] = vxz * sc;
+        v[5] = vyz * sc;
+    }
+}
+
+__global__ void k_sum_g(KP p, double *G) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    G[i] = p.g2[i] + p.ga[i] + p.gb[i];
+}
+
+// forces in caller order, unit conversion (src/d3.cu:203-219)
+__global__ void k_forces_out(KP p) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= p.n) return;
+    const int i = p.orig[s];
+    const double cf = HARTREE_EV * ANG2BOHR;
+    for (int k = 0; k < 3; ++k)
+        p.out[1 + 3 * i + k] = (p.f2[3 * s + k] + p.fa[3 * s + k] + p.fb[3 * s + k] + p.fc[3 * s + k]) * cf;
+}
+
+// deterministic total energy and virial: one block, fixed order
+__global__ void k_reduce(KP p) {
+    __shared__ double red[32][7];
+    double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int s = threadIdx.x; s < p.n; s += blockDim.x) {
+        acc[0] += p.e2[s] + p.ea[s] + p.eb[s];
+        for (int k = 0; k < 6; ++k) acc[1 + k] += p.v2[6 * (size_t)s + k] + p.va[6 * (size_t)s + k] + p.vc[6 * (size_t)s + k];
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int k = 0; k < 7; ++k) {
+        const double v = warp_sum(acc[k]);
+        if (lane == 0) red[wid][k] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            for (int k = 0; k < 7; ++k) t[k] += red[w][k];
+        p.out[0] = -t[0] * HARTREE_EV;
+        const double cs = HARTREE_EV * ANG2BOHR * ANG2BOHR * ANG2BOHR;
+        double *st = p.out + 1 + 3 * (size_t)p.n;
+        // symmetric virial: xx yy zz xy xz yz
+        st[0] = t[1] * cs;
+        st[4] = t[2] * cs;
+        st[8] = t[3] * cs;
+        st[1] = st[3] = t[4] * cs;
+        st[2] = st[6] = t[5] * cs;
+        st[5] = st[7] = t[6] * cs;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void ensure(size_t m) {
+        if (m <= n && p) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        size_t want = std::max<size_t>(m, 1);
+        D3_CUDA(cudaMalloc(&p, want * sizeof(T)));
+        n = want;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct Engine {
+    // configuration
+    int nref = 5;
+    bool extended = false;
+    std::vector<int> elements; // sorted unique atomic numbers (handle slots)
+    int ne = 0;
+    uint64_t max_atoms = 0;
+    double rc = 0, rc_cn = 0, rc_atm = 0;
+    float rc_f = 0, rc_cn_f = 0;
+    bool use_atm = false;
+    int damping = 1, functional = 0;
+    FuncParams fp{};
+    Options opt{};
+    // state
+    uint64_t n = 0;
+    bool atoms_set = false, cell_set = false;
+    CellGeom geom{};
+    bool box_mode = true;
+    int64_t mcb[3] = {1, 1, 1};
+    int nb[3] = {1, 1, 1};
+    std::vector<StencilRow> st2, stc, sta;
+    int dev_sms = 148;
+    cudaStream_t stream = nullptr;
+    // tables
+    DBuf<double> t_cnref, t_c6, t_r0, t_rcov, t_r2r4, t_pairA;
+    // atoms
+    DBuf<double> pos_in;
+    DBuf<int> type_in, bin_in;
+    DBuf<int4> shift_in, shift;
+    DBuf<double4> xw_in, xs;
+    DBuf<int> bin_cnt, bin_start, bin_fill, order, bin_s, orig, sorted_of;
+    DBuf<double> cn, w, dw, Y, e2, g2, f2, v2, ea, ga, fa, va, eb, gb, fb, fc, vc, G;
+    DBuf<int> atm_cnt, work;
+    DBuf<long long> atm_off;
+    DBuf<int2> atm_ent;
+    long long atm_cap = 0;
+    DBuf<int4> st_dev;
+    DBuf<double> out;
+    DBuf<unsigned int> status;
+    std::vector<double> host_out;
+
+    ~Engine() {
+        DBuf<double> *ds[] = {&t_cnref, &t_c6, &t_r0, &t_rcov, &t_r2r4, &t_pairA, &pos_in, &cn, &w, &dw, &Y, &e2,
+                              &g2, &f2, &v2, &ea, &ga, &fa, &va, &eb, &gb, &fb, &fc, &vc, &G, &out};
+        for (auto *d : ds) d->release();
+        DBuf<int> *is[] = {&type_in, &bin_in, &bin_cnt, &bin_start, &bin_fill, &order, &bin_s, &orig, &sorted_of,
+                           &atm_cnt, &work};
+        for (auto *d : is) d->release();
+        shift_in.release();
+        shift.release();
+        xw_in.release();
+        xs.release();
+        atm_off.release();
+        atm_ent.release();
+        st_dev.release();
+        status.release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+static const double FUNC_TABLE[7][7] = {
+    // s6, s8_zero, s8_bj, sr6, sr8, a1, a2 (src/d3_types.h:46-54)
+    {1.0, 0.722, 0.7875, 1.217, 1.0, 0.4289, 4.4407}, {1.0, 0.928, 1.2177, 1.287, 1.0, 0.4145, 4.8593},
+    {1.0, 1.703, 1.9889, 1.261, 1.0, 0.3981, 4.4211}, {1.0, 1.682, 2.6996, 1.094, 1.0, 0.4298, 4.2359},
+    {1.0, 1.683, 3.2822, 1.139, 1.0, 0.3946, 4.8516}, {1.0, 1.010, 2.3550, 0.923, 1.0, 0.5238, 3.5016},
+    {1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0}};
+
+static FuncParams func_params(int functional, int damping) {
+    int idx = (functional >= 0 && functional <= 5) ? functional : 6;
+    // the reference stores these as float (real_t); keep the float-rounded values
+    auto f = [](double v) { return (double)(float)v; };
+    const double *t = FUNC_TABLE[idx];
+    FuncParams p;
+    p.s6 = f(t[0]);
+    if (damping == 1) {
+        p.s8 = f(t[2]);
+        p.p1 = f(t[5]);
+        p.p2 = f(t[6]);
+    } else {
+        p.s8 = f(t[1]);
+        p.p1 = f(t[3]);
+        p.p2 = f(t[4]);
+    }
+    return p;
+}
+
+static void upload_pair_table(Engine *e) {
+    std::vector<double> r2r4(e->ne), r0(e->ne * e->ne);
+    // recompute host copies from the device tables
+    D3_CUDA(cudaMemcpy(r2r4.data(), e->t_r2r4.p, sizeof(double) * e->ne, cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(r0.data(), e->t_r0.p, sizeof(double) * e->ne * e->ne, cudaMemcpyDeviceToHost));
+    std::vector<double> pa((size_t)e->ne * e->ne * 4, 0.0);
+    for (int i = 0; i < e->ne; ++i)
+        for (int j = 0; j < e->ne; ++j) {
+            double *q = &pa[((size_t)i * e->ne + j) * 4];
+            if (e->damping == 1) {
+                const double R0 = std::sqrt(3.0 * r2r4[i] * r2r4[j]);
+                const double A = e->fp.p1 * R0 + e->fp.p2;
+                const double A2 = A * A, A4 = A2 * A2;
+                q[0] = A4 * A2;
+                q[1] = A4 * A4;
+                q[2] = R0;
+            } else {
+                q[0] = r0[(size_t)i * e->ne + j];
+            }
+        }
+    e->t_pairA.ensure(pa.size());
+    D3_CUDA(cudaMemcpy(e->t_pairA.p, pa.data(), sizeof(double) * pa.size(), cudaMemcpyHostToDevice));
+}
+
+Engine *engine_create(const uint16_t *elements, uint64_t n_elements, uint64_t max_atoms, double rc, double rc_cn,
+                      double rc_atm, bool use_atm, int damping, int functional, bool extended, std::string &err) {
+    Engine *e = nullptr;
+    try {
+        if (!elements && n_elements) throw std::runtime_error("elements is NULL");
+        if (max_atoms == 0) throw std::runtime_error("max_length must be positive");
+        if (max_atoms > (uint64_t)INT32_MAX / 2) throw std::runtime_error("max_length too large");
+        if (damping != 0 && damping != 1) throw std::runtime_error("unknown damping type");
+        const int NE = extended ? D3_NE_EXTENDED : D3_NE_ORIGINAL;
+        const int NR = extended ? D3_NREF_EXTENDED : D3_NREF_ORIGINAL;
+        bool present[128] = {false};
+        for (uint64_t i = 0; i < n_elements; ++i) {
+            int z = elements[i];
+            int slot = extended ? z - 1 : z;
+            if (z >= 118 || slot < 0 || slot >= NE)
+                throw std::runtime_error("element " + std::to_string(z) + " is outside the parameter table");
+            present[z] = true;
+        }
+        e = new Engine();
+        e->extended = extended;
+        e->nref = NR;
+        for (int z = 0; z < 118; ++z)
+            if (present[z]) e->elements.push_back(z);
+        e->ne = (int)e->elements.size();
+        if (e->ne == 0) throw std::runtime_error("no elements given");
+        if (e->ne > MAX_TYPES) throw std::runtime_error("too many distinct elements for one handle");
+        e->max_atoms = max_atoms;
+        e->rc = rc;
+        e->rc_cn = rc_cn;
+        e->rc_atm = rc_atm;
+        e->rc_f = (float)rc;
+        e->rc_cn_f = (float)rc_cn;
+        e->use_atm = use_atm;
+        e->damping = damping;
+        e->functional = functional;
+        e->fp = func_params(functional, damping);
+        int dev = 0;
+        D3_CUDA(cudaGetDevice(&dev));
+        D3_CUDA(cudaDeviceGetAttribute(&e->dev_sms, cudaDevAttrMultiProcessorCount, dev));
+        D3_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+        // parameter tables: full synthetic table, gathered for this handle's elements
+        std::vector<float> c6((size_t)NE * NE * NR * NR * 3), r0((size_t)NE * NE), rcv(NE), rr(NE);
+        d3_synth_fill(D3_SYNTH_SEED, NE, NR, extended ? 1 : 0, c6.data(), r0.data(), rcv.data(), rr.data());
+        const int ne = e->ne;
+        std::vector<double> cnref((size_t)ne * MAX_NREF, -1.0), c6m((size_t)ne * ne * NR * NR, 0.0),
+            r0m((size_t)ne * ne), rcovm(ne), r2r4m(ne);
+        std::vector<int> slot(ne);
+        for (int i = 0; i < ne; ++i) slot[i] = extended ? e->elements[i] - 1 : e->elements[i];
+        auto C = [&](int si, int sj, int a, int b, int k) {
+            return c6[((((size_t)si * NE + sj) * NR + a) * NR + b) * 3 + k];
+        };
+        for (int i = 0; i < ne; ++i) {
+            rcovm[i] = rcv[slot[i]];
+            r2r4m[i] = rr[slot[i]];
+            for (int a = 0; a < NR; ++a) cnref[(size_t)i * MAX_NREF + a] = C(slot[i], slot[i], a, 0, 1) > -1.0f
+                                                                                  ? (double)C(slot[i], slot[i], a, 0, 1)
+                                                                                  : -1.0;
+        }
+        // the factorised weights need CNref to depend on (element, reference) only and
+        // validity to be per element; check that for every element pair of this handle
+        for (int i = 0; i < ne; ++i)
+            for (int j = 0; j < ne; ++j) {
+                r0m[(size_t)i * ne + j] = r0[(size_t)slot[i] * NE + slot[j]];
+                for (int a = 0; a < NR; ++a)
+                    for (int b = 0; b < NR; ++b) {
+                        float c1 = C(slot[i], slot[j], a, b, 1), c2 = C(slot[i], slot[j], a, b, 2);
+                        bool valid = c1 > -1.0f && c2 > -1.0f;
+                        bool vi = cnref[(size_t)i * MAX_NREF + a] > -1.0, vj = cnref[(size_t)j * MAX_NREF + b] > -1.0;
+                        if (valid != (vi && vj) ||
+                            (valid && ((double)c1 != cnref[(size_t)i * MAX_NREF + a] ||
+                                       (double)c2 != cnref[(size_t)j * MAX_NREF + b])))
+                            throw std::runtime_error("parameter table is not separable per element; "
+                                                     "the factorised C6 form cannot be used");
+                        c6m[(((size_t)i * ne + j) * NR + a) * NR + b] = valid ? (double)C(slot[i], slot[j], a, b, 0) : 0.0;
+                    }
+            }
+        e->t_cnref.ensure(cnref.size());
+        e->t_c6.ensure(c6m.size());
+        e->t_r0.ensure(r0m.size());
+        e->t_rcov.ensure(ne);
+        e->t_r2r4.ensure(ne);
+        D3_CUDA(cudaMemcpy(e->t_cnref.p, cnref.data(), sizeof(double) * cnref.size(), cudaMemcpyHostToDevice));
+        D3_CUDA(cudaMemcpy(e->t_c6.p, c6m.data(), sizeof(double) * c6m.size(), cudaMemcpyHostToDevice));
+        D3_CUDA(cudaMemcpy(e->t_r0.p, r0m.data(), sizeof(double) * r0m.size(), cudaMemcpyHostToDevice));
+        D3_CUDA(cudaMemcpy(e->t_rcov.p, rcovm.data(), sizeof(double) * ne, cudaMemcpyHostToDevice));
+        D3_CUDA(cudaMemcpy(e->t_r2r4.p, r2r4m.data(), sizeof(double) * ne, cudaMemcpyHostToDevice));
+        upload_pair_table(e);
+        // per-atom buffers at capacity
+        const size_t N = max_atoms;
+        e->pos_in.ensure(3 * N);
+        e->type_in.ensure(N);
+        e->bin_in.ensure(N);
+        e->shift_in.ensure(N);
+        e->shift.ensure(N);
+        e->xw_in.ensure(N);
+        e->xs.ensure(N);
+        e->order.ensure(N);
+        e->bin_s.ensure(N);
+        e->orig.ensure(N);
+        e->sorted_of.ensure(N);
+        e->cn.ensure(N);
+        e->w.ensure(N * NR);
+        e->dw.ensure(N * NR);
+        e->Y.ensure(N * ne * NR);
+        e->e2.ensure(N);
+        e->g2.ensure(N);
+        e->f2.ensure(3 * N);
+        e->v2.ensure(6 * N);
+        e->ea.ensure(N);
+        e->ga.ensure(N);
+        e->fa.ensure(3 * N);
+        e->va.ensure(6 * N);
+        e->eb.ensure(N);
+        e->gb.ensure(N);
+        e->fb.ensure(3 * N);
+        e->fc.ensure(3 * N);
+        e->vc.ensure(6 * N);
+        e->G.ensure(N);
+        e->atm_cnt.ensure(N);
+        e->atm_off.ensure(N + 1);
+        e->work.ensure(1);
+        e->out.ensure(1 + 3 * N + 9);
+        e->status.ensure(1);
+        e->host_out.resize(1 + 3 * N + 9);
+        return e;
+    } catch (const std::exception &ex) {
+        err = ex.what();
+        delete e;
+        return nullptr;
+    }
+}
+
+void engine_destroy(Engine *e) {
+    if (!e) return;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    delete e;
+}
+
+void engine_set_options(Engine *e, const Options &o) { e->opt = o; }
+Options engine_get_options(const Engine *e) { return e->opt; }
+void engine_set_functional_params(Engine *e, const FuncParams &p) {
+    e->fp = p;
+    upload_pair_table(e);
+}
+uint64_t engine_num_atoms(const Engine *e) { return e->n; }
+const double *engine_device_results(const Engine *e) { return e->out.p; }
+
+int engine_set_atoms(Engine *e, const double *pos_bohr, const uint16_t *Z, uint64_t n, std::string &err) {
+    try {
+        if (n > e->max_atoms)
+            throw std::runtime_error("length " + std::to_string(n) + " exceeds the handle capacity " +
+                                     std::to_string(e->max_atoms));
+        if (n == 0) throw std::runtime_error("no atoms given");
+        std::vector<int> types(n);
+        for (uint64_t i = 0; i < n; ++i) {
+            auto it = std::lower_bound(e->elements.begin(), e->elements.end(), (int)Z[i]);
+            if (it == e->elements.end() || *it != (int)Z[i])
+                throw std::runtime_error("element " + std::to_string(Z[i]) + " was not given when the handle was created");
+            types[i] = (int)(it - e->elements.begin());
+        }
+        D3_CUDA(cudaMemcpyAsync(e->pos_in.p, pos_bohr, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, e->stream));
+        D3_CUDA(cudaMemcpyAsync(e->type_in.p, types.data(), sizeof(int) * n, cudaMemcpyHostToDevice, e->stream));
+        D3_CUDA(cudaStreamSynchronize(e->stream));
+        e->n = n;
+        e->atoms_set = true;
+        return 0;
+    } catch (const std::exception &ex) {
+        err = ex.what();
+        return 1;
+    }
+}
+
+int engine_set_cell(Engine *e, const double cell[9], const float cell_f[9], std::string &err) {
+    try {
+        for (int i = 0; i < 9; ++i)
+            if (!std::isfinite(cell[i])) throw std::runtime_error("cell has a non-finite entry");
+        CellGeom g = make_geom(cell);
+        if (!(std::fabs(g.volume) > 1e-12) || !std::isfinite(g.volume)) throw std::runtime_error("degenerate cell");
+        e->geom = g;
+        e->box_mode = reference_box(cell_f, e->rc_f, e->rc_cn_f, e->mcb);
+        const double rmin = std::min(e->rc_cn, e->use_atm ? std::min(e->rc, e->rc_atm) : e->rc);
+        const double target = std::max(rmin / 6.0, 1.0);
+        const int64_t max_bins = std::max<int64_t>(64, (int64_t)std::max<uint64_t>(e->max_atoms, 1) * 2);
+        choose_bins(g, target, max_bins, e->nb);
+        e->st2 = build_stencil(g, e->nb, e->rc);
+        e->stc = build_stencil(g, e->nb, e->rc_cn);
+        e->sta = e->use_atm ? build_stencil(g, e->nb, e->rc_atm) : std::vector<StencilRow>();
+        std::vector<int4> all;
+        for (auto *v : {&e->st2, &e->stc, &e->sta})
+            for (auto &r : *v) all.push_back(make_int4(r.dy, r.dz, r.dxlo, r.dxhi));
+        e->st_dev.ensure(all.size());
+        D3_CUDA(cudaMemcpy(e->st_dev.p, all.data(), sizeof(int4) * all.size(), cudaMemcpyHostToDevice));
+        const int nbins = e->nb[0] * e->nb[1] * e->nb[2];
+        e->bin_cnt.ensure(nbins);
+        e->bin_fill.ensure(nbins);
+        e->bin_start.ensure(nbins + 1);
+        e->cell_set = true;
+        return 0;
+    } catch (const std::exception &ex) {
+        err = ex.what();
+        return 1;
+    }
+}
+
+static KP make_kp(Engine *e) {
+    KP p;
+    memset(&p, 0, sizeof(p));
+    p.n = (int)e->n;
+    p.ne = e->ne;
+    p.nref = e->nref;
+    for (int i = 0; i < 9; ++i) {
+        p.h[i] = e->geom.h[i];
+        p.inv[i] = e->geom.inv[i];
+    }
+    p.vol = e->geom.volume;
+    for (int k = 0; k < 3; ++k) {
+        p.nb[k] = e->nb[k];
+        p.half[k] = (int)(e->mcb[k] / 2);
+    }
+    p.nbins = e->nb[0] * e->nb[1] * e->nb[2];
+    p.box_mode = e->box_mode ? 1 : 0;
+    // cutoffs: the reference compares squared distances against rc*rc of its float cutoff
+    p.rc2 = e->rc * e->rc;
+    p.rcn2 = e->rc_cn * e->rc_cn;
+    p.ratm2 = e->rc_atm * e->rc_atm;
+    p.rc_cn = e->rc_cn;
+    p.cnref = e->t_cnref.p;
+    p.c6 = e->t_c6.p;
+    p.r0ab = e->t_r0.p;
+    p.rcov = e->t_rcov.p;
+    p.r2r4 = e->t_r2r4.p;
+    p.pairA = e->t_pairA.p;
+    p.s6 = e->fp.s6;
+    p.s8 = e->fp.s8;
+    p.p1 = e->fp.p1;
+    p.p2 = e->fp.p2;
+    p.damping = e->damping;
+    p.smooth_cn = e->opt.smooth_cn ? 1 : 0;
+    p.atm_force_scaled = e->opt.atm_force_scaled ? 1 : 0;
+    p.pos_in = e->pos_in.p;
+    p.type_in = e->type_in.p;
+    p.bin_in = e->bin_in.p;
+    p.shift_in = e->shift_in.p;
+    p.xw_in = e->xw_in.p;
+    p.bin_cnt = e->bin_cnt.p;
+    p.bin_start = e->bin_start.p;
+    p.bin_fill = e->bin_fill.p;
+    p.order = e->order.p;
+    p.xs = e->xs.p;
+    p.shift = e->shift.p;
+    p.bin_s = e->bin_s.p;
+    p.orig = e->orig.p;
+    p.sorted_of = e->sorted_of.p;
+    p.cn = e->cn.p;
+    p.w = e->w.p;
+    p.dw = e->dw.p;
+    p.Y = e->Y.p;
+    p.e2 = e->e2.p;
+    p.g2 = e->g2.p;
+    p.f2 = e->f2.p;
+    p.v2 = e->v2.p;
+    p.ea = e->ea.p;
+    p.ga = e->ga.p;
+    p.fa = e->fa.p;
+    p.va = e->va.p;
+    p.eb = e->eb.p;
+    p.gb = e->gb.p;
+    p.fb = e->fb.p;
+    p.fc = e->fc.p;
+    p.vc = e->vc.p;
+    p.atm_cnt = e->atm_cnt.p;
+    p.atm_off = e->atm_off.p;
+    p.atm_ent = e->atm_ent.p;
+    p.atm_cap = e->atm_cap;
+    p.work = e->work.p;
+    p.st2 = e->st_dev.p;
+    p.nst2 = (int)e->st2.size();
+    p.stc = e->st_dev.p + e->st2.size();
+    p.nstc = (int)e->stc.size();
+    p.sta = e->st_dev.p + e->st2.size() + e->stc.size();
+    p.nsta = (int)e->sta.size();
+    p.out = e->out.p;
+    p.status = e->status.p;
+    return p;
+}
+
+template <int NR>
+static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
+    KP p = p0;
+    const int n = p.n;
+    const int T = 256;
+    const int gb = (n + T - 1) / T;
+    const int gw = (int)(((long long)n * 32 + T - 1) / T);
+    D3_CUDA(cudaMemsetAsync(p.bin_cnt, 0, sizeof(int) * p.nbins, s));
+    D3_CUDA(cudaMemsetAsync(p.bin_fill, 0, sizeof(int) * p.nbins, s));
+    k_bin<<<gb, T, 0, s>>>(p);
+    k_scan<int, int><<<1, 1024, 0, s>>>(p.bin_cnt, p.bin_start, p.nbins);
+    k_scatter<<<gb, T, 0, s>>>(p);
+    k_binsort<<<(p.nbins + T - 1) / T, T, 0, s>>>(p);
+    k_gather<<<gb, T, 0, s>>>(p);
+    k_cn<<<gw, T, 0, s>>>(p);
+    k_weights<NR><<<gb, T, 0, s>>>(p);
+    k_twobody<NR><<<gw, T, 0, s>>>(p);
+    D3_CUDA(cudaMemsetAsync(p.ea, 0, sizeof(double) * n, s));
+    D3_CUDA(cudaMemsetAsync(p.ga, 0, sizeof(double) * n, s));
+    D3_CUDA(cudaMemsetAsync(p.fa, 0, sizeof(double) * 3 * n, s));
+    D3_CUDA(cudaMemsetAsync(p.va, 0, sizeof(double) * 6 * n, s));
+    D3_CUDA(cudaMemsetAsync(p.eb, 0, sizeof(double) * n, s));
+    D3_CUDA(cudaMemsetAsync(p.gb, 0, sizeof(double) * n, s));
+    D3_CUDA(cudaMemsetAsync(p.fb, 0, sizeof(double) * 3 * n, s));
+    if (e->use_atm) {
+        k_atm_list<false><<<gw, T, 0, s>>>(p);
+        k_scan<long long, int><<<1, 1024, 0, s>>>(p.atm_cnt, p.atm_off, n);
+        k_atm_list<true><<<gw, T, 0, s>>>(p);
+        D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
+        // partner tile: as many entries as fit in ~160 KB next to the apex tables
+        const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double);
+        const size_t per = sizeof(Partner) + (size_t)p.ne * NR * sizeof(double);
+        const int tile = (int)std::max<size_t>(8, std::min<size_t>(128, (160 * 1024 - fixed) / per));
+        const size_t sm = (size_t)tile * per + fixed;
+        D3_CUDA(cudaFuncSetAttribute(k_atm<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int blocks_per_sm = 0;
+        D3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_atm<NR>, ATM_THREADS, sm));
+        const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, blocks_per_sm)));
+        k_atm<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
+    }
+    k_sum_g<<<gb, T, 0, s>>>(p, e->G.p);
+    k_chain<<<gw, T, 0, s>>>(p, e->G.p);
+    k_forces_out<<<gb, T, 0, s>>>(p);
+    k_reduce<<<1, 1024, 0, s>>>(p);
+    D3_CUDA(cudaGetLastError());
+}
+
+uint16_t engine_compute(Engine *e, double *energy, double *forces, double *stress, cudaStream_t stream, bool sync) {
+    if (!e->atoms_set || !e->cell_set) return ST_NOT_READY;
+    cudaStream_t s = stream ? stream : e->stream;
+    try {
+        const uint64_t n = e->n;
+        if (e->use_atm && e->atm_cap == 0) {
+            // initial list capacity from the density of the half sphere, with margin
+            const double rho = (double)n / std::fabs(e->geom.volume);
+            const double k_half = 0.5 * rho * 4.18879020478639 * e->rc_atm * e->rc_atm * e->rc_atm;
+            e->atm_cap = (long long)(n * (k_half * 1.25 + 64.0));
+            e->atm_ent.ensure((size_t)e->atm_cap);
+        }
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            D3_CUDA(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned int), s));
+            KP p = make_kp(e);
+            if (e->nref == 5)
+                launch_all<5>(e, p, s);
+            else
+                launch_all<7>(e, p, s);
+            if (!sync) return ST_OK;
+            unsigned int st = 0;
+            D3_CUDA(cudaMemcpyAsync(&st, e->status.p, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+            D3_CUDA(cudaStreamSynchronize(s));
+            if ((st & ST_LIST_OVERFLOW) && e->use_atm) {
+                long long need = 0;
+                D3_CUDA(cudaMemcpy(&need, e->atm_off.p + n, sizeof(long long), cudaMemcpyDeviceToHost));
+                e->atm_cap = (long long)(need * 1.1) + 1024;
+                e->atm_ent.ensure((size_t)e->atm_cap);
+                continue;
+            }
+            const size_t nout = 1 + 3 * n + 9;
+            D3_CUDA(cudaMemcpyAsync(e->host_out.data(), e->out.p, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
+            D3_CUDA(cudaStreamSynchronize(s));
+            if (energy) *energy = e->host_out[0];
+            if (forces) memcpy(forces, e->host_out.data() + 1, sizeof(double) * 3 * n);
+            if (stress) memcpy(stress, e->host_out.data() + 1 + 3 * n, sizeof(double) * 9);
+            return (uint16_t)st;
+        }
+        return ST_LIST_OVERFLOW;
+    } catch (const std::exception &ex) {
+        fprintf(stderr, "d3: %s\n", ex.what());
+        return ST_CUDA_ERROR;
+    }
+}
+
+int engine_debug_atom_arrays(Engine *e, double *cn, double *dedcn, double *energy_atoms) {
+    const uint64_t n = e->n;
+    std::vector<int> orig(n);
+    std::vector<double> a(n), b(n), c(n), d(n), g(n);
+    D3_CUDA(cudaStreamSynchronize(e->stream));
+    D3_CUDA(cudaMemcpy(orig.data(), e->orig.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(a.data(), e->cn.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(g.data(), e->G.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(b.data(), e->e2.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(c.data(), e->ea.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(d.data(), e->eb.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    for (uint64_t s = 0; s < n; ++s) {
+        const int i = orig[s];
+        if (cn) cn[i] = a[s];
+        if (dedcn) dedcn[i] = g[s];
+        if (energy_atoms) energy_atoms[i] = b[s] + (e->use_atm ? c[s] + d[s] : 0.0);
+    }
+    return 0;
+}
+
+int64_t engine_debug_atm_pairs(Engine *e, int64_t *outp, int64_t cap) {
+    // returns (apex, j, Tref_x, Tref_y, Tref_z) rows in caller indices and reference shifts
+    if (!e->use_atm) return 0;
+    const uint64_t n = e->n;
+    std::vector<long long> off(n + 1);
+    std::vector<int> orig(n);
+    std::vector<int4> sh(n);
+    D3_CUDA(cudaStreamSynchronize(e->stream));
+    D3_CUDA(cudaMemcpy(off.data(), e->atm_off.p, sizeof(long long) * (n + 1), cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(orig.data(), e->orig.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(sh.data(), e->shift.p, sizeof(int4) * n, cudaMemcpyDeviceToHost));
+    const long long tot = off[n];
+    std::vector<int2> ent((size_t)tot);
+    if (tot) D3_CUDA(cudaMemcpy(ent.data(), e->atm_ent.p, sizeof(int2) * tot, cudaMemcpyDeviceToHost));
+    if (!outp) return tot;
+    int64_t k = 0;
+    for (uint64_t a = 0; a < n && k < cap; ++a)
+        for (long long q = off[a]; q < off[a + 1] && k < cap; ++q, ++k) {
+            const int j = ent[q].x;
+            const int T[3] = {(int)(int8_t)(ent[q].y & 0xff), (int)(int8_t)((ent[q].y >> 8) & 0xff),
+                              (int)(int8_t)((ent[q].y >> 16) & 0xff)};
+            const int sa[3] = {sh[a].x, sh[a].y, sh[a].z}, sj[3] = {sh[j].x, sh[j].y, sh[j].z};
+            int64_t *r = outp + 5 * k;
+            r[0] = orig[a];
+            r[1] = orig[j];
+            // unwrapped: x_a - (x_j + Tref h) equals the wrapped pair vector
+            for (int c = 0; c < 3; ++c) r[2 + c] = T[c] + sa[c] - sj[c];
+        }
+    return k;
+}
+
+int engine_debug_bins(Engine *e, int64_t *wrap_shift, int64_t *bin_index, int nb_out[3]) {
+    const uint64_t n = e->n;
+    std::vector<int4> sh(n);
+    std::vector<int> b(n);
+    D3_CUDA(cudaStreamSynchronize(e->stream));
+    D3_CUDA(cudaMemcpy(sh.data(), e->shift_in.p, sizeof(int4) * n, cudaMemcpyDeviceToHost));
+    D3_CUDA(cudaMemcpy(b.data(), e->bin_in.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    for (uint64_t i = 0; i < n; ++i) {
+        if (wrap_shift) {
+            wrap_shift[3 * i] = sh[i].x;
+            wrap_shift[3 * i + 1] = sh[i].y;
+            wrap_shift[3 * i + 2] = sh[i].z;
+        }
+        if (bin_index) bin_index[i] = b[i];
+    }
+    if (nb_out)
+        for (int k = 0; k < 3; ++k) nb_out[k] = e->nb[k];
+    return 0;
+}
+
+} // namespace d3

@@ -1,0 +1,72 @@
+// Internal engine interface for the B200 D3 dispersion path.
+//
+// The engine replaces the reference's d3.cu driver, d3_buffer device storage and the
+// d3_kernel passes (LASP-D3 src/d3.cu:130-226, src/d3_buffer.cu, src/d3_kernel.cu):
+//   wrap + bin (GPU counting sort) -> CN -> per-atom Gaussian C6 weights ->
+//   [ATM half-list build -> ATM triplets] + two-body -> dE/dCN chain rule -> reductions.
+// Everything for one evaluation runs on one stream with no host synchronisation until
+// the final device-to-host copy.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "d3_geometry.h"
+
+namespace d3 {
+
+constexpr double ANG2BOHR = 1.0 / 0.52917726;   // src/d3.cu:50 (here in double)
+constexpr double HARTREE_EV = 27.211396641308;   // src/d3.cu:205
+constexpr int MAX_NREF = 7;
+constexpr int MAX_TYPES = 32;
+
+// status bits (0 = success, bit 0 = neighbour-list overflow as in the reference's
+// d3_internal.h:7, other bits are additions of this engine)
+enum : uint16_t {
+    ST_OK = 0,
+    ST_LIST_OVERFLOW = 1u << 0,
+    ST_BAD_INPUT = 1u << 1,      // non-finite coordinate or cell
+    ST_BAD_CELL = 1u << 2,       // degenerate cell
+    ST_SHIFT_RANGE = 1u << 3,    // lattice shift outside the packed range
+    ST_CUDA_ERROR = 1u << 4,
+    ST_NOT_READY = 1u << 5,      // atoms or cell not set
+};
+
+struct FuncParams {
+    double s6, s8, p1, p2; // zero: p1 = sr6, p2 = sr8; BJ: p1 = a1, p2 = a2
+};
+
+struct Options {
+    bool atm_force_scaled = false; // false: reference convention (ATM forces not scaled
+                                   // by the 1/2, 1/6 repeated-index factors)
+    bool smooth_cn = false;        // tanh^3 CN cutoff (reference SMOOTH_CUTOFF_CN)
+};
+
+struct Engine;
+
+Engine *engine_create(const uint16_t *elements, uint64_t n_elements, uint64_t max_atoms, double rc, double rc_cn,
+                      double rc_atm, bool use_atm, int damping, int functional, bool extended, std::string &err);
+void engine_destroy(Engine *e);
+int engine_set_atoms(Engine *e, const double *pos_bohr, const uint16_t *Z, uint64_t n, std::string &err);
+int engine_set_cell(Engine *e, const double cell_bohr[9], const float cell_bohr_f[9], std::string &err);
+void engine_set_options(Engine *e, const Options &o);
+Options engine_get_options(const Engine *e);
+void engine_set_functional_params(Engine *e, const FuncParams &p);
+// Runs the whole evaluation on `stream` (the engine's own stream when null) and,
+// when sync is true, waits and copies results to the host outputs (eV, eV/A, eV/A^3,
+// caller's atom order). Returns the status word.
+uint16_t engine_compute(Engine *e, double *energy_ev, double *forces_ev_a, double *stress_ev_a3,
+                        cudaStream_t stream, bool sync);
+// device-resident results of the last evaluation (eV units, caller order)
+const double *engine_device_results(const Engine *e); // [1 + 3n + 9]
+uint64_t engine_num_atoms(const Engine *e);
+
+// diagnostics for tests: coordination numbers, dE/dCN, per-atom energies (hartree),
+// in the caller's atom order; ATM list (caller indices and reference lattice shifts)
+int engine_debug_atom_arrays(Engine *e, double *cn, double *dedcn, double *energy_atoms);
+int64_t engine_debug_atm_pairs(Engine *e, int64_t *out, int64_t cap);
+int engine_debug_bins(Engine *e, int64_t *wrap_shift, int64_t *bin_index, int nb_out[3]);
+
+} // namespace d3

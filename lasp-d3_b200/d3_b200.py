@@ -1,0 +1,168 @@
+"""ctypes binding of libd3.so for Python callers that want the FP64 path and the
+engine extensions (the reference-compatible cffi binding is d3_cffi.py).
+
+    from d3_b200 import D3
+    d3 = D3(elements=[1, 6, 8], max_atoms=96, rc=95.0, rc_cn=40.0, rc_atm=40.0)
+    d3.set_cell(cell)            # Angstrom, rows = lattice vectors
+    d3.set_atoms(pos, Z)         # Angstrom
+    e, f, s = d3.compute()       # eV, eV/A [n,3], eV/A^3 [3,3] (float64)
+
+The library must be built (python lasp-d3_b200/build.py); loading fails loudly when
+it is missing -- there is no CPU fallback.
+"""
+import ctypes
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libd3.so")
+HEADER = os.path.join(HERE, "..", "include", "d3.h")
+
+ZERO_DAMPING, BJ_DAMPING = 0, 1
+OPT_ATM_FORCE_SCALED, OPT_SMOOTH_CN = 1, 2
+TABLE_5REF, TABLE_7REF = 0, 1
+
+_lib = None
+
+
+def load_library(path=None):
+    """Load libd3.so (raises OSError when it is not built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise OSError("libd3.so not found at %s; build it with python lasp-d3_b200/build.py" % p)
+    lib = ctypes.CDLL(p)
+    vp, u64, i64, f32, f64 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+    lib.init_d3_handle.restype = vp
+    lib.init_d3_handle.argtypes = [vp, u64, u64, f32, f32, ctypes.c_int, ctypes.c_int]
+    lib.init_d3_handle_with_atm.restype = vp
+    lib.init_d3_handle_with_atm.argtypes = [vp, u64, u64, f32, f32, f32, ctypes.c_int, ctypes.c_int]
+    lib.set_atoms.restype = None
+    lib.set_atoms.argtypes = [vp, vp, vp, u64]
+    lib.set_cell.restype = None
+    lib.set_cell.argtypes = [vp, vp]
+    lib.free_d3_handle.restype = None
+    lib.free_d3_handle.argtypes = [vp]
+    lib.clear_d3_handle.restype = None
+    lib.clear_d3_handle.argtypes = [vp]
+    lib.compute_dispersion_energy_from_handle.restype = None
+    lib.compute_dispersion_energy_from_handle.argtypes = [vp, vp, vp, vp]
+    lib.compute_dispersion_energy_from_handle_status.restype = ctypes.c_uint16
+    lib.compute_dispersion_energy_from_handle_status.argtypes = [vp, vp, vp, vp]
+    lib.compute_dispersion_energy.restype = None
+    lib.compute_dispersion_energy.argtypes = [vp, vp, u64, vp, f32, f32, ctypes.c_int, ctypes.c_int, vp, vp, vp]
+    lib.d3_init_handle_ex.restype = vp
+    lib.d3_init_handle_ex.argtypes = [vp, u64, u64, f64, f64, f64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.d3_set_atoms_f64.restype = ctypes.c_int
+    lib.d3_set_atoms_f64.argtypes = [vp, vp, vp, u64]
+    lib.d3_set_cell_f64.restype = ctypes.c_int
+    lib.d3_set_cell_f64.argtypes = [vp, vp]
+    lib.d3_compute_f64.restype = ctypes.c_uint16
+    lib.d3_compute_f64.argtypes = [vp, vp, vp, vp]
+    lib.d3_set_option.restype = ctypes.c_int
+    lib.d3_set_option.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.d3_set_functional_params.restype = ctypes.c_int
+    lib.d3_set_functional_params.argtypes = [vp, f64, f64, f64, f64]
+    lib.d3_compute_async.restype = ctypes.c_uint16
+    lib.d3_compute_async.argtypes = [vp, vp]
+    lib.d3_device_results.restype = vp
+    lib.d3_device_results.argtypes = [vp]
+    lib.d3_last_error.restype = ctypes.c_char_p
+    lib.d3_last_error.argtypes = []
+    lib.d3_debug_atom_arrays.restype = ctypes.c_int
+    lib.d3_debug_atom_arrays.argtypes = [vp, vp, vp, vp]
+    lib.d3_debug_atm_pairs.restype = i64
+    lib.d3_debug_atm_pairs.argtypes = [vp, vp, i64]
+    lib.d3_debug_bins.restype = ctypes.c_int
+    lib.d3_debug_bins.argtypes = [vp, vp, vp, vp]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def declared_symbols(header=HEADER):
+    """Function names declared in include/d3.h."""
+    txt = open(header).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", txt)) - {"if", "sizeof", "defined"})
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class D3:
+    """One engine handle (FP64 path)."""
+
+    def __init__(self, elements, max_atoms, rc=95.0, rc_cn=40.0, rc_atm=None, damping=BJ_DAMPING, functional=0,
+                 table=TABLE_5REF):
+        self.lib = load_library()
+        el = np.ascontiguousarray(sorted(set(int(z) for z in elements)), np.uint16)
+        self.h = self.lib.d3_init_handle_ex(_ptr(el), len(el), int(max_atoms), float(rc), float(rc_cn),
+                                            float(rc_atm) if rc_atm else 0.0, int(damping), int(functional),
+                                            int(table))
+        if not self.h:
+            raise RuntimeError("d3_init_handle_ex failed: %s" % self.lib.d3_last_error().decode())
+        self.n = 0
+
+    def set_option(self, opt, value):
+        if self.lib.d3_set_option(self.h, int(opt), int(value)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+
+    def set_functional_params(self, s6, s8, p1, p2):
+        self.lib.d3_set_functional_params(self.h, s6, s8, p1, p2)
+
+    def set_atoms(self, pos, Z):
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+        z = np.ascontiguousarray(Z, np.uint16)
+        if self.lib.d3_set_atoms_f64(self.h, _ptr(pos), _ptr(z), len(z)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+        self.n = len(z)
+
+    def set_cell(self, cell):
+        c = np.ascontiguousarray(cell, np.float64).reshape(9)
+        if self.lib.d3_set_cell_f64(self.h, _ptr(c)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+
+    def compute(self, check=True):
+        e = np.zeros(1)
+        f = np.zeros((self.n, 3))
+        s = np.zeros(9)
+        st = self.lib.d3_compute_f64(self.h, _ptr(e), _ptr(f), _ptr(s))
+        self.status = int(st)
+        if check and st != 0:
+            raise RuntimeError("d3_compute_f64 status %d: %s" % (st, self.lib.d3_last_error().decode()))
+        return float(e[0]), f, s.reshape(3, 3)
+
+    def atom_arrays(self):
+        cn, g, e = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        self.lib.d3_debug_atom_arrays(self.h, _ptr(cn), _ptr(g), _ptr(e))
+        return cn, g, e
+
+    def atm_pairs(self):
+        m = self.lib.d3_debug_atm_pairs(self.h, None, 0)
+        rows = np.zeros((max(m, 1), 5), np.int64)
+        k = self.lib.d3_debug_atm_pairs(self.h, _ptr(rows), m)
+        return rows[:k]
+
+    def bins(self):
+        sh = np.zeros((self.n, 3), np.int64)
+        b = np.zeros(self.n, np.int64)
+        nb = np.zeros(3, np.int32)
+        self.lib.d3_debug_bins(self.h, _ptr(sh), _ptr(b), _ptr(nb))
+        return sh, b, nb
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.free_d3_handle(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

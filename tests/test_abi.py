@@ -1,0 +1,67 @@
+"""The C-ABI library builds, loads and exports every symbol include/d3.h declares
+(no compute call: these run without a GPU)."""
+import ctypes
+import os
+import subprocess
+
+import pytest
+
+import d3_b200
+
+REFERENCE_ABI = [
+    "compute_dispersion_energy", "init_d3_handle", "init_d3_handle_with_atm", "set_atoms", "set_cell",
+    "free_d3_handle", "clear_d3_handle", "compute_dispersion_energy_from_handle",
+    "compute_dispersion_energy_from_handle_status",
+]
+
+
+def _exported(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if " T " in line}
+
+
+def test_library_exports_every_declared_symbol():
+    assert os.path.exists(d3_b200.LIB_PATH), "build libd3.so first (python lasp-d3_b200/build.py)"
+    declared = set(d3_b200.declared_symbols())
+    assert set(REFERENCE_ABI) <= declared
+    missing = declared - _exported(d3_b200.LIB_PATH)
+    assert not missing, missing
+
+
+def test_reference_abi_symbols_are_c_linkage():
+    exp = _exported(d3_b200.LIB_PATH)
+    for s in REFERENCE_ABI:
+        assert s in exp  # unmangled: callable from C, Fortran bind(c) and cffi
+
+
+def test_library_loads_and_binds():
+    lib = d3_b200.load_library()
+    assert lib.d3_last_error() is not None
+
+
+def test_header_compiles_as_c():
+    hdr = os.path.abspath(os.path.join(os.path.dirname(d3_b200.__file__), "..", "include"))
+    src = '#include "d3.h"\nint main(void){ d3_handle_t *h = 0; (void)h; return 0; }\n'
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", hdr, "-x", "c", "-", "-o", "/dev/null"],
+                       input=src, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_null_handle_paths_do_not_crash():
+    lib = d3_b200.load_library()
+    assert lib.compute_dispersion_energy_from_handle_status(None, None, None, None) == 1
+    lib.set_atoms(None, None, None, 0)
+    lib.set_cell(None, None)
+    lib.clear_d3_handle(None)
+    lib.free_d3_handle(None)
+    assert lib.d3_set_option(None, 1, 1) == 1
+    assert b"NULL" in lib.d3_last_error()
+
+
+def test_cffi_binding_declares_reference_api():
+    pytest.importorskip("cffi")
+    import d3_cffi
+
+    for s in REFERENCE_ABI[:2] + ["init_d3_handle_with_atm", "set_atoms", "set_cell",
+                                  "compute_dispersion_energy_from_handle_status"]:
+        assert hasattr(d3_cffi.lib, s)
