@@ -1,0 +1,337 @@
+"""Benchmark of the D3(BJ)+ATM energy/force/stress path on B200.
+
+Workload (one "step" = one full evaluation: wrap/bin, CN, C6 weights, two-body, ATM
+list + triplets, dE/dCN chain rule, reductions, E + F + stress):
+  20,000-atom triclinic periodic box, cell rows a=(58,0,0), b=(5,58,0), c=(3,4,58) A,
+  uniform positions with a 1.0 A minimum-image rejection, H 40 / C 30 / N 10 / O 15 /
+  Cu 5 %, PBE-D3(BJ) (s6 1, s8 0.7875, a1 0.4289, a2 4.4407) with ATM, 5-reference
+  table, cutoffs 95 (two-body) / 40 (CN) / 40 (ATM) bohr. Seeded synthetic input; the
+  parameter table is the seeded synthetic table (the real D3 tables are not available).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Multi-GPU (torchrun, one process per GPU): every rank evaluates its own box (different
+seed), no data-path collective; value = all atoms / max-over-ranks time ("weak").
+The reference arm times the reference's own CUDA build (oracle/_ref) through its C ABI
+on a bounded sample of the same generator (rank 0 only).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lasp-d3_b200"))
+
+METRIC = "D3(BJ)+ATM atoms/s (E+F+stress) on 1 B200: plain vs chosen form at stated error"
+RC, RC_CN, RC_ATM = 95.0, 40.0, 40.0
+N_ATOMS = 20000
+# Algorithmic FLOPs of one ATM triplet term as the reference writes it
+# (src/d3_kernel.cu:1331-1447: geometry, angular term and its three derivatives, C9 and
+# its CN derivatives, damping and derivative, energy, forces, symmetric virial), counted
+# with add/mul/cmp = 1, fma = 2, div/sqrt/pow = 1; C6 interpolation is per pair and not
+# included. See DESIGN.md ("Roofline") for the itemised count.
+ATM_FLOP_PER_TRIPLET = 294
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload_config(n, form):
+    return {
+        "workload": "%d-atom triclinic periodic box (a=(58,0,0) b=(5,58,0) c=(3,4,58) A, scaled for other sizes), "
+                    "H40/C30/N10/O15/Cu5 %%, 1.0 A min-image rejection; PBE-D3(BJ)+ATM, 5-reference synthetic "
+                    "table, rc 95 / rc_CN 40 / rc_ATM 40 bohr; energy+forces+stress" % n,
+        "atoms_per_gpu": n,
+        "form": form,
+        "l2": "flushed between timed steps (256 MiB device write)",
+        "parallelism": "replicas: one box per GPU, no collective",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons, power = [], None, set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_cpu_baseline(sys_, sample=48, seed=7):
+    """FP64 oracle (C/OpenMP, all host threads) on a bounded sample: CN for every atom,
+    then two-body, ATM (as apex) and chain rule for `sample` random central atoms."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    n = len(sys_["Z"])
+    rng = np.random.default_rng(seed)
+    sub = np.sort(rng.choice(n, size=sample, replace=False))
+    cores = os.cpu_count() or 1
+    kw = dict(rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0, c6_mode=1, nthreads=cores)
+    t0 = time.perf_counter()
+    oracle.compute(sys_["pos"], sys_["Z"], sys_["cell"], subset=np.zeros(0, np.int64), **kw)
+    t_cn = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.compute(sys_["pos"], sys_["Z"], sys_["cell"], subset=sub, **kw)
+    t_sub = time.perf_counter() - t0 - t_cn
+    per_atom_s = t_sub / sample + t_cn / n
+    return {"value": 1.0 / per_atom_s, "unit": "atoms/s", "cores": cores, "kind": "port",
+            "sample": "FP64 C/OpenMP oracle of the reference formulas (factorised C6) on the same box: CN for all "
+                      "%d atoms (%.1f s) plus two-body, ATM apex and chain rule for %d random atoms (%.1f s); "
+                      "atoms/s = 1 / (t_sample/%d + t_cn/%d)" % (n, t_cn, sample, t_sub, sample, n)}
+
+
+def engine_arm(args, world, rank, local):
+    import torch
+
+    import d3_systems as S
+    from d3_b200 import D3, peak_probe
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    n = args.atoms
+    sys_ = S.triclinic_box(n, seed=1 + rank)
+    d = D3(sys_["Z"], n, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
+    d.set_cell(sys_["cell"])
+    d.set_atoms(sys_["pos"], sys_["Z"])
+    energy, forces, stress = d.compute()  # sizes the ATM list
+    stream = torch.cuda.Stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.zero_()
+            d.compute_async(stream.cuda_stream)
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    step_ms, atm_ms, passes = [], [], []
+    counters = None
+    barrier()
+    with torch.cuda.stream(stream):
+        for _ in range(args.steps):
+            flush.zero_()
+            s_ev = torch.cuda.Event(enable_timing=True)
+            e_ev = torch.cuda.Event(enable_timing=True)
+            s_ev.record(stream)
+            st = d.compute_async(stream.cuda_stream)
+            e_ev.record(stream)
+            e_ev.synchronize()
+            if st != 0:
+                raise RuntimeError("engine status %d" % st)
+            step_ms.append(s_ev.elapsed_time(e_ev))
+            pt, counters = d.pass_times()
+            passes.append(pt)
+            atm_ms.append(pt["atm"])
+    barrier()
+    clocks = sampler.stop()
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * n / (ms_per_step * 1e-3)
+
+    # end to end through the reference-facing C ABI: float host buffers in, float out,
+    # host<->device copies inside the timed region
+    import ctypes
+
+    lib = d.lib
+    z16 = np.ascontiguousarray(sys_["Z"], np.uint16)
+    posf = np.ascontiguousarray(sys_["pos"], np.float32)
+    cellf = np.ascontiguousarray(sys_["cell"], np.float32)
+    h = lib.init_d3_handle_with_atm(z16.ctypes.data, n, n, RC, RC_CN, RC_ATM, 1, 0)
+    lib.set_cell(h, cellf.ctypes.data)
+    ef = np.zeros(1, np.float32)
+    ff = np.zeros((n, 3), np.float32)
+    sf = np.zeros(9, np.float32)
+    lib.set_atoms(h, posf.ctypes.data, z16.ctypes.data, n)
+    lib.compute_dispersion_energy_from_handle_status(h, ef.ctypes.data, ff.ctypes.data, sf.ctypes.data)
+    for _ in range(max(1, args.warmup - 1)):
+        lib.set_atoms(h, posf.ctypes.data, z16.ctypes.data, n)
+        lib.compute_dispersion_energy_from_handle_status(h, ef.ctypes.data, ff.ctypes.data, sf.ctypes.data)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        lib.set_atoms(h, posf.ctypes.data, z16.ctypes.data, n)
+        st = lib.compute_dispersion_energy_from_handle_status(h, ef.ctypes.data, ff.ctypes.data, sf.ctypes.data)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    lib.free_d3_handle(h)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * n * args.steps / e2e_s, "unit": "atoms/s",
+           "h2d_bytes_per_step": 3 * n * 8 + n * 4, "d2h_bytes_per_step": (1 + 3 * n + 9) * 8 + 4,
+           "path": "set_atoms(float coords) + compute_dispersion_energy_from_handle_status, host buffers"}
+
+    # roofline of the dominant kernel (ATM triplets), FP64 pipe
+    triplets = int(counters[0]) // 2
+    atm_s = statistics.mean(atm_ms) * 1e-3
+    achieved = triplets * ATM_FLOP_PER_TRIPLET / atm_s / 1e12
+    peak = peak_probe(True)
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tfile):
+        traffic = json.load(open(tfile)).get("atm_fp64_bytes_per_launch")
+    roofline = {"bound": "fp64", "kernel": "k_atm (ATM triplets)", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": "measured FP64 FMA throughput of this GPU by d3_peak_probe (MEASURED_PEAKS.json has "
+                               "no FP64 figure)",
+                "algorithmic": "%d in-range triplets x %d FLOP per launch" % (triplets, ATM_FLOP_PER_TRIPLET)}
+    line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(n, "plain FP64"),
+            "roofline": roofline, "e2e": e2e, "gpu_launches": d.launches_per_eval() * args.steps, "clocks": clocks,
+            "passes_ms": {k: statistics.mean(p[k] for p in passes) for k in passes[0]},
+            "counters": {"atm_triplets": triplets, "twobody_ordered_pairs": int(counters[1]),
+                         "cn_ordered_pairs": int(counters[2])},
+            "energy_ev": energy}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = run_cpu_baseline(sys_)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    d.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def reference_arm(args, world, rank, local):
+    """The reference's own CUDA build (oracle/_ref/libd3_ref.so) through its C ABI."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_lib
+
+    import d3_systems as S
+
+    if not ref_lib.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libd3_ref.so is missing"}))
+        return
+    n = args.ref_atoms
+    sys_ = S.triclinic_box(n, seed=1)
+    # the reference's compute call is synchronous (src/d3.cu:201): wall clock around it
+    h = ref_lib.RefHandle(sys_["Z"], n, RC, RC_CN, RC_ATM, damping=1, functional=0)
+    h.set_system(sys_["pos"], sys_["Z"], sys_["cell"])
+    for _ in range(args.warmup):
+        h.compute()
+    times = []
+    sampler = ClockSampler(local)
+    sampler.start()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e, f, s, st = h.compute()
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    h.close()
+    sec = statistics.mean(times)
+    value = n / sec
+    sample = ("reference CUDA build (LASP-D3 sources, sm_100a, synthetic table) through "
+              "compute_dispersion_energy_from_handle_status on the same generator at %d atoms (cell scaled to "
+              "density); its cost per atom grows with N (all-pairs ATM), so this overstates its throughput at %d "
+              "atoms" % (n, N_ATOMS))
+    line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": workload_config(N_ATOMS, "reference CUDA build, bounded sample of %d atoms" % n),
+            "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": 1, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "clocks": clocks, "energy_ev": e}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--atoms", type=int, default=N_ATOMS)
+    ap.add_argument("--ref-atoms", type=int, default=2000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        reference_arm(args, world, rank, local)
+    else:
+        engine_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -125,6 +125,25 @@ int d3_set_functional_params(d3_handle_t *handle, double s6, double s8, double p
 uint16_t d3_compute_async(d3_handle_t *handle, void *cuda_stream);
 const double *d3_device_results(d3_handle_t *handle);
 
+/* Device time (ms, CUDA events on the evaluation's stream) of each pass of the last
+   evaluation: [0] wrap+bin, [1] CN + C6 weights, [2] two-body, [3] ATM list,
+   [4] ATM triplets, [5] chain rule, [6] finalize; returns the number written.
+   counters (may be NULL) receives 4 values: ATM in-range triplet visits (two per
+   triplet), two-body in-range ordered pairs, CN in-range ordered pairs, 0. */
+int d3_pass_times(d3_handle_t *handle, float *ms, int cap, uint64_t *counters);
+
+/* Number of kernels one evaluation launches. */
+int d3_launches_per_eval(d3_handle_t *handle);
+
+/* Self-check of the refined reciprocal square root, reciprocal and inverse cube
+   root used by the ATM kernel: max relative error against CUDA's double-precision
+   functions over [1e-12, 1e14], written to max_rel_err[3]. */
+int d3_selftest_math(double *max_rel_err);
+
+/* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the FP64 (fp64 = 1) or FP32
+   pipe of the current device: the denominator of the engine's roofline figures. */
+double d3_peak_probe(int fp64);
+
 /* Last error message of this thread ("" if none). */
 const char *d3_last_error(void);
 

@@ -245,6 +245,38 @@ const double *d3_device_results(d3_handle_t *handle) {
 
 const char *d3_last_error(void) { return g_last_error.c_str(); }
 
+int d3_pass_times(d3_handle_t *handle, float *ms, int cap, uint64_t *counters) {
+    if (!handle) return -1;
+    try {
+        return d3::engine_pass_times(H(handle)->engine, ms, cap, reinterpret_cast<unsigned long long *>(counters));
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int d3_launches_per_eval(d3_handle_t *handle) {
+    return handle ? d3::engine_launches_per_eval(H(handle)->engine) : -1;
+}
+
+double d3_peak_probe(int fp64) {
+    try {
+        return d3::engine_peak_probe(fp64);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return -1.0;
+    }
+}
+
+int d3_selftest_math(double *max_rel_err) {
+    try {
+        return d3::engine_selftest_math(max_rel_err);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
 int d3_debug_atom_arrays(d3_handle_t *handle, double *cn, double *dedcn, double *energy_atoms) {
     if (!handle) return 1;
     try {

@@ -98,6 +98,9 @@ struct KP {
     // outputs
     double *out; // [0]=E(eV), [1..3n]=F(eV/A), [3n+1..3n+9]=stress(eV/A^3)
     unsigned int *status;
+    // work counters: [0] ATM in-range visits (2 per triplet), [1] two-body in-range
+    // ordered pairs, [2] CN in-range ordered pairs
+    unsigned long long *counters;
 };
 
 __device__ __forceinline__ int floordiv(int a, int b) {
@@ -280,6 +283,7 @@ __global__ void k_cn(KP p) {
     const int4 si = p.shift[i];
     const double ri = p.rcov[(int)xi.w];
     double acc = 0.0;
+    unsigned int npair = 0;
     traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, bool act) {
         if (!act) return;
         if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
@@ -291,10 +295,15 @@ __global__ void k_cn(KP p) {
         if (d2 <= p.rcn2 && d2 > 0.0) {
             double dd;
             acc += cn_term(p, sqrt(d2), ri + p.rcov[(int)xj.w], &dd);
+            ++npair;
         }
     });
     acc = warp_sum(acc);
-    if ((threadIdx.x & 31) == 0) p.cn[i] = acc;
+    for (int o = 16; o > 0; o >>= 1) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+    if ((threadIdx.x & 31) == 0) {
+        p.cn[i] = acc;
+        atomicAdd(&p.counters[2], (unsigned long long)npair);
+    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -373,6 +382,7 @@ __global__ void k_twobody(KP p) {
     }
     const double rri = p.r2r4[ti];
     double e = 0, g = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+    unsigned int npair = 0;
     traverse(p, p.bin_s[i], p.st2, p.nst2, [&](int j, int Tx, int Ty, int Tz, bool act) {
         if (!act) return;
         if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
@@ -382,6 +392,7 @@ __global__ void k_twobody(KP p) {
         const double dx = xi.x - (xj.x + sx), dy = xi.y - (xj.y + sy), dz = xi.z - (xj.z + sz);
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (!(r2 < p.rc2 && r2 > 0.0)) return;
+        ++npair;
         const int tj = (int)xj.w;
         const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
         double c6 = 0.0, dc6 = 0.0;
@@ -439,7 +450,9 @@ __global__ void k_twobody(KP p) {
     vxy = warp_sum(vxy);
     vxz = warp_sum(vxz);
     vyz = warp_sum(vyz);
+    for (int o = 16; o > 0; o >>= 1) npair += __shfl_xor_sync(0xffffffffu, npair, o);
     if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&p.counters[1], (unsigned long long)npair);
         p.e2[i] = e;
         p.g2[i] = g;
         p.f2[3 * i] = fx;
@@ -506,244 +519,7 @@ __global__ void k_atm_list(KP p) {
 
 __device__ __forceinline__ int sext8(int v) { return (v << 24) >> 24; }
 
-// ------------------------------------------------------------------------------------
-// ATM triplets (src/d3_kernel.cu:1199-1509) over the half list of each apex.
-// Persistent CTAs take apexes from a work counter (largest lists first). A thread owns
-// one list entry x and visits every other entry y of the same apex (both orders of
-// each unordered pair), so every accumulation into x is thread-private; the apex's
-// share is halved per visit. Partner entries are staged through shared memory.
-// ------------------------------------------------------------------------------------
-struct Partner {
-    double vx, vy, vz, d2, r, s, lam, g;
-    int j, t, pad0, pad1;
-};
-
-constexpr int ATM_THREADS = 128;
-
-template <int NR>
-__global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
-    extern __shared__ double smem[];
-    const int ne = p.ne;
-    Partner *ptile = reinterpret_cast<Partner *>(smem);
-    double *ytile = reinterpret_cast<double *>(ptile + tile); // [tile][ne][NR]
-    double *yapex = ytile + (size_t)tile * ne * NR;           // [ne][NR] apex Y
-    double *r0s = yapex + ne * NR;                            // [ne][ne]
-    __shared__ int s_item;
-    __shared__ double red[ATM_THREADS / 32][12];
-    const int tid = threadIdx.x;
-    if (p.atm_off[p.n] > p.atm_cap) return; // list overflowed: the host grows it and re-runs
-    for (int k = tid; k < ne * ne; k += blockDim.x) r0s[k] = p.r0ab[k];
-    const double x16c = 4294967296.0 / 43046721.0; // (4/3)^16 = 4^16 / 3^16
-    const double third = 1.0 / 3.0;
-    while (true) {
-        __syncthreads();
-        if (tid == 0) s_item = atomicAdd(p.work, 1);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= p.n) break;
-        const int a = p.sorted_of[p.n - 1 - item];
-        const long long e0 = p.atm_off[a];
-        const int m = (int)(p.atm_off[a + 1] - e0);
-        const double4 xa = p.xs[a];
-        const int ta = (int)xa.w;
-        for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
-        double wa[NR], dwa[NR];
-#pragma unroll
-        for (int b = 0; b < NR; ++b) {
-            wa[b] = p.w[(size_t)a * NR + b];
-            dwa[b] = p.dw[(size_t)a * NR + b];
-        }
-        __syncthreads();
-        double ea = 0, ga = 0, fax = 0, fay = 0, faz = 0;
-        double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
-        for (int q0 = 0; q0 < m; q0 += blockDim.x) {
-            const int q = q0 + tid;
-            const bool active = q < m;
-            // own entry x
-            double vqx = 0, vqy = 0, vqz = 0, dq = 1, rq = 1, sq = 0, lam_qa = 0, lam_aq = 0, gq = 0;
-            double wq[NR], dwq[NR];
-            int jq = -1, tq = 0;
-            if (active) {
-                const int2 ent = p.atm_ent[e0 + q];
-                jq = ent.x;
-                const int Tx = sext8(ent.y & 0xff), Ty = sext8((ent.y >> 8) & 0xff), Tz = sext8((ent.y >> 16) & 0xff);
-                const double4 xj = p.xs[jq];
-                tq = (int)xj.w;
-                double sx, sy, sz;
-                image_vec(p, Tx, Ty, Tz, sx, sy, sz);
-                vqx = xj.x + sx - xa.x;
-                vqy = xj.y + sy - xa.y;
-                vqz = xj.z + sz - xa.z;
-                dq = vqx * vqx + vqy * vqy + vqz * vqz;
-                rq = sqrt(dq);
-#pragma unroll
-                for (int b = 0; b < NR; ++b) {
-                    wq[b] = p.w[(size_t)jq * NR + b];
-                    dwq[b] = p.dw[(size_t)jq * NR + b];
-                }
-                const double *ya = yapex + tq * NR;        // C6_aq = y_{a,tq} . w_q
-                const double *yq = p.Y + ((size_t)jq * ne + ta) * NR; // dC6/dCN_a = y_{q,ta} . dw_a
-                double c6 = 0, dca = 0, dcq = 0;
-#pragma unroll
-                for (int b = 0; b < NR; ++b) {
-                    c6 += ya[b] * wq[b];
-                    dcq += ya[b] * dwq[b];
-                    dca += yq[b] * dwa[b];
-                }
-                sq = sqrt(c6);
-                lam_aq = c6 > 0 ? dca / c6 : 0.0;
-                lam_qa = c6 > 0 ? dcq / c6 : 0.0;
-                gq = pow(r0s[ta * ne + tq] / rq, 16.0 * third);
-            } else {
-#pragma unroll
-                for (int b = 0; b < NR; ++b) wq[b] = dwq[b] = 0.0;
-            }
-            double eq = 0, gq_acc = 0, fqx = 0, fqy = 0, fqz = 0;
-            for (int p0 = 0; p0 < m; p0 += tile) {
-                const int cnt = min(tile, m - p0);
-                __syncthreads();
-                for (int k = tid; k < cnt; k += blockDim.x) {
-                    const int2 ent = p.atm_ent[e0 + p0 + k];
-                    const int jp = ent.x;
-                    const int Tx = sext8(ent.y & 0xff), Ty = sext8((ent.y >> 8) & 0xff), Tz = sext8((ent.y >> 16) & 0xff);
-                    const double4 xj = p.xs[jp];
-                    const int tp = (int)xj.w;
-                    double sx, sy, sz;
-                    image_vec(p, Tx, Ty, Tz, sx, sy, sz);
-                    Partner pr;
-                    pr.vx = xj.x + sx - xa.x;
-                    pr.vy = xj.y + sy - xa.y;
-                    pr.vz = xj.z + sz - xa.z;
-                    pr.d2 = pr.vx * pr.vx + pr.vy * pr.vy + pr.vz * pr.vz;
-                    pr.r = sqrt(pr.d2);
-                    const double *ya = yapex + tp * NR;
-                    const double *yp = p.Y + ((size_t)jp * ne + ta) * NR;
-                    double c6 = 0, dca = 0;
-#pragma unroll
-                    for (int b = 0; b < NR; ++b) {
-                        c6 += ya[b] * p.w[(size_t)jp * NR + b];
-                        dca += yp[b] * dwa[b];
-                    }
-                    pr.s = sqrt(c6);
-                    pr.lam = c6 > 0 ? dca / c6 : 0.0; // dlnC6_ap/dCN_a
-                    pr.g = pow(r0s[ta * ne + tp] / pr.r, 16.0 * third);
-                    pr.j = jp;
-                    pr.t = tp;
-                    ptile[k] = pr;
-                    for (int u = 0; u < ne * NR; ++u) ytile[(size_t)k * ne * NR + u] = p.Y[(size_t)jp * ne * NR + u];
-                }
-                __syncthreads();
-                if (!active) continue;
-                for (int k = 0; k < cnt; ++k) {
-                    if (p0 + k == q) continue;
-                    const Partner &pr = ptile[k];
-                    const double rx = vqx - pr.vx, ry = vqy - pr.vy, rz = vqz - pr.vz;
-                    const double d3 = rx * rx + ry * ry + rz * rz;
-                    if (d3 > p.ratm2 || d3 < 1e-12) continue;
-                    const double r3 = sqrt(d3);
-                    const double *yp = ytile + ((size_t)k * ne + tq) * NR; // C6_qp = y_{p,tq} . w_q
-                    double c6 = 0, dc6 = 0;
-#pragma unroll
-                    for (int b = 0; b < NR; ++b) {
-                        c6 += yp[b] * wq[b];
-                        dc6 += yp[b] * dwq[b];
-                    }
-                    const double s3 = sqrt(c6);
-                    const double lam_qp = c6 > 0 ? dc6 / c6 : 0.0;
-                    const double g3 = pow(r0s[tq * ne + pr.t] / r3, 16.0 * third);
-                    // weights (reference scale factors, src/d3_kernel.cu:1282-1290)
-                    const bool same = (jq == pr.j), qa = (jq == a), pa = (pr.j == a);
-                    double w, wf;
-                    if (same && qa) {
-                        w = 1.0 / 3.0;
-                        wf = 2.0;
-                    } else if (same) {
-                        w = 1.0;
-                        wf = 2.0;
-                    } else if (qa || pa) {
-                        w = 0.5;
-                        wf = 1.0;
-                    } else {
-                        w = 1.0;
-                        wf = 1.0;
-                    }
-                    if (p.atm_force_scaled) wf = w;
-                    const double d1 = dq, d2 = pr.d2;
-                    const double rsq = d1 * d2 * d3;
-                    const double rprod = rq * pr.r * r3;
-                    const double t1 = d1 + d2 - d3, t2 = d1 - d2 + d3, t3 = -d1 + d2 + d3;
-                    const double cosp = t1 * t2 * t3 / (8.0 * rsq);
-                    const double ir9 = 1.0 / (rsq * rprod);
-                    const double A = (1.0 + 3.0 * cosp) * ir9;
-                    const double dd = 0.375 * ir9 / rsq;
-                    const double dang1 = dd * (d1 * d1 * d1 + d1 * d1 * (d2 + d3) + d1 * (3.0 * d3 * d3 + 2.0 * d3 * d2 + 3.0 * d2 * d2) -
-                                               5.0 * (d3 - d2) * (d3 - d2) * (d3 + d2));
-                    const double dang2 = dd * (d2 * d2 * d2 + d2 * d2 * (d3 + d1) + d2 * (3.0 * d3 * d3 + 2.0 * d3 * d1 + 3.0 * d1 * d1) -
-                                               5.0 * (d3 - d1) * (d3 - d1) * (d3 + d1));
-                    const double dang3 = dd * (d3 * d3 * d3 + d3 * d3 * (d2 + d1) + d3 * (3.0 * d2 * d2 + 2.0 * d2 * d1 + 3.0 * d1 * d1) -
-                                               5.0 * (d2 - d1) * (d2 - d1) * (d2 + d1));
-                    const double x16 = x16c * gq * pr.g * g3;
-                    const double fd = 1.0 / (1.0 + 6.0 * x16);
-                    const double dfd = 32.0 * x16 * fd * fd;
-                    const double C9 = -sq * pr.s * s3;
-                    const double Et = C9 * A * fd;
-                    const double f1 = -C9 * (dang1 * fd - A * dfd) / d1;
-                    const double f2 = -C9 * (dang2 * fd - A * dfd) / d2;
-                    const double f3 = -C9 * (dang3 * fd - A * dfd) / d3;
-                    // own entry (atom x): energy share, dE/dCN_x, force on x
-                    eq += w * Et * third;
-                    gq_acc += w * 0.5 * Et * (lam_qa + lam_qp);
-                    fqx += wf * (f1 * vqx + f3 * rx);
-                    fqy += wf * (f1 * vqy + f3 * ry);
-                    fqz += wf * (f1 * vqz + f3 * rz);
-                    // apex share, halved (each unordered pair is visited twice)
-                    const double wh = 0.5 * w, wfh = 0.5 * wf;
-                    ea += wh * Et * third;
-                    ga += wh * 0.5 * Et * (lam_aq + pr.lam);
-                    fax -= wfh * (f1 * vqx + f2 * pr.vx);
-                    fay -= wfh * (f1 * vqy + f2 * pr.vy);
-                    faz -= wfh * (f1 * vqz + f2 * pr.vz);
-                    vxx += wh * (f1 * vqx * vqx + f2 * pr.vx * pr.vx + f3 * rx * rx);
-                    vyy += wh * (f1 * vqy * vqy + f2 * pr.vy * pr.vy + f3 * ry * ry);
-                    vzz += wh * (f1 * vqz * vqz + f2 * pr.vz * pr.vz + f3 * rz * rz);
-                    vxy += wh * (f1 * vqx * vqy + f2 * pr.vx * pr.vy + f3 * rx * ry);
-                    vxz += wh * (f1 * vqx * vqz + f2 * pr.vx * pr.vz + f3 * rx * rz);
-                    vyz += wh * (f1 * vqy * vqz + f2 * pr.vy * pr.vz + f3 * ry * rz);
-                }
-            }
-            if (active) {
-                atomicAdd(&p.eb[jq], eq);
-                atomicAdd(&p.gb[jq], gq_acc);
-                atomicAdd(&p.fb[3 * jq], fqx);
-                atomicAdd(&p.fb[3 * jq + 1], fqy);
-                atomicAdd(&p.fb[3 * jq + 2], fqz);
-            }
-        }
-        // apex reduction over the CTA (fixed order)
-        double vals[11] = {ea, ga, fax, fay, faz, vxx, vyy, vzz, vxy, vxz, vyz};
-        const int lane = tid & 31, wid = tid >> 5;
-#pragma unroll
-        for (int k = 0; k < 11; ++k) {
-            const double v = warp_sum(vals[k]);
-            if (lane == 0) red[wid][k] = v;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double tot[11];
-            for (int k = 0; k < 11; ++k) {
-                tot[k] = 0;
-                for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) tot[k] += red[w2][k];
-            }
-            p.ea[a] = tot[0];
-            p.ga[a] = tot[1];
-            p.fa[3 * a] = tot[2];
-            p.fa[3 * a + 1] = tot[3];
-            p.fa[3 * a + 2] = tot[4];
-            const double sc = -1.0 / p.vol;
-            for (int k = 0; k < 6; ++k) p.va[6 * (size_t)a + k] = tot[5 + k] * sc;
-        }
-    }
-}
+#include "d3_atm.cuh"
 
 // ------------------------------------------------------------------------------------
 // chain rule (src/d3_kernel.cu:1511-1698): F_i += (dE/dCN_i + dE/dCN_j) dCN_ij/dr r_hat
@@ -911,7 +687,13 @@ struct Engine {
     DBuf<int4> st_dev;
     DBuf<double> out;
     DBuf<unsigned int> status;
+    DBuf<unsigned long long> counters;
     std::vector<double> host_out;
+    // pass boundaries of the last evaluation: bin | cn+weights | two-body | atm list |
+    // atm | chain | finalize
+    static constexpr int NEV = 8;
+    cudaEvent_t ev[NEV] = {};
+    bool have_events = false;
 
     ~Engine() {
         DBuf<double> *ds[] = {&t_cnref, &t_c6, &t_r0, &t_rcov, &t_r2r4, &t_pairA, &pos_in, &cn, &w, &dw, &Y, &e2,
@@ -928,6 +710,9 @@ struct Engine {
         atm_ent.release();
         st_dev.release();
         status.release();
+        counters.release();
+        for (auto &x : ev)
+            if (x) cudaEventDestroy(x);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -1105,6 +890,8 @@ Engine *engine_create(const uint16_t *elements, uint64_t n_elements, uint64_t ma
         e->work.ensure(1);
         e->out.ensure(1 + 3 * N + 9);
         e->status.ensure(1);
+        e->counters.ensure(4);
+        for (auto &x : e->ev) D3_CUDA(cudaEventCreate(&x));
         e->host_out.resize(1 + 3 * N + 9);
         return e;
     } catch (const std::exception &ex) {
@@ -1265,6 +1052,7 @@ static KP make_kp(Engine *e) {
     p.nsta = (int)e->sta.size();
     p.out = e->out.p;
     p.status = e->status.p;
+    p.counters = e->counters.p;
     return p;
 }
 
@@ -1275,6 +1063,9 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     const int T = 256;
     const int gb = (n + T - 1) / T;
     const int gw = (int)(((long long)n * 32 + T - 1) / T);
+    cudaEvent_t *ev = e->ev;
+    D3_CUDA(cudaEventRecord(ev[0], s));
+    D3_CUDA(cudaMemsetAsync(p.counters, 0, sizeof(unsigned long long) * 4, s));
     D3_CUDA(cudaMemsetAsync(p.bin_cnt, 0, sizeof(int) * p.nbins, s));
     D3_CUDA(cudaMemsetAsync(p.bin_fill, 0, sizeof(int) * p.nbins, s));
     k_bin<<<gb, T, 0, s>>>(p);
@@ -1282,9 +1073,12 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     k_scatter<<<gb, T, 0, s>>>(p);
     k_binsort<<<(p.nbins + T - 1) / T, T, 0, s>>>(p);
     k_gather<<<gb, T, 0, s>>>(p);
+    D3_CUDA(cudaEventRecord(ev[1], s));
     k_cn<<<gw, T, 0, s>>>(p);
     k_weights<NR><<<gb, T, 0, s>>>(p);
+    D3_CUDA(cudaEventRecord(ev[2], s));
     k_twobody<NR><<<gw, T, 0, s>>>(p);
+    D3_CUDA(cudaEventRecord(ev[3], s));
     D3_CUDA(cudaMemsetAsync(p.ea, 0, sizeof(double) * n, s));
     D3_CUDA(cudaMemsetAsync(p.ga, 0, sizeof(double) * n, s));
     D3_CUDA(cudaMemsetAsync(p.fa, 0, sizeof(double) * 3 * n, s));
@@ -1296,6 +1090,9 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
         k_atm_list<false><<<gw, T, 0, s>>>(p);
         k_scan<long long, int><<<1, 1024, 0, s>>>(p.atm_cnt, p.atm_off, n);
         k_atm_list<true><<<gw, T, 0, s>>>(p);
+    }
+    D3_CUDA(cudaEventRecord(ev[4], s));
+    if (e->use_atm) {
         D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
         // partner tile: as many entries as fit in ~160 KB next to the apex tables
         const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double);
@@ -1308,11 +1105,109 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
         const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, blocks_per_sm)));
         k_atm<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
     }
+    D3_CUDA(cudaEventRecord(ev[5], s));
     k_sum_g<<<gb, T, 0, s>>>(p, e->G.p);
     k_chain<<<gw, T, 0, s>>>(p, e->G.p);
+    D3_CUDA(cudaEventRecord(ev[6], s));
     k_forces_out<<<gb, T, 0, s>>>(p);
     k_reduce<<<1, 1024, 0, s>>>(p);
+    D3_CUDA(cudaEventRecord(ev[7], s));
+    e->have_events = true;
     D3_CUDA(cudaGetLastError());
+}
+
+int engine_pass_times(Engine *e, float *ms, int cap, unsigned long long *counters) {
+    if (!e->have_events) return 0;
+    D3_CUDA(cudaEventSynchronize(e->ev[Engine::NEV - 1]));
+    int k = 0;
+    for (; k < Engine::NEV - 1 && k < cap; ++k) D3_CUDA(cudaEventElapsedTime(&ms[k], e->ev[k], e->ev[k + 1]));
+    if (counters) D3_CUDA(cudaMemcpy(counters, e->counters.p, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost));
+    return k;
+}
+
+int engine_launches_per_eval(const Engine *e) { return e->use_atm ? 16 : 12; }
+
+// Accuracy check of the Newton-refined helpers used by the ATM kernel against CUDA's
+// double-precision 1/sqrt, 1/x and cbrt over log-spaced inputs in [1e-12, 1e14].
+__global__ void k_selftest_math(double *err, int m) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const double x = exp(log(1e-12) + (log(1e14) - log(1e-12)) * (double)i / (double)(m - 1));
+    const double e0 = fabs(rsqrt_nr(x) * sqrt(x) - 1.0);
+    const double e1 = fabs(rcp_nr(x) * x - 1.0);
+    const double c = cbrt(x);
+    const double e2 = fabs(rcbrt_nr(x) * c - 1.0);
+    err[3 * i] = e0;
+    err[3 * i + 1] = e1;
+    err[3 * i + 2] = e2;
+}
+
+// FMA throughput probe: 8 independent FMA chains per thread, enough blocks to fill the
+// GPU; the result is written so the chains are not removed. Used to measure the FP64 and
+// FP32 pipe peaks the roofline is reported against.
+template <typename T>
+__global__ void k_fma_probe(T *out, int iters, T a, T b) {
+    T x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            x0 = fma(x0, a, b);
+            x1 = fma(x1, a, b);
+            x2 = fma(x2, a, b);
+            x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b);
+            x5 = fma(x5, a, b);
+            x6 = fma(x6, a, b);
+            x7 = fma(x7, a, b);
+        }
+    }
+    const T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == (T)-1.2345) out[blockIdx.x] = s;
+}
+
+double engine_peak_probe(int fp64) {
+    int dev = 0, sms = 148;
+    D3_CUDA(cudaGetDevice(&dev));
+    D3_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    void *out = nullptr;
+    D3_CUDA(cudaMalloc(&out, 8 * 65536));
+    cudaEvent_t a, b;
+    D3_CUDA(cudaEventCreate(&a));
+    D3_CUDA(cudaEventCreate(&b));
+    const int blocks = sms * 8, threads = 256, iters = fp64 ? 2048 : 4096;
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        D3_CUDA(cudaEventRecord(a));
+        if (fp64)
+            k_fma_probe<double><<<blocks, threads>>>((double *)out, iters, 0.999999, 1e-7);
+        else
+            k_fma_probe<float><<<blocks, threads>>>((float *)out, iters, 0.999999f, 1e-7f);
+        D3_CUDA(cudaEventRecord(b));
+        D3_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        D3_CUDA(cudaEventElapsedTime(&ms, a, b));
+        if (rep > 0) best = std::min(best, ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    const double flops = 2.0 * 8.0 * 16.0 * iters * (double)blocks * threads;
+    return flops / (best * 1e-3) / 1e12; // TFLOP/s
+}
+
+int engine_selftest_math(double max_rel[3]) {
+    const int m = 1 << 16;
+    double *d = nullptr;
+    D3_CUDA(cudaMalloc(&d, sizeof(double) * 3 * m));
+    k_selftest_math<<<(m + 255) / 256, 256>>>(d, m);
+    std::vector<double> h(3 * (size_t)m);
+    cudaError_t err = cudaMemcpy(h.data(), d, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    D3_CUDA(err);
+    for (int k = 0; k < 3; ++k) max_rel[k] = 0;
+    for (int i = 0; i < m; ++i)
+        for (int k = 0; k < 3; ++k) max_rel[k] = std::max(max_rel[k], h[3 * (size_t)i + k]);
+    return 0;
 }
 
 uint16_t engine_compute(Engine *e, double *energy, double *forces, double *stress, cudaStream_t stream, bool sync) {

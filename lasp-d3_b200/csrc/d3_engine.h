@@ -63,6 +63,16 @@ uint16_t engine_compute(Engine *e, double *energy_ev, double *forces_ev_a, doubl
 const double *engine_device_results(const Engine *e); // [1 + 3n + 9]
 uint64_t engine_num_atoms(const Engine *e);
 
+// per-pass device times (ms) of the last evaluation, from CUDA events on its stream:
+// [bin, cn+weights, two-body, atm-list, atm, chain, finalize]; work counters
+// [atm in-range visits, two-body ordered pairs, cn ordered pairs, 0]
+int engine_pass_times(Engine *e, float *ms, int cap, unsigned long long *counters);
+int engine_launches_per_eval(const Engine *e);
+// max relative error of the ATM kernel's refined rsqrt / reciprocal / inverse cube root
+int engine_selftest_math(double max_rel[3]);
+// measured FMA throughput of the FP64 (fp64 = 1) or FP32 pipe, TFLOP/s
+double engine_peak_probe(int fp64);
+
 // diagnostics for tests: coordination numbers, dE/dCN, per-atom energies (hartree),
 // in the caller's atom order; ATM list (caller indices and reference lattice shifts)
 int engine_debug_atom_arrays(Engine *e, double *cn, double *dedcn, double *energy_atoms);

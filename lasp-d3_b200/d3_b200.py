@@ -71,6 +71,14 @@ def load_library(path=None):
     lib.d3_compute_async.argtypes = [vp, vp]
     lib.d3_device_results.restype = vp
     lib.d3_device_results.argtypes = [vp]
+    lib.d3_pass_times.restype = ctypes.c_int
+    lib.d3_pass_times.argtypes = [vp, vp, ctypes.c_int, vp]
+    lib.d3_launches_per_eval.restype = ctypes.c_int
+    lib.d3_launches_per_eval.argtypes = [vp]
+    lib.d3_peak_probe.restype = ctypes.c_double
+    lib.d3_peak_probe.argtypes = [ctypes.c_int]
+    lib.d3_selftest_math.restype = ctypes.c_int
+    lib.d3_selftest_math.argtypes = [vp]
     lib.d3_last_error.restype = ctypes.c_char_p
     lib.d3_last_error.argtypes = []
     lib.d3_debug_atom_arrays.restype = ctypes.c_int
@@ -89,6 +97,20 @@ def declared_symbols(header=HEADER):
     txt = open(header).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
     return sorted(set(re.findall(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", txt)) - {"if", "sizeof", "defined"})
+
+
+def selftest_math():
+    """Max relative errors of the ATM kernel's refined rsqrt, reciprocal, rcbrt."""
+    lib = load_library()
+    e = np.zeros(3)
+    if lib.d3_selftest_math(_ptr(e)):
+        raise RuntimeError(lib.d3_last_error().decode())
+    return e
+
+
+def peak_probe(fp64=True):
+    """Measured FMA throughput of the FP64 / FP32 pipe (TFLOP/s)."""
+    return float(load_library().d3_peak_probe(1 if fp64 else 0))
 
 
 def _ptr(a):
@@ -137,6 +159,24 @@ class D3:
         if check and st != 0:
             raise RuntimeError("d3_compute_f64 status %d: %s" % (st, self.lib.d3_last_error().decode()))
         return float(e[0]), f, s.reshape(3, 3)
+
+    def pass_times(self):
+        """Device ms per pass of the last evaluation and the work counters."""
+        ms = np.zeros(8, np.float32)
+        cnt = np.zeros(4, np.uint64)
+        k = self.lib.d3_pass_times(self.h, _ptr(ms), 8, _ptr(cnt))
+        names = ["bin", "cn", "twobody", "atm_list", "atm", "chain", "finalize"]
+        return dict(zip(names, ms[:k].tolist())), cnt
+
+    def launches_per_eval(self):
+        return int(self.lib.d3_launches_per_eval(self.h))
+
+    def compute_async(self, stream_ptr=None):
+        """Enqueue one evaluation on a CUDA stream (int handle or None); no host sync."""
+        return int(self.lib.d3_compute_async(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def device_results_ptr(self):
+        return self.lib.d3_device_results(self.h)
 
     def atom_arrays(self):
         cn, g, e = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
