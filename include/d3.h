@@ -137,7 +137,8 @@ int d3_launches_per_eval(d3_handle_t *handle);
 
 /* Self-check of the refined reciprocal square root, reciprocal and inverse cube
    root used by the ATM kernel: max relative error against CUDA's double-precision
-   functions over [1e-12, 1e14], written to max_rel_err[3]. */
+   functions over [1e-12, 1e14], written to max_rel_err[6] (one Newton step:
+   rsqrt, rcp, rcbrt; two Newton steps: rsqrt, rcp, rcbrt). */
 int d3_selftest_math(double *max_rel_err);
 
 /* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of the FP64 (fp64 = 1) or FP32

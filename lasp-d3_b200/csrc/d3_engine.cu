@@ -1095,7 +1095,8 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     if (e->use_atm) {
         D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
         // partner tile: as many entries as fit in ~160 KB next to the apex tables
-        const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double);
+        const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double) +
+                             ATM_PERM_CAP * sizeof(unsigned short);
         const size_t per = sizeof(Partner) + (size_t)p.ne * NR * sizeof(double);
         const int tile = (int)std::max<size_t>(8, std::min<size_t>(128, (160 * 1024 - fixed) / per));
         const size_t sm = (size_t)tile * per + fixed;
@@ -1133,13 +1134,13 @@ __global__ void k_selftest_math(double *err, int m) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
     const double x = exp(log(1e-12) + (log(1e14) - log(1e-12)) * (double)i / (double)(m - 1));
-    const double e0 = fabs(rsqrt_nr(x) * sqrt(x) - 1.0);
-    const double e1 = fabs(rcp_nr(x) * x - 1.0);
-    const double c = cbrt(x);
-    const double e2 = fabs(rcbrt_nr(x) * c - 1.0);
-    err[3 * i] = e0;
-    err[3 * i + 1] = e1;
-    err[3 * i + 2] = e2;
+    const double sq = sqrt(x), c = cbrt(x);
+    err[6 * i + 0] = fabs(rsqrt_nr(x) * sq - 1.0);
+    err[6 * i + 1] = fabs(rcp_nr(x) * x - 1.0);
+    err[6 * i + 2] = fabs(rcbrt_nr(x) * c - 1.0);
+    err[6 * i + 3] = fabs(rsqrt_nr2(x) * sq - 1.0);
+    err[6 * i + 4] = fabs(rcp_nr2(x) * x - 1.0);
+    err[6 * i + 5] = fabs(rcbrt_nr2(x) * c - 1.0);
 }
 
 // FMA throughput probe: 8 independent FMA chains per thread, enough blocks to fill the
@@ -1195,18 +1196,18 @@ double engine_peak_probe(int fp64) {
     return flops / (best * 1e-3) / 1e12; // TFLOP/s
 }
 
-int engine_selftest_math(double max_rel[3]) {
+int engine_selftest_math(double max_rel[6]) {
     const int m = 1 << 16;
     double *d = nullptr;
-    D3_CUDA(cudaMalloc(&d, sizeof(double) * 3 * m));
+    D3_CUDA(cudaMalloc(&d, sizeof(double) * 6 * m));
     k_selftest_math<<<(m + 255) / 256, 256>>>(d, m);
-    std::vector<double> h(3 * (size_t)m);
-    cudaError_t err = cudaMemcpy(h.data(), d, sizeof(double) * 3 * m, cudaMemcpyDeviceToHost);
+    std::vector<double> h(6 * (size_t)m);
+    cudaError_t err = cudaMemcpy(h.data(), d, sizeof(double) * 6 * m, cudaMemcpyDeviceToHost);
     cudaFree(d);
     D3_CUDA(err);
-    for (int k = 0; k < 3; ++k) max_rel[k] = 0;
+    for (int k = 0; k < 6; ++k) max_rel[k] = 0;
     for (int i = 0; i < m; ++i)
-        for (int k = 0; k < 3; ++k) max_rel[k] = std::max(max_rel[k], h[3 * (size_t)i + k]);
+        for (int k = 0; k < 6; ++k) max_rel[k] = std::max(max_rel[k], h[6 * (size_t)i + k]);
     return 0;
 }
 

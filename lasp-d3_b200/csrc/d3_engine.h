@@ -68,8 +68,9 @@ uint64_t engine_num_atoms(const Engine *e);
 // [atm in-range visits, two-body ordered pairs, cn ordered pairs, 0]
 int engine_pass_times(Engine *e, float *ms, int cap, unsigned long long *counters);
 int engine_launches_per_eval(const Engine *e);
-// max relative error of the ATM kernel's refined rsqrt / reciprocal / inverse cube root
-int engine_selftest_math(double max_rel[3]);
+// max relative error of the ATM kernel's refined rsqrt / reciprocal / inverse cube root:
+// [one Newton step x3, two Newton steps x3]
+int engine_selftest_math(double max_rel[6]);
 // measured FMA throughput of the FP64 (fp64 = 1) or FP32 pipe, TFLOP/s
 double engine_peak_probe(int fp64);
 

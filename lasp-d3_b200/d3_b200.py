@@ -100,9 +100,10 @@ def declared_symbols(header=HEADER):
 
 
 def selftest_math():
-    """Max relative errors of the ATM kernel's refined rsqrt, reciprocal, rcbrt."""
+    """Max relative errors of the ATM kernel's refined rsqrt, reciprocal, rcbrt
+    (one Newton step, then two Newton steps)."""
     lib = load_library()
-    e = np.zeros(3)
+    e = np.zeros(6)
     if lib.d3_selftest_math(_ptr(e)):
         raise RuntimeError(lib.d3_last_error().decode())
     return e
