@@ -145,6 +145,25 @@ int d3_selftest_math(double *max_rel_err);
    pipe of the current device: the denominator of the engine's roofline figures. */
 double d3_peak_probe(int fp64);
 
+/* Coordination numbers of one periodic structure without any device allocation (no
+   counterpart in the reference). For callers that must not allocate device memory
+   where they call the library -- e.g. an MD-engine plugin inside its time-step loop,
+   where cudaMalloc would synchronise the device, or an application whose memory is all
+   owned by its own pool allocator. Inputs and outputs are caller-owned device buffers:
+   coords [n][3] (double, Angstrom), elements [n] (atomic numbers), cn [n] (double,
+   written). cell is a host array (Angstrom, rows = lattice vectors), cn_cutoff in bohr,
+   table D3_TABLE_5REF or D3_TABLE_7REF. Work is enqueued on cuda_stream (NULL = the
+   default stream) with no host synchronisation. At most D3_NOALLOC_MAX_ATOMS atoms:
+   larger sizes are rejected with an error (return 1, see d3_last_error). The only
+   scratch is a fixed array in device memory shared by all calls on a device (held until
+   the process exits): calls that overlap on the GPU race on it. The first call on each
+   device does a one-time set-up and should come before any stream capture. Returns 0
+   on success. Atoms whose element is outside the table get CN = NaN. */
+#define D3_NOALLOC_MAX_ATOMS 8192
+int d3_coordination_numbers_noalloc(const double *coords, const uint16_t *elements, uint64_t num_atoms,
+                                    const double cell[9], double cn_cutoff, int table, double *cn,
+                                    void *cuda_stream);
+
 /* Last error message of this thread ("" if none). */
 const char *d3_last_error(void);
 

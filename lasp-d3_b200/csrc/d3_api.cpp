@@ -68,6 +68,11 @@ uint16_t compute_float(Handle *h, real_t *energy, real_t *force, real_t *stress)
 
 } // namespace
 
+namespace d3 {
+// lets other translation units of the library report through d3_last_error()
+void record_error(const std::string &msg) { g_last_error = msg; }
+} // namespace d3
+
 extern "C" {
 
 d3_handle_t *init_d3_handle(uint16_t *elements, uint64_t num_elements, uint64_t max_length, real_t cutoff_radius,
