@@ -137,45 +137,18 @@ def run_cpu_baseline(sys_, sample=48, seed=7):
                       "atoms/s = 1 / (t_sample/%d + t_cn/%d)" % (n, t_cn, sample, t_sub, sample, n)}
 
 
-def engine_arm(args, world, rank, local):
+def time_form(d, args, flush, stream, barrier):
+    """Warm-up and K timed evaluations of one engine handle on `stream` (device time by
+    CUDA events, L2 flushed between steps). Returns per-step ms, ATM ms, passes, counters."""
     import torch
-
-    import d3_systems as S
-    from d3_b200 import D3, peak_probe
-
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
-    n = args.atoms
-    sys_ = S.triclinic_box(n, seed=1 + rank)
-    d = D3(sys_["Z"], n, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
-    d.set_cell(sys_["cell"])
-    d.set_atoms(sys_["pos"], sys_["Z"])
-    energy, forces, stress = d.compute()  # sizes the ATM list
-    stream = torch.cuda.Stream()
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
-        torch.cuda.synchronize()
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             flush.zero_()
             d.compute_async(stream.cuda_stream)
     barrier()
-    sampler = ClockSampler(local)
-    sampler.start()
     step_ms, atm_ms, passes = [], [], []
     counters = None
-    barrier()
     with torch.cuda.stream(stream):
         for _ in range(args.steps):
             flush.zero_()
@@ -192,80 +165,140 @@ def engine_arm(args, world, rank, local):
             passes.append(pt)
             atm_ms.append(pt["atm"])
     barrier()
-    clocks = sampler.stop()
-    total_ms = float(sum(step_ms))
+    return step_ms, atm_ms, passes, counters
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def engine_arm(args, world, rank, local):
+    import torch
+
+    import d3_systems as S
+    from d3_b200 import D3, OPT_PRECISION, peak_probe
+
+    torch.cuda.set_device(local)
     if world > 1:
+        import datetime
+
         import torch.distributed as dist
 
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    ms_per_step = total_ms / args.steps
-    value = world * n / (ms_per_step * 1e-3)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    n = args.atoms
+    sys_ = S.triclinic_box(n, seed=1 + rank)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    forms = {}
+    sampler = ClockSampler(local)
+    sampler.start()
+    for form, prec in (("plain", 0), ("precision", 1)):
+        d = D3(sys_["Z"], n, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
+        d.set_option(OPT_PRECISION, prec)
+        d.set_cell(sys_["cell"])
+        d.set_atoms(sys_["pos"], sys_["Z"])
+        energy, forces, stress = d.compute()  # sizes the ATM list; result checked below
+        step_ms, atm_ms, passes, counters = time_form(d, args, flush, stream, barrier)
+        total_ms = max_over_ranks(float(sum(step_ms)), world)
+        ms_per_step = total_ms / args.steps
+        forms[form] = {"value": world * n / (ms_per_step * 1e-3), "ms_per_step": ms_per_step,
+                       "atm_ms": statistics.mean(atm_ms), "counters": counters,
+                       "passes_ms": {k: statistics.mean(p[k] for p in passes) for k in passes[0]},
+                       "energy": energy, "forces": forces, "stress": stress,
+                       "launches": d.launches_per_eval()}
+        d.close()
+    clocks = sampler.stop()
+    ref = forms["plain"]
+    prec = forms["precision"]
+    err = {"energy_rel": abs(prec["energy"] - ref["energy"]) / abs(ref["energy"]),
+           "force_max_ev_per_a": float(np.abs(prec["forces"] - ref["forces"]).max()),
+           "force_rms_ev_per_a": float(np.sqrt(np.mean((prec["forces"] - ref["forces"]) ** 2))),
+           "stress_max_ev_per_a3": float(np.abs(prec["stress"] - ref["stress"]).max()),
+           "against": "the FP64 plain form on the same input (which matches the FP64 oracle to 1e-9 relative)"}
+    meets = err["energy_rel"] <= 1e-6 and err["force_max_ev_per_a"] <= 1e-4
+    chosen = "precision" if meets else "plain"
+    ch = forms[chosen]
 
     # end to end through the reference-facing C ABI: float host buffers in, float out,
-    # host<->device copies inside the timed region
-    import ctypes
+    # host<->device copies inside the timed region, in the chosen form
+    from d3_b200 import load_library
 
-    lib = d.lib
+    lib = load_library()
     z16 = np.ascontiguousarray(sys_["Z"], np.uint16)
     posf = np.ascontiguousarray(sys_["pos"], np.float32)
     cellf = np.ascontiguousarray(sys_["cell"], np.float32)
     h = lib.init_d3_handle_with_atm(z16.ctypes.data, n, n, RC, RC_CN, RC_ATM, 1, 0)
+    lib.d3_set_option(h, OPT_PRECISION, 1 if chosen == "precision" else 0)
     lib.set_cell(h, cellf.ctypes.data)
     ef = np.zeros(1, np.float32)
     ff = np.zeros((n, 3), np.float32)
     sf = np.zeros(9, np.float32)
-    lib.set_atoms(h, posf.ctypes.data, z16.ctypes.data, n)
-    lib.compute_dispersion_energy_from_handle_status(h, ef.ctypes.data, ff.ctypes.data, sf.ctypes.data)
-    for _ in range(max(1, args.warmup - 1)):
+    for _ in range(max(1, args.warmup)):
         lib.set_atoms(h, posf.ctypes.data, z16.ctypes.data, n)
         lib.compute_dispersion_energy_from_handle_status(h, ef.ctypes.data, ff.ctypes.data, sf.ctypes.data)
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         lib.set_atoms(h, posf.ctypes.data, z16.ctypes.data, n)
-        st = lib.compute_dispersion_energy_from_handle_status(h, ef.ctypes.data, ff.ctypes.data, sf.ctypes.data)
+        lib.compute_dispersion_energy_from_handle_status(h, ef.ctypes.data, ff.ctypes.data, sf.ctypes.data)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     lib.free_d3_handle(h)
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
     e2e = {"value": world * n * args.steps / e2e_s, "unit": "atoms/s",
            "h2d_bytes_per_step": 3 * n * 8 + n * 4, "d2h_bytes_per_step": (1 + 3 * n + 9) * 8 + 4,
-           "path": "set_atoms(float coords) + compute_dispersion_energy_from_handle_status, host buffers"}
+           "path": "set_atoms(float coords) + compute_dispersion_energy_from_handle_status, host buffers, %s form"
+                   % chosen}
 
-    # roofline of the dominant kernel (ATM triplets), FP64 pipe
-    triplets = int(counters[0]) // 2
-    atm_s = statistics.mean(atm_ms) * 1e-3
+    # roofline of the dominant kernel (ATM triplets) of the chosen form
+    triplets = int(ch["counters"][0]) // 2
+    atm_s = ch["atm_ms"] * 1e-3
     achieved = triplets * ATM_FLOP_PER_TRIPLET / atm_s / 1e12
-    peak = peak_probe(True)
+    fp64 = chosen == "plain"
+    peak = peak_probe(fp64)
     traffic = None
     tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     if os.path.exists(tfile):
-        traffic = json.load(open(tfile)).get("atm_fp64_bytes_per_launch")
-    roofline = {"bound": "fp64", "kernel": "k_atm (ATM triplets)", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
-                "peak_source": "measured FP64 FMA throughput of this GPU by d3_peak_probe (MEASURED_PEAKS.json has "
-                               "no FP64 figure)",
+        traffic = json.load(open(tfile)).get("atm_fp64_bytes_per_launch" if fp64 else "atm_fp32_bytes_per_launch")
+    roofline = {"bound": "fp64" if fp64 else "fp32",
+                "kernel": "k_atm (ATM triplets, FP64)" if fp64 else "k_atm32 (ATM triplets, FP32 arithmetic)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": "measured %s FMA throughput of this GPU by d3_peak_probe (MEASURED_PEAKS.json has no "
+                               "FP64/FP32 figure)" % ("FP64" if fp64 else "FP32"),
                 "algorithmic": "%d in-range triplets x %d FLOP per launch" % (triplets, ATM_FLOP_PER_TRIPLET)}
-    line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(n, "plain FP64"),
-            "roofline": roofline, "e2e": e2e, "gpu_launches": d.launches_per_eval() * args.steps, "clocks": clocks,
-            "passes_ms": {k: statistics.mean(p[k] for p in passes) for k in passes[0]},
-            "counters": {"atm_triplets": triplets, "twobody_ordered_pairs": int(counters[1]),
-                         "cn_ordered_pairs": int(counters[2])},
-            "energy_ev": energy}
+    forms_out = {}
+    for k, f in forms.items():
+        forms_out[k] = {"value": f["value"], "unit": "atoms/s", "ms_per_step": f["ms_per_step"],
+                        "passes_ms": f["passes_ms"], "energy_ev": f["energy"]}
+    forms_out["precision"]["error_vs_fp64"] = err
+    line = {"metric": METRIC, "value": ch["value"], "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ch["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if fp64 else "f32", "data": "synthetic",
+            "config": workload_config(n, "%s form (%s)" % (chosen, "FP64 throughout" if fp64 else
+                                                         "FP32 pair/triplet arithmetic, FP64 C6 weights, dE/dCN "
+                                                         "and reductions")),
+            "chosen_form": chosen, "forms": forms_out,
+            "roofline": roofline, "e2e": e2e, "gpu_launches": ch["launches"] * args.steps, "clocks": clocks,
+            "counters": {"atm_triplets": triplets, "twobody_ordered_pairs": int(ch["counters"][1]),
+                         "cn_ordered_pairs": int(ch["counters"][2])}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = run_cpu_baseline(sys_)
     if rank == 0:
         print(json.dumps(line), flush=True)
-    d.close()
     if world > 1:
         import torch.distributed as dist
 

@@ -109,7 +109,10 @@ uint16_t d3_compute_f64(d3_handle_t *handle, double *energy, double *force, doub
 enum {
     D3_OPT_ATM_FORCE_SCALED = 1, /* 1: apply the 1/2, 1/6 repeated-index ATM factors to forces too
                                     (forces = -dE/dx); 0 (default): reference convention */
-    D3_OPT_SMOOTH_CN = 2         /* tanh^3 CN cutoff (reference compile-time SMOOTH_CUTOFF_CN) */
+    D3_OPT_SMOOTH_CN = 2,        /* tanh^3 CN cutoff (reference compile-time SMOOTH_CUTOFF_CN) */
+    D3_OPT_PRECISION = 3         /* 0 (default): FP64 throughout (plain form); 1: FP32 pair and
+                                    triplet arithmetic with FP64 C6 weights, dE/dCN and final
+                                    reductions (precision form) */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);
 

@@ -221,6 +221,13 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
     switch (option) {
     case D3_OPT_ATM_FORCE_SCALED: o.atm_force_scaled = value != 0; break;
     case D3_OPT_SMOOTH_CN: o.smooth_cn = value != 0; break;
+    case D3_OPT_PRECISION:
+        if (value != 0 && value != 1) {
+            set_error("D3_OPT_PRECISION takes 0 (FP64) or 1 (FP32 pair/triplet arithmetic)");
+            return 1;
+        }
+        o.precision = value;
+        break;
     default: set_error("unknown option " + std::to_string(option)); return 1;
     }
     d3::engine_set_options(H(handle)->engine, o);

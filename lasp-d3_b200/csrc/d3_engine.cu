@@ -98,6 +98,10 @@ struct KP {
     // outputs
     double *out; // [0]=E(eV), [1..3n]=F(eV/A), [3n+1..3n+9]=stress(eV/A^3)
     unsigned int *status;
+    // precision form: FP32 copies of positions, weights and C6 rows
+    int precision;
+    float4 *xs32;
+    float *w32, *dw32, *Y32;
     // work counters: [0] ATM in-range visits (2 per triplet), [1] two-body in-range
     // ordered pairs, [2] CN in-range ordered pairs
     unsigned long long *counters;
@@ -116,9 +120,15 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // Traverse every candidate (j, T) of binned atom i through a row-compressed stencil.
-// All 32 lanes call f(j, T, active) together (converged), so f may use warp votes.
-template <class F>
-__device__ __forceinline__ void traverse(const KP &p, int bin, const int4 *rows, int nrows, F &&f) {
+// All 32 lanes call f(j, Tx, Ty, Tz, shift, active) together (converged), so f may use
+// warp votes; shift = T h (bohr) is computed once per contiguous range of candidates.
+// row_end() is called (converged) after each stencil row.
+struct NoRowEnd {
+    __device__ __forceinline__ void operator()() const {}
+};
+
+template <class F, class R = NoRowEnd>
+__device__ __forceinline__ void traverse(const KP &p, int bin, const int4 *rows, int nrows, F &&f, R &&row_end = R()) {
     const int lane = threadIdx.x & 31;
     const int nb0 = p.nb[0], nb1 = p.nb[1], nb2 = p.nb[2];
     const int bx = bin % nb0, by = (bin / nb0) % nb1, bz = bin / (nb0 * nb1);
@@ -134,11 +144,14 @@ __device__ __forceinline__ void traverse(const KP &p, int bin, const int4 *rows,
             const int a = max(xlo, px * nb0) - px * nb0;
             const int b = min(xhi, px * nb0 + nb0 - 1) - px * nb0;
             const int jlo = p.bin_start[rowbase + a], jhi = p.bin_start[rowbase + b + 1];
+            const double3 sh = make_double3(px * p.h[0] + Ty * p.h[3] + Tz * p.h[6], px * p.h[1] + Ty * p.h[4] + Tz * p.h[7],
+                                            px * p.h[2] + Ty * p.h[5] + Tz * p.h[8]);
             for (int base = jlo; base < jhi; base += 32) {
                 const int j = base + lane;
-                f(j, px, Ty, Tz, j < jhi);
+                f(j, px, Ty, Tz, sh, j < jhi);
             }
         }
+        row_end();
     }
 }
 
@@ -252,7 +265,9 @@ __global__ void k_gather(KP p) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= p.n) return;
     const int i = p.order[s];
-    p.xs[s] = p.xw_in[i];
+    const double4 x = p.xw_in[i];
+    p.xs[s] = x;
+    if (p.precision) p.xs32[s] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
     p.shift[s] = p.shift_in[i];
     p.bin_s[s] = p.bin_in[i];
     p.orig[s] = i;
@@ -284,13 +299,11 @@ __global__ void k_cn(KP p) {
     const double ri = p.rcov[(int)xi.w];
     double acc = 0.0;
     unsigned int npair = 0;
-    traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, bool act) {
+    traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         if (!act) return;
         if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
         const double4 xj = p.xs[j];
-        double sx, sy, sz;
-        image_vec(p, Tx, Ty, Tz, sx, sy, sz);
-        const double dx = xi.x - (xj.x + sx), dy = xi.y - (xj.y + sy), dz = xi.z - (xj.z + sz);
+        const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
         const double d2 = dx * dx + dy * dy + dz * dz;
         if (d2 <= p.rcn2 && d2 > 0.0) {
             double dd;
@@ -347,8 +360,13 @@ __global__ void k_weights(KP p) {
 #pragma unroll
     for (int a = 0; a < NR; ++a) {
         const double wn = w[a] * isw;
+        const double dwn = dw[a] * isw - wn * ratio;
         p.w[(size_t)i * NR + a] = wn;
-        p.dw[(size_t)i * NR + a] = dw[a] * isw - wn * ratio;
+        p.dw[(size_t)i * NR + a] = dwn;
+        if (p.precision) {
+            p.w32[(size_t)i * NR + a] = (float)wn;
+            p.dw32[(size_t)i * NR + a] = (float)dwn;
+        }
         w[a] = wn;
     }
     for (int tt = 0; tt < p.ne; ++tt) {
@@ -360,6 +378,7 @@ __global__ void k_weights(KP p) {
 #pragma unroll
             for (int a = 0; a < NR; ++a) acc += w[a] * C[a * NR + b];
             Yo[b] = acc;
+            if (p.precision) p.Y32[((size_t)i * p.ne + tt) * NR + b] = (float)acc;
         }
     }
 }
@@ -383,13 +402,11 @@ __global__ void k_twobody(KP p) {
     const double rri = p.r2r4[ti];
     double e = 0, g = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
     unsigned int npair = 0;
-    traverse(p, p.bin_s[i], p.st2, p.nst2, [&](int j, int Tx, int Ty, int Tz, bool act) {
+    traverse(p, p.bin_s[i], p.st2, p.nst2, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         if (!act) return;
         if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
         const double4 xj = p.xs[j];
-        double sx, sy, sz;
-        image_vec(p, Tx, Ty, Tz, sx, sy, sz);
-        const double dx = xi.x - (xj.x + sx), dy = xi.y - (xj.y + sy), dz = xi.z - (xj.z + sz);
+        const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
         const double r2 = dx * dx + dy * dy + dz * dz;
         if (!(r2 < p.rc2 && r2 > 0.0)) return;
         ++npair;
@@ -485,13 +502,11 @@ __global__ void k_atm_list(KP p) {
     if (FILL) pos = p.atm_off[a];
     int count = 0;
     bool range_err = false;
-    traverse(p, p.bin_s[a], p.sta, p.nsta, [&](int j, int Tx, int Ty, int Tz, bool act) {
+    traverse(p, p.bin_s[a], p.sta, p.nsta, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         bool keep = false;
         if (act && p.orig[j] <= oa && in_box(p, sa, p.shift[j], Tx, Ty, Tz)) {
             const double4 xj = p.xs[j];
-            double sx, sy, sz;
-            image_vec(p, Tx, Ty, Tz, sx, sy, sz);
-            const double dx = xa.x - (xj.x + sx), dy = xa.y - (xj.y + sy), dz = xa.z - (xj.z + sz);
+            const double dx = xa.x - (xj.x + sh.x), dy = xa.y - (xj.y + sh.y), dz = xa.z - (xj.z + sh.z);
             const double d2 = dx * dx + dy * dy + dz * dz;
             keep = !(d2 > p.ratm2 || d2 < 1e-12);
         }
@@ -519,7 +534,248 @@ __global__ void k_atm_list(KP p) {
 
 __device__ __forceinline__ int sext8(int v) { return (v << 24) >> 24; }
 
+// ------------------------------------------------------------------------------------
+// precision form: CN, two-body and chain rule with FP32 pair arithmetic. Sums are kept
+// in FP32 within one stencil row and carried across rows in FP64 (blocked summation);
+// dE/dCN is accumulated in FP64.
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ float cn_term32(float r2, float rsum, float *dcn_over_r) {
+    const float ir = rsqrtf(r2);
+    const float e = __expf(-16.0f * fmaf(rsum, ir, -1.0f));
+    const float ope = 1.0f + e;
+    const float inv = __fdividef(1.0f, ope);
+    *dcn_over_r = -16.0f * e * rsum * ir * ir * ir * inv * inv;
+    return inv;
+}
+
+__global__ void k_cn32(KP p) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= p.n) return;
+    const float4 xi = p.xs32[i];
+    const int4 si = p.shift[i];
+    const float ri = (float)p.rcov[(int)xi.w];
+    const float rcn2 = (float)p.rcn2;
+    double acc = 0.0;
+    float part = 0.0f;
+    unsigned int npair = 0;
+    traverse(
+        p, p.bin_s[i], p.stc, p.nstc,
+        [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+            if (!act) return;
+            if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+            const float4 xj = p.xs32[j];
+            const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
+                        dz = (xi.z - (float)sh.z) - xj.z;
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (d2 <= rcn2 && d2 > 0.0f) {
+                float dd;
+                part += cn_term32(d2, ri + (float)p.rcov[(int)xj.w], &dd);
+                ++npair;
+            }
+        },
+        [&]() {
+            acc += part;
+            part = 0.0f;
+        });
+    acc = warp_sum(acc);
+    for (int o = 16; o > 0; o >>= 1) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+    if ((threadIdx.x & 31) == 0) {
+        p.cn[i] = acc;
+        atomicAdd(&p.counters[2], (unsigned long long)npair);
+    }
+}
+
+template <int NR>
+__global__ void k_twobody32(KP p) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= p.n) return;
+    const float4 xi = p.xs32[i];
+    const int4 si = p.shift[i];
+    const int ti = (int)xi.w;
+    float wi[NR], dwi[NR];
+#pragma unroll
+    for (int a = 0; a < NR; ++a) {
+        wi[a] = p.w32[(size_t)i * NR + a];
+        dwi[a] = p.dw32[(size_t)i * NR + a];
+    }
+    const float rri = (float)p.r2r4[ti];
+    const float rc2 = (float)p.rc2, s6 = (float)p.s6, s8 = (float)p.s8, p1 = (float)p.p1, p2 = (float)p.p2;
+    double E = 0, G = 0, FX = 0, FY = 0, FZ = 0, VXX = 0, VYY = 0, VZZ = 0, VXY = 0, VXZ = 0, VYZ = 0;
+    float e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+    unsigned int npair = 0;
+    traverse(
+        p, p.bin_s[i], p.st2, p.nst2,
+        [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+            if (!act) return;
+            if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+            const float4 xj = p.xs32[j];
+            const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
+                        dz = (xi.z - (float)sh.z) - xj.z;
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (!(r2 < rc2 && r2 > 0.0f)) return;
+            ++npair;
+            const int tj = (int)xj.w;
+            const float *yj = p.Y32 + ((size_t)j * p.ne + ti) * NR;
+            float c6 = 0.f, dc6 = 0.f;
+#pragma unroll
+            for (int b = 0; b < NR; ++b) {
+                const float y = yj[b];
+                c6 = fmaf(y, wi[b], c6);
+                dc6 = fmaf(y, dwi[b], dc6);
+            }
+            const float rr = 3.0f * rri * (float)p.r2r4[tj];
+            const float c8 = c6 * rr, dc8 = dc6 * rr;
+            const double *pa = p.pairA + ((size_t)ti * p.ne + tj) * 4;
+            float E6, E8, Gt, fs;
+            if (p.damping == 1) {
+                const float r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
+                const float i6 = __fdividef(1.0f, r6 + (float)pa[0]), i8 = __fdividef(1.0f, r8 + (float)pa[1]);
+                E6 = s6 * c6 * i6;
+                E8 = s8 * c8 * i8;
+                Gt = s6 * dc6 * i6 + s8 * dc8 * i8;
+                fs = -6.0f * E6 * r4 * i6 - 8.0f * E8 * r6 * i8;
+            } else {
+                const float ir = rsqrtf(r2), ir2 = ir * ir;
+                const float ir6 = ir2 * ir2 * ir2, ir8 = ir6 * ir2;
+                const float R0 = (float)pa[0];
+                const float x6 = p1 * R0 * ir, x8 = p2 * R0 * ir;
+                const float x6_2 = x6 * x6, x6_4 = x6_2 * x6_2, x6_8 = x6_4 * x6_4, x6_14 = x6_8 * x6_4 * x6_2;
+                const float x8_2 = x8 * x8, x8_4 = x8_2 * x8_2, x8_8 = x8_4 * x8_4, x8_16 = x8_8 * x8_8;
+                const float f6 = __fdividef(1.0f, fmaf(6.0f, x6_14, 1.0f)), f8 = __fdividef(1.0f, fmaf(6.0f, x8_16, 1.0f));
+                const float df6 = 84.0f * f6 * f6 * x6_14 * ir, df8 = 96.0f * f8 * f8 * x8_16 * ir;
+                E6 = s6 * c6 * f6 * ir6;
+                E8 = s8 * c8 * f8 * ir8;
+                Gt = s6 * f6 * dc6 * ir6 + s8 * f8 * dc8 * ir8;
+                fs = s6 * c6 * (-6.0f * f6 * ir8 + df6 * ir6 * ir) + s8 * c8 * (-8.0f * f8 * ir8 * ir2 + df8 * ir8 * ir);
+            }
+            e += 0.5f * (E6 + E8);
+            G += (double)Gt;
+            fx = fmaf(fs, dx, fx);
+            fy = fmaf(fs, dy, fy);
+            fz = fmaf(fs, dz, fz);
+            const float fdx = fs * dx, fdy = fs * dy;
+            vxx = fmaf(fdx, dx, vxx);
+            vyy = fmaf(fdy, dy, vyy);
+            vzz = fmaf(fs * dz, dz, vzz);
+            vxy = fmaf(fdx, dy, vxy);
+            vxz = fmaf(fdx, dz, vxz);
+            vyz = fmaf(fdy, dz, vyz);
+        },
+        [&]() {
+            E += e;
+            FX += fx;
+            FY += fy;
+            FZ += fz;
+            VXX += vxx;
+            VYY += vyy;
+            VZZ += vzz;
+            VXY += vxy;
+            VXZ += vxz;
+            VYZ += vyz;
+            e = fx = fy = fz = vxx = vyy = vzz = vxy = vxz = vyz = 0.0f;
+        });
+    E = warp_sum(E);
+    G = warp_sum(G);
+    FX = warp_sum(FX);
+    FY = warp_sum(FY);
+    FZ = warp_sum(FZ);
+    VXX = warp_sum(VXX);
+    VYY = warp_sum(VYY);
+    VZZ = warp_sum(VZZ);
+    VXY = warp_sum(VXY);
+    VXZ = warp_sum(VXZ);
+    VYZ = warp_sum(VYZ);
+    for (int o = 16; o > 0; o >>= 1) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&p.counters[1], (unsigned long long)npair);
+        p.e2[i] = E;
+        p.g2[i] = G;
+        p.f2[3 * i] = FX;
+        p.f2[3 * i + 1] = FY;
+        p.f2[3 * i + 2] = FZ;
+        const double sc = -1.0 / (2.0 * p.vol);
+        double *v = p.v2 + 6 * (size_t)i;
+        v[0] = VXX * sc;
+        v[1] = VYY * sc;
+        v[2] = VZZ * sc;
+        v[3] = VXY * sc;
+        v[4] = VXZ * sc;
+        v[5] = VYZ * sc;
+    }
+}
+
+__global__ void k_chain32(KP p, const double *Gd) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= p.n) return;
+    const float4 xi = p.xs32[i];
+    const int4 si = p.shift[i];
+    const float ri = (float)p.rcov[(int)xi.w];
+    const double gi = Gd[i];
+    const float rcn2 = (float)p.rcn2;
+    double FX = 0, FY = 0, FZ = 0, VXX = 0, VYY = 0, VZZ = 0, VXY = 0, VXZ = 0, VYZ = 0;
+    float fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+    traverse(
+        p, p.bin_s[i], p.stc, p.nstc,
+        [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+            if (!act) return;
+            if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+            const float4 xj = p.xs32[j];
+            const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
+                        dz = (xi.z - (float)sh.z) - xj.z;
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (!(d2 <= rcn2 && d2 > 0.0f)) return;
+            float dcn;
+            cn_term32(d2, ri + (float)p.rcov[(int)xj.w], &dcn);
+            const float dE = (float)(gi + Gd[j]) * dcn;
+            const float fdx = dE * dx, fdy = dE * dy;
+            fx += fdx;
+            fy += fdy;
+            fz = fmaf(dE, dz, fz);
+            vxx = fmaf(fdx, dx, vxx);
+            vyy = fmaf(fdy, dy, vyy);
+            vzz = fmaf(dE * dz, dz, vzz);
+            vxy = fmaf(fdx, dy, vxy);
+            vxz = fmaf(fdx, dz, vxz);
+            vyz = fmaf(fdy, dz, vyz);
+        },
+        [&]() {
+            FX += fx;
+            FY += fy;
+            FZ += fz;
+            VXX += vxx;
+            VYY += vyy;
+            VZZ += vzz;
+            VXY += vxy;
+            VXZ += vxz;
+            VYZ += vyz;
+            fx = fy = fz = vxx = vyy = vzz = vxy = vxz = vyz = 0.0f;
+        });
+    FX = warp_sum(FX);
+    FY = warp_sum(FY);
+    FZ = warp_sum(FZ);
+    VXX = warp_sum(VXX);
+    VYY = warp_sum(VYY);
+    VZZ = warp_sum(VZZ);
+    VXY = warp_sum(VXY);
+    VXZ = warp_sum(VXZ);
+    VYZ = warp_sum(VYZ);
+    if ((threadIdx.x & 31) == 0) {
+        p.fc[3 * i] = FX;
+        p.fc[3 * i + 1] = FY;
+        p.fc[3 * i + 2] = FZ;
+        const double sc = -1.0 / (2.0 * p.vol);
+        double *v = p.vc + 6 * (size_t)i;
+        v[0] = VXX * sc;
+        v[1] = VYY * sc;
+        v[2] = VZZ * sc;
+        v[3] = VXY * sc;
+        v[4] = VXZ * sc;
+        v[5] = VYZ * sc;
+    }
+}
+
 #include "d3_atm.cuh"
+#include "d3_atm32.cuh"
 
 // ------------------------------------------------------------------------------------
 // chain rule (src/d3_kernel.cu:1511-1698): F_i += (dE/dCN_i + dE/dCN_j) dCN_ij/dr r_hat
@@ -532,13 +788,11 @@ __global__ void k_chain(KP p, const double *G) {
     const double ri = p.rcov[(int)xi.w];
     const double gi = G[i];
     double fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
-    traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, bool act) {
+    traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         if (!act) return;
         if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
         const double4 xj = p.xs[j];
-        double sx, sy, sz;
-        image_vec(p, Tx, Ty, Tz, sx, sy, sz);
-        const double dx = xi.x - (xj.x + sx), dy = xi.y - (xj.y + sy), dz = xi.z - (xj.z + sz);
+        const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
         const double d2 = dx * dx + dy * dy + dz * dz;
         if (!(d2 <= p.rcn2 && d2 > 0.0)) return;
         double dcn;
@@ -681,6 +935,8 @@ struct Engine {
     DBuf<int> bin_cnt, bin_start, bin_fill, order, bin_s, orig, sorted_of;
     DBuf<double> cn, w, dw, Y, e2, g2, f2, v2, ea, ga, fa, va, eb, gb, fb, fc, vc, G;
     DBuf<int> atm_cnt, work;
+    DBuf<float4> xs32;
+    DBuf<float> w32, dw32, Y32;
     DBuf<long long> atm_off;
     DBuf<int2> atm_ent;
     long long atm_cap = 0;
@@ -704,6 +960,10 @@ struct Engine {
         for (auto *d : is) d->release();
         shift_in.release();
         shift.release();
+        xs32.release();
+        w32.release();
+        dw32.release();
+        Y32.release();
         xw_in.release();
         xs.release();
         atm_off.release();
@@ -1007,6 +1267,18 @@ static KP make_kp(Engine *e) {
     p.p2 = e->fp.p2;
     p.damping = e->damping;
     p.smooth_cn = e->opt.smooth_cn ? 1 : 0;
+    p.precision = e->opt.precision;
+    if (p.precision) {
+        const size_t N = e->max_atoms;
+        e->xs32.ensure(N);
+        e->w32.ensure(N * e->nref);
+        e->dw32.ensure(N * e->nref);
+        e->Y32.ensure(N * e->ne * e->nref);
+    }
+    p.xs32 = e->xs32.p;
+    p.w32 = e->w32.p;
+    p.dw32 = e->dw32.p;
+    p.Y32 = e->Y32.p;
     p.atm_force_scaled = e->opt.atm_force_scaled ? 1 : 0;
     p.pos_in = e->pos_in.p;
     p.type_in = e->type_in.p;
@@ -1074,10 +1346,16 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     k_binsort<<<(p.nbins + T - 1) / T, T, 0, s>>>(p);
     k_gather<<<gb, T, 0, s>>>(p);
     D3_CUDA(cudaEventRecord(ev[1], s));
-    k_cn<<<gw, T, 0, s>>>(p);
+    if (p.precision)
+        k_cn32<<<gw, T, 0, s>>>(p);
+    else
+        k_cn<<<gw, T, 0, s>>>(p);
     k_weights<NR><<<gb, T, 0, s>>>(p);
     D3_CUDA(cudaEventRecord(ev[2], s));
-    k_twobody<NR><<<gw, T, 0, s>>>(p);
+    if (p.precision)
+        k_twobody32<NR><<<gw, T, 0, s>>>(p);
+    else
+        k_twobody<NR><<<gw, T, 0, s>>>(p);
     D3_CUDA(cudaEventRecord(ev[3], s));
     D3_CUDA(cudaMemsetAsync(p.ea, 0, sizeof(double) * n, s));
     D3_CUDA(cudaMemsetAsync(p.ga, 0, sizeof(double) * n, s));
@@ -1094,21 +1372,37 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     D3_CUDA(cudaEventRecord(ev[4], s));
     if (e->use_atm) {
         D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
-        // partner tile: as many entries as fit in ~160 KB next to the apex tables
-        const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double) +
-                             ATM_PERM_CAP * sizeof(unsigned short);
-        const size_t per = sizeof(Partner) + (size_t)p.ne * NR * sizeof(double);
-        const int tile = (int)std::max<size_t>(8, std::min<size_t>(128, (160 * 1024 - fixed) / per));
-        const size_t sm = (size_t)tile * per + fixed;
-        D3_CUDA(cudaFuncSetAttribute(k_atm<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        int blocks_per_sm = 0;
-        D3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_atm<NR>, ATM_THREADS, sm));
-        const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, blocks_per_sm)));
-        k_atm<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
+        if (p.precision) {
+            const size_t fixed = (size_t)p.ne * NR * sizeof(double) + ((p.ne * p.ne + 1) & ~1) * sizeof(float) +
+                                 ATM_PERM_CAP * sizeof(unsigned short) + 16;
+            const size_t per = sizeof(Partner32) + (size_t)p.ne * NR * sizeof(float);
+            const int tile = (int)std::max<size_t>(8, std::min<size_t>(128, (100 * 1024 - fixed) / per)) & ~1;
+            const size_t sm = (size_t)tile * per + fixed;
+            D3_CUDA(cudaFuncSetAttribute(k_atm32<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            int blocks_per_sm = 0;
+            D3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_atm32<NR>, ATM_THREADS, sm));
+            const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, blocks_per_sm)));
+            k_atm32<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
+        } else {
+            // partner tile: as many entries as fit in ~160 KB next to the apex tables
+            const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double) +
+                                 ATM_PERM_CAP * sizeof(unsigned short);
+            const size_t per = sizeof(Partner) + (size_t)p.ne * NR * sizeof(double);
+            const int tile = (int)std::max<size_t>(8, std::min<size_t>(128, (160 * 1024 - fixed) / per));
+            const size_t sm = (size_t)tile * per + fixed;
+            D3_CUDA(cudaFuncSetAttribute(k_atm<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            int blocks_per_sm = 0;
+            D3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_atm<NR>, ATM_THREADS, sm));
+            const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, blocks_per_sm)));
+            k_atm<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
+        }
     }
     D3_CUDA(cudaEventRecord(ev[5], s));
     k_sum_g<<<gb, T, 0, s>>>(p, e->G.p);
-    k_chain<<<gw, T, 0, s>>>(p, e->G.p);
+    if (p.precision)
+        k_chain32<<<gw, T, 0, s>>>(p, e->G.p);
+    else
+        k_chain<<<gw, T, 0, s>>>(p, e->G.p);
     D3_CUDA(cudaEventRecord(ev[6], s));
     k_forces_out<<<gb, T, 0, s>>>(p);
     k_reduce<<<1, 1024, 0, s>>>(p);

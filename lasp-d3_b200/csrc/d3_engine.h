@@ -42,6 +42,8 @@ struct Options {
     bool atm_force_scaled = false; // false: reference convention (ATM forces not scaled
                                    // by the 1/2, 1/6 repeated-index factors)
     bool smooth_cn = false;        // tanh^3 CN cutoff (reference SMOOTH_CUTOFF_CN)
+    int precision = 0;             // 0: FP64 plain form; 1: FP32 pair/triplet arithmetic with
+                                   // FP64 weights, dE/dCN and reductions (precision form)
 };
 
 struct Engine;

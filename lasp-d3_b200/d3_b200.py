@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libd3.so")
 HEADER = os.path.join(HERE, "..", "include", "d3.h")
 
 ZERO_DAMPING, BJ_DAMPING = 0, 1
-OPT_ATM_FORCE_SCALED, OPT_SMOOTH_CN = 1, 2
+OPT_ATM_FORCE_SCALED, OPT_SMOOTH_CN, OPT_PRECISION = 1, 2, 3
 TABLE_5REF, TABLE_7REF = 0, 1
 
 _lib = None

@@ -1,0 +1,54 @@
+"""Precision form (FP32 pair/triplet arithmetic, FP64 weights, dE/dCN and reductions)
+against the FP64 oracle. Targets of the form: energy within 1e-6 relative, forces within
+1e-4 eV/A, stress within 1e-6 eV/A^3 (the north-star bar for the mixed-precision form)."""
+import numpy as np
+import pytest
+
+import d3_systems as S
+import oracle
+from d3_b200 import D3, OPT_ATM_FORCE_SCALED, OPT_PRECISION
+
+pytestmark = pytest.mark.gpu
+
+
+def run(sys_, rc, rc_cn, rc_atm, damping, functional, table=0, options=()):
+    d = D3(sys_["Z"], len(sys_["Z"]), rc=rc, rc_cn=rc_cn, rc_atm=rc_atm, damping=damping, functional=functional,
+           table=table)
+    d.set_option(OPT_PRECISION, 1)
+    for o, v in options:
+        d.set_option(o, v)
+    d.set_cell(sys_["cell"])
+    d.set_atoms(sys_["pos"], sys_["Z"])
+    e, f, s = d.compute()
+    d.close()
+    return e, f, s
+
+
+@pytest.mark.parametrize("damping", [0, 1])
+@pytest.mark.parametrize("case", ["small", "fe", "water", "tric"])
+def test_precision_form_error_bounds(case, damping):
+    if case == "small":
+        sys_, kw = S.gtest_small_system(), dict(rc=40.0, rc_cn=40.0, rc_atm=40.0, functional=1)
+    elif case == "fe":
+        sys_ = S.gtest_bcc_fe(True)
+        sys_["pos"] = sys_["pos"] + np.random.default_rng(0).uniform(-0.1, 0.1, sys_["pos"].shape)
+        kw = dict(rc=30.0, rc_cn=30.0, rc_atm=30.0, functional=1)
+    elif case == "water":
+        sys_, kw = S.water_box(0), dict(rc=95.0, rc_cn=40.0, rc_atm=40.0, functional=0)
+    else:
+        sys_, kw = S.triclinic_box(400, seed=21), dict(rc=95.0, rc_cn=40.0, rc_atm=40.0, functional=0)
+    e, f, s = run(sys_, damping=damping, **kw)
+    r = oracle.compute(sys_["pos"], sys_["Z"], sys_["cell"], damping=damping, **kw)
+    assert abs(e - r["energy"]) <= 1e-6 * abs(r["energy"]), (e, r["energy"])
+    assert np.abs(f - r["forces"]).max() <= 1e-4
+    assert np.abs(s - r["stress"]).max() <= 1e-6
+
+
+def test_precision_form_scaled_atm_forces():
+    sys_ = S.gtest_bcc_fe()
+    sys_["pos"] = sys_["pos"] + np.random.default_rng(4).uniform(-0.1, 0.1, sys_["pos"].shape)
+    kw = dict(rc=30.0, rc_cn=30.0, rc_atm=30.0, functional=1, damping=1)
+    e, f, s = run(sys_, options=((OPT_ATM_FORCE_SCALED, 1),), **kw)
+    r = oracle.compute(sys_["pos"], sys_["Z"], sys_["cell"], atm_force_scaled=True, **kw)
+    assert abs(e - r["energy"]) <= 1e-6 * abs(r["energy"])
+    assert np.abs(f - r["forces"]).max() <= 1e-4
