@@ -32,12 +32,14 @@ sys.path.insert(0, os.path.join(ROOT, "lasp-d3_b200"))
 METRIC = "D3(BJ)+ATM atoms/s (E+F+stress) on 1 B200: plain vs chosen form at stated error"
 RC, RC_CN, RC_ATM = 95.0, 40.0, 40.0
 N_ATOMS = 20000
-# Algorithmic FLOPs of one ATM triplet term as the reference writes it
-# (src/d3_kernel.cu:1331-1447: geometry, angular term and its three derivatives, C9 and
-# its CN derivatives, damping and derivative, energy, forces, symmetric virial), counted
-# with add/mul/cmp = 1, fma = 2, div/sqrt/pow = 1; C6 interpolation is per pair and not
-# included. See DESIGN.md ("Roofline") for the itemised count.
-ATM_FLOP_PER_TRIPLET = 294
+# Algorithmic FLOPs of one in-range ATM triplet term as the reference writes it
+# (src/d3_kernel.cu:1331-1447: distances and range test 20, distance powers 24, r^2/r 3,
+# cosine numerators 6, cosine and angular term 8, three angular derivatives 72, C9 and
+# its CN derivatives 19, damping and its derivative 21, energy 7, dE/dCN 15, the three
+# force scalars once 18, 3x3 stress 99, forces 33), counted with add/mul/cmp = 1,
+# div/sqrt/pow = 1, each accumulation as one add; the C6 interpolation (per atom pair)
+# and the image translation (enumeration) are not included.
+ATM_FLOP_PER_TRIPLET = 345
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -349,6 +351,113 @@ def reference_arm(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def batch_mode(args):
+    """Batching form: many independent structures in one handle (one launch per pass, the
+    ATM pass one persistent launch over every structure's apexes), autotuned."""
+    import torch
+
+    import d3_autotune
+    import d3_systems as S
+    from d3_b200 import D3Batch, OPT_PRECISION
+
+    torch.cuda.set_device(0)
+    sts = S.batch_structs(count=args.batch, seed=3)
+    elements = sorted(set(int(z) for s in sts for z in s["Z"]))
+    ntot = sum(len(s["Z"]) for s in sts)
+    vol = sum(abs(np.linalg.det(s["cell"])) for s in sts)
+    out = {"metric": "D3(BJ)+ATM atoms/s (E+F+stress), %d-structure batch in one launch per pass" % len(sts),
+           "unit": "atoms/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "data": "synthetic",
+           "config": {"workload": "%d periodic structures, atom counts log-uniform in [8, 2000] (%d atoms in total), "
+                                  "cubic cells at 0.1 atoms/A^3 sheared by +-10 %% tilts, Dirichlet(1) compositions over "
+                                  "H/C/N/O/Si/Cu; PBE-D3(BJ)+ATM, rc 95 / 40 / 40 bohr" % (len(sts), ntot)},
+           "forms": {}}
+    stream = torch.cuda.Stream()
+    for form, prec in (("plain", 0), ("precision", 1)):
+        b = D3Batch(elements, len(sts), ntot, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
+        b.set_option(OPT_PRECISION, prec)
+        b.set_structures(sts)
+        key = d3_autotune.workload_key(ntot / len(sts), vol / len(sts), RC, RC_CN, RC_ATM, prec) + "|batch"
+        tuned = d3_autotune.tune(b, key, repeats=1)
+        e, _, _ = b.compute()
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                b.compute_async(stream.cuda_stream)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_ev.record(stream)
+            b.compute_async(stream.cuda_stream)
+            e_ev.record(stream)
+            e_ev.synchronize()
+            ms.append(s_ev.elapsed_time(e_ev))
+        pt, cnt = b.pass_times()
+        out["forms"][form] = {"value": ntot / (statistics.mean(ms) * 1e-3), "ms_per_step": statistics.mean(ms),
+                              "passes_ms": pt, "autotuned": {k: v for k, v in tuned.items() if k != "trials"},
+                              "energy_sum_ev": float(np.sum(e))}
+        b.close()
+    out["value"] = out["forms"]["precision"]["value"]
+    print(json.dumps(out), flush=True)
+
+
+def md_mode(args):
+    """200 MD-style steps of the 20,000-atom box (Gaussian displacement sigma = 0.01 A per
+    step, cell fixed) captured once in a CUDA graph and replayed; precision form, autotuned."""
+    import torch
+
+    import d3_autotune
+    import d3_systems as S
+    from d3_b200 import D3, OPT_PRECISION
+
+    torch.cuda.set_device(0)
+    n = args.atoms
+    sys_ = S.triclinic_box(n, seed=1)
+    d = D3(sys_["Z"], n, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
+    d.set_option(OPT_PRECISION, 1)
+    d.set_cell(sys_["cell"])
+    d.set_atoms(sys_["pos"], sys_["Z"])
+    vol = abs(np.linalg.det(sys_["cell"]))
+    tuned = d3_autotune.tune(d, d3_autotune.workload_key(n, vol, RC, RC_CN, RC_ATM, 1), repeats=1)
+    d.compute()  # list capacity for the trajectory (the list grows on overflow only outside capture)
+    pos = torch.tensor(sys_["pos"], dtype=torch.float64, device="cuda")
+    noise = torch.empty_like(pos)
+    stream = torch.cuda.Stream()
+    stream.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(stream):
+        # warm-up step outside capture
+        noise.normal_(0.0, 0.01)
+        pos.add_(noise)
+        d.set_positions_device(pos.data_ptr(), stream.cuda_stream)
+        d.compute_async(stream.cuda_stream)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        noise.normal_(0.0, 0.01)
+        pos.add_(noise)
+        d.set_positions_device(pos.data_ptr(), stream.cuda_stream)
+        d.compute_async(stream.cuda_stream)
+    torch.cuda.synchronize()
+    steps = args.md_steps
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        s_ev.record(stream)
+        for _ in range(steps):
+            graph.replay()
+        e_ev.record(stream)
+    e_ev.synchronize()
+    ms = s_ev.elapsed_time(e_ev)
+    out = {"metric": "D3(BJ)+ATM MD steps/s (E+F+stress per step), CUDA graph, %d-atom box" % n,
+           "value": steps / (ms * 1e-3), "unit": "steps/s", "atoms_per_s": n * steps / (ms * 1e-3),
+           "ms_per_step": ms / steps, "steps": steps, "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+           "config": {"workload": "%d-atom triclinic box, Gaussian displacement 0.01 A per step, cell fixed; "
+                                  "precision form; graph = displacement + set_positions_device + evaluation" % n},
+           "autotuned": {k: v for k, v in tuned.items() if k != "trials"}}
+    del graph
+    d.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -358,8 +467,17 @@ def main():
     ap.add_argument("--atoms", type=int, default=N_ATOMS)
     ap.add_argument("--ref-atoms", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["single", "batch", "md"], default="single")
+    ap.add_argument("--batch", type=int, default=2048)
+    ap.add_argument("--md-steps", type=int, default=200)
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.mode == "batch":
+        batch_mode(args)
+        return
+    if args.mode == "md":
+        md_mode(args)
+        return
     if args.impl == "reference":
         reference_arm(args, world, rank, local)
     else:

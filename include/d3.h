@@ -110,9 +110,12 @@ enum {
     D3_OPT_ATM_FORCE_SCALED = 1, /* 1: apply the 1/2, 1/6 repeated-index ATM factors to forces too
                                     (forces = -dE/dx); 0 (default): reference convention */
     D3_OPT_SMOOTH_CN = 2,        /* tanh^3 CN cutoff (reference compile-time SMOOTH_CUTOFF_CN) */
-    D3_OPT_PRECISION = 3         /* 0 (default): FP64 throughout (plain form); 1: FP32 pair and
+    D3_OPT_PRECISION = 3,        /* 0 (default): FP64 throughout (plain form); 1: FP32 pair and
                                     triplet arithmetic with FP64 C6 weights, dE/dCN and final
                                     reductions (precision form) */
+    D3_OPT_BIN_DIVISOR = 4,      /* cell-list bin width = smallest cutoff / value (1..32, default 6) */
+    D3_OPT_ATM_TILE = 5,         /* ATM partner tile entries (0 = automatic) */
+    D3_OPT_ATM_CTAS_PER_SM = 6   /* persistent ATM CTAs per SM (0 = occupancy limit) */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);
 
@@ -120,13 +123,38 @@ int d3_set_option(d3_handle_t *handle, int option, int value);
    (sr6, sr8) for zero damping or (a1, a2) for BJ damping. */
 int d3_set_functional_params(d3_handle_t *handle, double s6, double s8, double p1, double p2);
 
+/* Batching form: many independent periodic structures in one handle, evaluated by one
+   launch per pass (the ATM pass is one persistent launch over all structures' apexes).
+   d3_init_batch sizes the handle for up to max_structures structures holding together
+   up to max_total_atoms atoms. d3_set_batch_f64 takes the atom counts per structure,
+   the concatenated coordinates [n][3] and elements [n] (structure by structure, Angstrom)
+   and one cell per structure [n_structures][9] (Angstrom, rows = lattice vectors).
+   d3_compute_batch_f64 returns energies [n_structures] (eV), forces [n][3] (eV/A, same
+   order as given) and stresses [n_structures][9] (eV/A^3). The single-structure calls
+   refuse a handle that holds more than one structure. */
+d3_handle_t *d3_init_batch(const uint16_t *elements, uint64_t n_elements, uint64_t max_structures,
+                           uint64_t max_total_atoms, double rc, double rc_cn, double rc_atm, int damping_type,
+                           int functional_type, int table);
+int d3_set_batch_f64(d3_handle_t *handle, uint64_t n_structures, const uint64_t *atom_counts, const double *coords,
+                     const uint16_t *elements, const double *cells);
+uint16_t d3_compute_batch_f64(d3_handle_t *handle, double *energies, double *forces, double *stresses);
+int d3_num_structures(d3_handle_t *handle);
+
+/* Replace the positions of the atoms already set (same count and elements) from device
+   memory (double, Angstrom, [n][3]), ordered on cuda_stream; with d3_compute_async this
+   lets an MD loop run without host copies and be captured in a CUDA graph. */
+int d3_set_positions_device(d3_handle_t *handle, const double *coords_dev, void *cuda_stream);
+
 /* Enqueue one evaluation on a CUDA stream (cudaStream_t passed as void*, NULL = the
    handle's stream) with no host synchronisation; results stay on the device at
-   d3_device_results(): [0] energy, [1..3n] forces, [3n+1..3n+9] stress (double, eV
-   units). The neighbour-list capacity must already be sufficient (run one
+   d3_device_results(): energies [S], forces [3n], stresses [9S] (double, eV units; S = 1
+   for a single-structure handle). The neighbour-list capacity must already be sufficient (run one
    d3_compute_f64 or compute_dispersion_energy_from_handle_status first). */
 uint16_t d3_compute_async(d3_handle_t *handle, void *cuda_stream);
 const double *d3_device_results(d3_handle_t *handle);
+/* Copy the device results of the last evaluation to host arrays (energies [S], forces
+   [n][3], stresses [S][9]; any may be NULL). Synchronise the evaluation's stream first. */
+int d3_fetch_results(d3_handle_t *handle, double *energies, double *forces, double *stresses);
 
 /* Device time (ms, CUDA events on the evaluation's stream) of each pass of the last
    evaluation: [0] wrap+bin, [1] CN + C6 weights, [2] two-body, [3] ATM list,

@@ -50,6 +50,10 @@ d3_handle_t *make_handle(const uint16_t *elements, uint64_t n_el, uint64_t max_l
 }
 
 uint16_t compute_float(Handle *h, real_t *energy, real_t *force, real_t *stress) {
+    if (d3::engine_num_structures(h->engine) > 1) {
+        set_error("handle holds a batch of structures; use d3_compute_batch_f64");
+        return d3::ST_BAD_INPUT;
+    }
     const uint64_t n = d3::engine_num_atoms(h->engine);
     h->f64_forces.resize(3 * n);
     double e = 0, s[9] = {0};
@@ -206,6 +210,10 @@ uint16_t d3_compute_f64(d3_handle_t *handle, double *energy, double *force, doub
         set_error("handle is NULL in d3_compute_f64");
         return 1;
     }
+    if (d3::engine_num_structures(H(handle)->engine) > 1) {
+        set_error("handle holds a batch of structures; use d3_compute_batch_f64");
+        return d3::ST_BAD_INPUT;
+    }
     uint16_t st = d3::engine_compute(H(handle)->engine, energy, force, stress, nullptr, true);
     if (st & (d3::ST_CUDA_ERROR | d3::ST_NOT_READY))
         set_error(st & d3::ST_NOT_READY ? "atoms or cell not set" : "CUDA error during compute");
@@ -221,6 +229,15 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
     switch (option) {
     case D3_OPT_ATM_FORCE_SCALED: o.atm_force_scaled = value != 0; break;
     case D3_OPT_SMOOTH_CN: o.smooth_cn = value != 0; break;
+    case D3_OPT_BIN_DIVISOR:
+        if (value < 1 || value > 32) {
+            set_error("D3_OPT_BIN_DIVISOR takes 1..32");
+            return 1;
+        }
+        o.bin_divisor = value;
+        break;
+    case D3_OPT_ATM_TILE: o.atm_tile = value < 0 ? 0 : value; break;
+    case D3_OPT_ATM_CTAS_PER_SM: o.atm_ctas_per_sm = value < 0 ? 0 : value; break;
     case D3_OPT_PRECISION:
         if (value != 0 && value != 1) {
             set_error("D3_OPT_PRECISION takes 0 (FP64) or 1 (FP32 pair/triplet arithmetic)");
@@ -230,9 +247,89 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
         break;
     default: set_error("unknown option " + std::to_string(option)); return 1;
     }
-    d3::engine_set_options(H(handle)->engine, o);
+    try {
+        d3::engine_set_options(H(handle)->engine, o);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
     return 0;
 }
+
+d3_handle_t *d3_init_batch(const uint16_t *elements, uint64_t n_elements, uint64_t max_structures,
+                           uint64_t max_total_atoms, double rc, double rc_cn, double rc_atm, int damping_type,
+                           int functional_type, int table) {
+    std::string err;
+    d3::Engine *e = d3::engine_create(elements, n_elements, max_total_atoms, rc, rc_cn, rc_atm, rc_atm > 0.0,
+                                      damping_type, functional_type, table == D3_TABLE_7REF, err, max_structures);
+    if (!e) {
+        set_error(err);
+        return nullptr;
+    }
+    Handle *h = new Handle();
+    h->engine = e;
+    return reinterpret_cast<d3_handle_t *>(h);
+}
+
+int d3_set_batch_f64(d3_handle_t *handle, uint64_t n_structures, const uint64_t *atom_counts, const double *coords,
+                     const uint16_t *elements, const double *cells) {
+    if (!handle || !atom_counts || !coords || !elements || !cells) {
+        set_error("NULL argument in d3_set_batch_f64");
+        return 1;
+    }
+    uint64_t n = 0;
+    for (uint64_t k = 0; k < n_structures; ++k) n += atom_counts[k];
+    std::vector<double> b(3 * n), cb(9 * n_structures);
+    std::vector<float> cf(9 * n_structures);
+    const float a2b = 1.0f / 0.52917726f;
+    for (uint64_t i = 0; i < 3 * n; ++i) b[i] = coords[i] * d3::ANG2BOHR;
+    for (uint64_t i = 0; i < 9 * n_structures; ++i) {
+        cb[i] = cells[i] * d3::ANG2BOHR;
+        cf[i] = (float)cells[i] * a2b;
+    }
+    std::string err;
+    if (d3::engine_set_batch(H(handle)->engine, n_structures, atom_counts, b.data(), elements, cb.data(), cf.data(),
+                             err)) {
+        set_error(err);
+        return 1;
+    }
+    return 0;
+}
+
+uint16_t d3_compute_batch_f64(d3_handle_t *handle, double *energies, double *forces, double *stresses) {
+    if (!handle) {
+        set_error("handle is NULL in d3_compute_batch_f64");
+        return 1;
+    }
+    uint16_t st = d3::engine_compute(H(handle)->engine, energies, forces, stresses, nullptr, true);
+    if (st & (d3::ST_CUDA_ERROR | d3::ST_NOT_READY))
+        set_error(st & d3::ST_NOT_READY ? "atoms or cell not set" : "CUDA error during compute");
+    return st;
+}
+
+int d3_set_positions_device(d3_handle_t *handle, const double *coords_dev, void *cuda_stream) {
+    if (!handle || !coords_dev) {
+        set_error("NULL argument in d3_set_positions_device");
+        return 1;
+    }
+    return d3::engine_set_positions_device(H(handle)->engine, coords_dev, (cudaStream_t)cuda_stream);
+}
+
+int d3_fetch_results(d3_handle_t *handle, double *energies, double *forces, double *stresses) {
+    if (!handle) {
+        set_error("handle is NULL in d3_fetch_results");
+        return 1;
+    }
+    try {
+        d3::engine_fetch_results(H(handle)->engine, energies, forces, stresses);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+    return 0;
+}
+
+int d3_num_structures(d3_handle_t *handle) { return handle ? d3::engine_num_structures(H(handle)->engine) : -1; }
 
 int d3_set_functional_params(d3_handle_t *handle, double s6, double s8, double p1, double p2) {
     if (!handle) {

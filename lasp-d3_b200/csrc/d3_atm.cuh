@@ -109,6 +109,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
         const int m = (int)(p.atm_off[a + 1] - e0);
         const double4 xa = p.xs[a];
         const int ta = (int)xa.w;
+        const SG &g = p.sg[p.sid[a]];
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
         double dwa[NR];
 #pragma unroll
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
                 const int Tx = sext8(ent.y & 0xff), Ty = sext8((ent.y >> 8) & 0xff), Tz = sext8((ent.y >> 16) & 0xff);
                 const double4 xj = p.xs[ent.x];
                 double sx, sy, sz;
-                image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+                image_vec(g, Tx, Ty, Tz, sx, sy, sz);
                 const double dx = xj.x + sx - xa.x, dy = xj.y + sy - xa.y, dz = xj.z + sz - xa.z;
                 const int sh = min(ATM_SHELLS - 1, (int)(sqrt(dx * dx + dy * dy + dz * dz) * inv_rc * ATM_SHELLS));
                 atomicAdd(&shell_cnt[sh], 1);
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
                 const int Tx = sext8(ent.y & 0xff), Ty = sext8((ent.y >> 8) & 0xff), Tz = sext8((ent.y >> 16) & 0xff);
                 const double4 xj = p.xs[ent.x];
                 double sx, sy, sz;
-                image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+                image_vec(g, Tx, Ty, Tz, sx, sy, sz);
                 const double dx = xj.x + sx - xa.x, dy = xj.y + sy - xa.y, dz = xj.z + sz - xa.z;
                 const int sh = min(ATM_SHELLS - 1, (int)(sqrt(dx * dx + dy * dy + dz * dz) * inv_rc * ATM_SHELLS));
                 perm[atomicAdd(&shell_off[sh], 1)] = (unsigned short)k;
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
                 const double4 xj = p.xs[jq];
                 tq = (int)xj.w;
                 double sx, sy, sz;
-                image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+                image_vec(g, Tx, Ty, Tz, sx, sy, sz);
                 vqx = xj.x + sx - xa.x;
                 vqy = xj.y + sy - xa.y;
                 vqz = xj.z + sz - xa.z;
@@ -220,7 +221,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
                     const double4 xj = p.xs[jp];
                     const int tp = (int)xj.w;
                     double sx, sy, sz;
-                    image_vec(p, Tx, Ty, Tz, sx, sy, sz);
+                    image_vec(g, Tx, Ty, Tz, sx, sy, sz);
                     Partner pr;
                     pr.vx = xj.x + sx - xa.x;
                     pr.vy = xj.y + sy - xa.y;
@@ -381,7 +382,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
             p.fa[3 * a] = tot[2];
             p.fa[3 * a + 1] = tot[3];
             p.fa[3 * a + 2] = tot[4];
-            const double sc = -1.0 / p.vol;
+            const double sc = -1.0 / g.vol;
             for (int k = 0; k < 6; ++k) p.va[6 * (size_t)a + k] = tot[5 + k] * sc;
         }
     }

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 
 #include "d3_synth_params.h"
@@ -47,14 +48,26 @@ constexpr double K3 = 4.0;
 // ------------------------------------------------------------------------------------
 // kernel parameter block (passed by value)
 // ------------------------------------------------------------------------------------
+// geometry of one structure (a batch holds many; a plain handle holds one)
+struct SG {
+    double h[9], inv[9], vol; // rows = lattice vectors (bohr), inverse, signed volume
+    int nb[3], nbins;         // bin grid of this structure
+    int bin_base;             // first global bin index of this structure
+    int box_mode;             // 1: the reference's image box applies (ALL_ITERATE)
+    int half[3];              // image box half-widths
+    int atom_base, natoms;    // atom range in caller order
+    int st2_off, st2_n, stc_off, stc_n, sta_off, sta_n; // stencil rows (two-body, CN, ATM)
+};
+
 struct KP {
-    int n;
+    int n;                    // atoms of all structures
+    int nstruct;
+    int nbins_total;
     int ne, nref;
-    double h[9], inv[9], vol;
-    int nb[3];
-    int nbins;
-    int box_mode;
-    int half[3];
+    const SG *sg;
+    const int *sid_in;        // structure of each atom, caller order
+    int *sid;                 // structure of each atom, binned order
+    const int4 *stencils;     // all stencil rows (x = dy, y = dz, z = dxlo, w = dxhi)
     double rc2, rcn2, ratm2, rc_cn;
     // tables
     const double *cnref; // [ne][MAX_NREF]
@@ -88,15 +101,9 @@ struct KP {
     int2 *atm_ent;
     long long atm_cap;
     int *work;
-    // stencils (x = dy, y = dz, z = dxlo, w = dxhi)
-    const int4 *st2;
-    int nst2;
-    const int4 *stc;
-    int nstc;
-    const int4 *sta;
-    int nsta;
-    // outputs
-    double *out; // [0]=E(eV), [1..3n]=F(eV/A), [3n+1..3n+9]=stress(eV/A^3)
+    // outputs: [0, S) energies (eV), [S, S+3n) forces (eV/A, caller order),
+    // [S+3n, S+3n+9S) stresses (eV/A^3, row-major per structure)
+    double *out;
     unsigned int *status;
     // precision form: FP32 copies of positions, weights and C6 rows
     int precision;
@@ -128,9 +135,12 @@ struct NoRowEnd {
 };
 
 template <class F, class R = NoRowEnd>
-__device__ __forceinline__ void traverse(const KP &p, int bin, const int4 *rows, int nrows, F &&f, R &&row_end = R()) {
+__device__ __forceinline__ void traverse(const KP &p, const SG &g, int bin_global, const int4 *rows, int nrows, F &&f,
+                                         R &&row_end = R()) {
     const int lane = threadIdx.x & 31;
-    const int nb0 = p.nb[0], nb1 = p.nb[1], nb2 = p.nb[2];
+    const int nb0 = g.nb[0], nb1 = g.nb[1], nb2 = g.nb[2];
+    const int bin = bin_global - g.bin_base;
+    const int *bstart = p.bin_start + g.bin_base;
     const int bx = bin % nb0, by = (bin / nb0) % nb1, bz = bin / (nb0 * nb1);
     for (int r = 0; r < nrows; ++r) {
         const int4 row = rows[r];
@@ -143,9 +153,9 @@ __device__ __forceinline__ void traverse(const KP &p, int bin, const int4 *rows,
         for (int px = plo; px <= phi; ++px) {
             const int a = max(xlo, px * nb0) - px * nb0;
             const int b = min(xhi, px * nb0 + nb0 - 1) - px * nb0;
-            const int jlo = p.bin_start[rowbase + a], jhi = p.bin_start[rowbase + b + 1];
-            const double3 sh = make_double3(px * p.h[0] + Ty * p.h[3] + Tz * p.h[6], px * p.h[1] + Ty * p.h[4] + Tz * p.h[7],
-                                            px * p.h[2] + Ty * p.h[5] + Tz * p.h[8]);
+            const int jlo = bstart[rowbase + a], jhi = bstart[rowbase + b + 1];
+            const double3 sh = make_double3(px * g.h[0] + Ty * g.h[3] + Tz * g.h[6], px * g.h[1] + Ty * g.h[4] + Tz * g.h[7],
+                                            px * g.h[2] + Ty * g.h[5] + Tz * g.h[8]);
             for (int base = jlo; base < jhi; base += 32) {
                 const int j = base + lane;
                 f(j, px, Ty, Tz, sh, j < jhi);
@@ -155,17 +165,17 @@ __device__ __forceinline__ void traverse(const KP &p, int bin, const int4 *rows,
     }
 }
 
-__device__ __forceinline__ bool in_box(const KP &p, int4 si, int4 sj, int Tx, int Ty, int Tz) {
-    if (!p.box_mode) return true;
+__device__ __forceinline__ bool in_box(const SG &g, int4 si, int4 sj, int Tx, int Ty, int Tz) {
+    if (!g.box_mode) return true;
     // reference lattice shift of this image in unwrapped coordinates
     const int rx = Tx + si.x - sj.x, ry = Ty + si.y - sj.y, rz = Tz + si.z - sj.z;
-    return abs(rx) <= p.half[0] && abs(ry) <= p.half[1] && abs(rz) <= p.half[2];
+    return abs(rx) <= g.half[0] && abs(ry) <= g.half[1] && abs(rz) <= g.half[2];
 }
 
-__device__ __forceinline__ void image_vec(const KP &p, int Tx, int Ty, int Tz, double &sx, double &sy, double &sz) {
-    sx = Tx * p.h[0] + Ty * p.h[3] + Tz * p.h[6];
-    sy = Tx * p.h[1] + Ty * p.h[4] + Tz * p.h[7];
-    sz = Tx * p.h[2] + Ty * p.h[5] + Tz * p.h[8];
+__device__ __forceinline__ void image_vec(const SG &g, int Tx, int Ty, int Tz, double &sx, double &sy, double &sz) {
+    sx = Tx * g.h[0] + Ty * g.h[3] + Tz * g.h[6];
+    sy = Tx * g.h[1] + Ty * g.h[4] + Tz * g.h[7];
+    sz = Tx * g.h[2] + Ty * g.h[5] + Tz * g.h[8];
 }
 
 // ------------------------------------------------------------------------------------
@@ -174,25 +184,26 @@ __device__ __forceinline__ void image_vec(const KP &p, int Tx, int Ty, int Tz, d
 __global__ void k_bin(KP p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
+    const SG &g = p.sg[p.sid_in[i]];
     const double x = p.pos_in[3 * i], y = p.pos_in[3 * i + 1], z = p.pos_in[3 * i + 2];
     int s[3], b[3];
     bool bad = !(isfinite(x) && isfinite(y) && isfinite(z));
     for (int k = 0; k < 3; ++k) {
-        double f = x * p.inv[0 * 3 + k] + y * p.inv[1 * 3 + k] + z * p.inv[2 * 3 + k];
+        double f = x * g.inv[0 * 3 + k] + y * g.inv[1 * 3 + k] + z * g.inv[2 * 3 + k];
         if (bad || fabs(f) > 1.0e6) {
             bad = true;
             f = 0.0;
         }
         double fl = floor(f);
         s[k] = (int)fl;
-        int bk = (int)((f - fl) * p.nb[k]);
-        b[k] = min(max(bk, 0), p.nb[k] - 1);
+        int bk = (int)((f - fl) * g.nb[k]);
+        b[k] = min(max(bk, 0), g.nb[k] - 1);
     }
     if (bad) atomicOr(p.status, ST_BAD_INPUT);
-    const int bin = b[0] + p.nb[0] * (b[1] + p.nb[1] * b[2]);
-    double xw = x - (s[0] * p.h[0] + s[1] * p.h[3] + s[2] * p.h[6]);
-    double yw = y - (s[0] * p.h[1] + s[1] * p.h[4] + s[2] * p.h[7]);
-    double zw = z - (s[0] * p.h[2] + s[1] * p.h[5] + s[2] * p.h[8]);
+    const int bin = g.bin_base + b[0] + g.nb[0] * (b[1] + g.nb[1] * b[2]);
+    double xw = x - (s[0] * g.h[0] + s[1] * g.h[3] + s[2] * g.h[6]);
+    double yw = y - (s[0] * g.h[1] + s[1] * g.h[4] + s[2] * g.h[7]);
+    double zw = z - (s[0] * g.h[2] + s[1] * g.h[5] + s[2] * g.h[8]);
     if (bad) xw = yw = zw = 0.0;
     p.bin_in[i] = bin;
     p.shift_in[i] = make_int4(s[0], s[1], s[2], 0);
@@ -249,7 +260,7 @@ __global__ void k_scatter(KP p) {
 // make the in-bin order deterministic: ascending caller index (bins hold few atoms)
 __global__ void k_binsort(KP p) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= p.nbins) return;
+    if (b >= p.nbins_total) return;
     const int lo = p.bin_start[b], hi = p.bin_start[b + 1];
     for (int i = lo + 1; i < hi; ++i) {
         int v = p.order[i], k = i - 1;
@@ -270,6 +281,7 @@ __global__ void k_gather(KP p) {
     if (p.precision) p.xs32[s] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)x.w);
     p.shift[s] = p.shift_in[i];
     p.bin_s[s] = p.bin_in[i];
+    p.sid[s] = p.sid_in[i];
     p.orig[s] = i;
     p.sorted_of[i] = s;
 }
@@ -294,14 +306,15 @@ __device__ __forceinline__ double cn_term(const KP &p, double r, double rsum, do
 __global__ void k_cn(KP p) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= p.n) return;
+    const SG &g = p.sg[p.sid[i]];
     const double4 xi = p.xs[i];
     const int4 si = p.shift[i];
     const double ri = p.rcov[(int)xi.w];
     double acc = 0.0;
     unsigned int npair = 0;
-    traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+    traverse(p, g, p.bin_s[i], p.stencils + g.stc_off, g.stc_n, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         if (!act) return;
-        if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+        if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
         const double4 xj = p.xs[j];
         const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
         const double d2 = dx * dx + dy * dy + dz * dz;
@@ -390,6 +403,7 @@ template <int NR>
 __global__ void k_twobody(KP p) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= p.n) return;
+    const SG &g = p.sg[p.sid[i]];
     const double4 xi = p.xs[i];
     const int4 si = p.shift[i];
     const int ti = (int)xi.w;
@@ -400,11 +414,11 @@ __global__ void k_twobody(KP p) {
         dwi[a] = p.dw[(size_t)i * NR + a];
     }
     const double rri = p.r2r4[ti];
-    double e = 0, g = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+    double e = 0, gacc = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
     unsigned int npair = 0;
-    traverse(p, p.bin_s[i], p.st2, p.nst2, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+    traverse(p, g, p.bin_s[i], p.stencils + g.st2_off, g.st2_n, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         if (!act) return;
-        if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+        if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
         const double4 xj = p.xs[j];
         const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
         const double r2 = dx * dx + dy * dy + dz * dz;
@@ -445,7 +459,7 @@ __global__ void k_twobody(KP p) {
             fs = p.s6 * c6 * (-6.0 * f6 * ir8 + df6 * ir6 * ir) + p.s8 * c8 * (-8.0 * f8 * ir8 * ir2 + df8 * ir8 * ir);
         }
         e += 0.5 * (E6 + E8);
-        g += G;
+        gacc += G;
         fx += fs * dx;
         fy += fs * dy;
         fz += fs * dz;
@@ -457,7 +471,7 @@ __global__ void k_twobody(KP p) {
         vyz += fs * dy * dz;
     });
     e = warp_sum(e);
-    g = warp_sum(g);
+    gacc = warp_sum(gacc);
     fx = warp_sum(fx);
     fy = warp_sum(fy);
     fz = warp_sum(fz);
@@ -471,11 +485,11 @@ __global__ void k_twobody(KP p) {
     if ((threadIdx.x & 31) == 0) {
         atomicAdd(&p.counters[1], (unsigned long long)npair);
         p.e2[i] = e;
-        p.g2[i] = g;
+        p.g2[i] = gacc;
         p.f2[3 * i] = fx;
         p.f2[3 * i + 1] = fy;
         p.f2[3 * i + 2] = fz;
-        const double sc = -1.0 / (2.0 * p.vol);
+        const double sc = -1.0 / (2.0 * g.vol);
         double *v = p.v2 + 6 * (size_t)i;
         v[0] = vxx * sc;
         v[1] = vyy * sc;
@@ -494,6 +508,7 @@ template <bool FILL>
 __global__ void k_atm_list(KP p) {
     const int a = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (a >= p.n) return;
+    const SG &g = p.sg[p.sid[a]];
     const int lane = threadIdx.x & 31;
     const double4 xa = p.xs[a];
     const int4 sa = p.shift[a];
@@ -502,9 +517,9 @@ __global__ void k_atm_list(KP p) {
     if (FILL) pos = p.atm_off[a];
     int count = 0;
     bool range_err = false;
-    traverse(p, p.bin_s[a], p.sta, p.nsta, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+    traverse(p, g, p.bin_s[a], p.stencils + g.sta_off, g.sta_n, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         bool keep = false;
-        if (act && p.orig[j] <= oa && in_box(p, sa, p.shift[j], Tx, Ty, Tz)) {
+        if (act && p.orig[j] <= oa && in_box(g, sa, p.shift[j], Tx, Ty, Tz)) {
             const double4 xj = p.xs[j];
             const double dx = xa.x - (xj.x + sh.x), dy = xa.y - (xj.y + sh.y), dz = xa.z - (xj.z + sh.z);
             const double d2 = dx * dx + dy * dy + dz * dz;
@@ -551,6 +566,7 @@ __device__ __forceinline__ float cn_term32(float r2, float rsum, float *dcn_over
 __global__ void k_cn32(KP p) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= p.n) return;
+    const SG &g = p.sg[p.sid[i]];
     const float4 xi = p.xs32[i];
     const int4 si = p.shift[i];
     const float ri = (float)p.rcov[(int)xi.w];
@@ -559,10 +575,10 @@ __global__ void k_cn32(KP p) {
     float part = 0.0f;
     unsigned int npair = 0;
     traverse(
-        p, p.bin_s[i], p.stc, p.nstc,
+        p, g, p.bin_s[i], p.stencils + g.stc_off, g.stc_n,
         [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
             if (!act) return;
-            if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+            if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
             const float4 xj = p.xs32[j];
             const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
                         dz = (xi.z - (float)sh.z) - xj.z;
@@ -589,6 +605,7 @@ template <int NR>
 __global__ void k_twobody32(KP p) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= p.n) return;
+    const SG &g = p.sg[p.sid[i]];
     const float4 xi = p.xs32[i];
     const int4 si = p.shift[i];
     const int ti = (int)xi.w;
@@ -604,10 +621,10 @@ __global__ void k_twobody32(KP p) {
     float e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
     unsigned int npair = 0;
     traverse(
-        p, p.bin_s[i], p.st2, p.nst2,
+        p, g, p.bin_s[i], p.stencils + g.st2_off, g.st2_n,
         [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
             if (!act) return;
-            if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+            if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
             const float4 xj = p.xs32[j];
             const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
                         dz = (xi.z - (float)sh.z) - xj.z;
@@ -693,7 +710,7 @@ __global__ void k_twobody32(KP p) {
         p.f2[3 * i] = FX;
         p.f2[3 * i + 1] = FY;
         p.f2[3 * i + 2] = FZ;
-        const double sc = -1.0 / (2.0 * p.vol);
+        const double sc = -1.0 / (2.0 * g.vol);
         double *v = p.v2 + 6 * (size_t)i;
         v[0] = VXX * sc;
         v[1] = VYY * sc;
@@ -707,6 +724,7 @@ __global__ void k_twobody32(KP p) {
 __global__ void k_chain32(KP p, const double *Gd) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= p.n) return;
+    const SG &g = p.sg[p.sid[i]];
     const float4 xi = p.xs32[i];
     const int4 si = p.shift[i];
     const float ri = (float)p.rcov[(int)xi.w];
@@ -715,10 +733,10 @@ __global__ void k_chain32(KP p, const double *Gd) {
     double FX = 0, FY = 0, FZ = 0, VXX = 0, VYY = 0, VZZ = 0, VXY = 0, VXZ = 0, VYZ = 0;
     float fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
     traverse(
-        p, p.bin_s[i], p.stc, p.nstc,
+        p, g, p.bin_s[i], p.stencils + g.stc_off, g.stc_n,
         [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
             if (!act) return;
-            if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+            if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
             const float4 xj = p.xs32[j];
             const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
                         dz = (xi.z - (float)sh.z) - xj.z;
@@ -763,7 +781,7 @@ __global__ void k_chain32(KP p, const double *Gd) {
         p.fc[3 * i] = FX;
         p.fc[3 * i + 1] = FY;
         p.fc[3 * i + 2] = FZ;
-        const double sc = -1.0 / (2.0 * p.vol);
+        const double sc = -1.0 / (2.0 * g.vol);
         double *v = p.vc + 6 * (size_t)i;
         v[0] = VXX * sc;
         v[1] = VYY * sc;
@@ -783,14 +801,15 @@ __global__ void k_chain32(KP p, const double *Gd) {
 __global__ void k_chain(KP p, const double *G) {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= p.n) return;
+    const SG &g = p.sg[p.sid[i]];
     const double4 xi = p.xs[i];
     const int4 si = p.shift[i];
     const double ri = p.rcov[(int)xi.w];
     const double gi = G[i];
     double fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
-    traverse(p, p.bin_s[i], p.stc, p.nstc, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+    traverse(p, g, p.bin_s[i], p.stencils + g.stc_off, g.stc_n, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         if (!act) return;
-        if (!in_box(p, si, p.shift[j], Tx, Ty, Tz)) return;
+        if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
         const double4 xj = p.xs[j];
         const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
         const double d2 = dx * dx + dy * dy + dz * dz;
@@ -821,7 +840,7 @@ __global__ void k_chain(KP p, const double *G) {
         p.fc[3 * i] = fx;
         p.fc[3 * i + 1] = fy;
         p.fc[3 * i + 2] = fz;
-        const double sc = -1.0 / (2.0 * p.vol);
+        const double sc = -1.0 / (2.0 * g.vol);
         double *v = p.vc + 6 * (size_t)i;
         v[0] = vxx * sc;
         v[1] = vyy * sc;
@@ -844,15 +863,19 @@ __global__ void k_forces_out(KP p) {
     if (s >= p.n) return;
     const int i = p.orig[s];
     const double cf = HARTREE_EV * ANG2BOHR;
+    double *F = p.out + p.nstruct;
     for (int k = 0; k < 3; ++k)
-        p.out[1 + 3 * i + k] = (p.f2[3 * s + k] + p.fa[3 * s + k] + p.fb[3 * s + k] + p.fc[3 * s + k]) * cf;
+        F[3 * i + k] = (p.f2[3 * s + k] + p.fa[3 * s + k] + p.fb[3 * s + k] + p.fc[3 * s + k]) * cf;
 }
 
-// deterministic total energy and virial: one block, fixed order
+// deterministic total energy and virial of each structure: one block per structure over
+// its atoms (contiguous in binned order), fixed order
 __global__ void k_reduce(KP p) {
     __shared__ double red[32][7];
+    const SG &g = p.sg[blockIdx.x];
+    const int lo = p.bin_start[g.bin_base], hi = p.bin_start[g.bin_base + g.nbins];
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-    for (int s = threadIdx.x; s < p.n; s += blockDim.x) {
+    for (int s = lo + threadIdx.x; s < hi; s += blockDim.x) {
         acc[0] += p.e2[s] + p.ea[s] + p.eb[s];
         for (int k = 0; k < 6; ++k) acc[1 + k] += p.v2[6 * (size_t)s + k] + p.va[6 * (size_t)s + k] + p.vc[6 * (size_t)s + k];
     }
@@ -866,9 +889,9 @@ __global__ void k_reduce(KP p) {
         double t[7] = {0, 0, 0, 0, 0, 0, 0};
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
             for (int k = 0; k < 7; ++k) t[k] += red[w][k];
-        p.out[0] = -t[0] * HARTREE_EV;
+        p.out[blockIdx.x] = -t[0] * HARTREE_EV;
         const double cs = HARTREE_EV * ANG2BOHR * ANG2BOHR * ANG2BOHR;
-        double *st = p.out + 1 + 3 * (size_t)p.n;
+        double *st = p.out + p.nstruct + 3 * (size_t)p.n + 9 * (size_t)blockIdx.x;
         // symmetric virial: xx yy zz xy xz yz
         st[0] = t[1] * cs;
         st[4] = t[2] * cs;
@@ -909,6 +932,7 @@ struct Engine {
     std::vector<int> elements; // sorted unique atomic numbers (handle slots)
     int ne = 0;
     uint64_t max_atoms = 0;
+    uint64_t max_structs = 1;
     double rc = 0, rc_cn = 0, rc_atm = 0;
     float rc_f = 0, rc_cn_f = 0;
     bool use_atm = false;
@@ -918,11 +942,16 @@ struct Engine {
     // state
     uint64_t n = 0;
     bool atoms_set = false, cell_set = false;
-    CellGeom geom{};
-    bool box_mode = true;
-    int64_t mcb[3] = {1, 1, 1};
-    int nb[3] = {1, 1, 1};
-    std::vector<StencilRow> st2, stc, sta;
+    int nstruct = 0;
+    int nbins_total = 0;
+    std::vector<SG> sg;          // per-structure geometry
+    std::vector<CellGeom> geoms; // per-structure cell (host)
+    std::vector<int4> stencil_rows;
+    std::vector<uint64_t> counts; // atoms per structure, cells (bohr, float copy) of the geometry
+    std::vector<double> cells;
+    std::vector<float> cells_f;
+    double first_cell[9] = {0};  // single-structure API: cell kept until atoms are set
+    float first_cell_f[9] = {0};
     int dev_sms = 148;
     cudaStream_t stream = nullptr;
     // tables
@@ -934,7 +963,8 @@ struct Engine {
     DBuf<double4> xw_in, xs;
     DBuf<int> bin_cnt, bin_start, bin_fill, order, bin_s, orig, sorted_of;
     DBuf<double> cn, w, dw, Y, e2, g2, f2, v2, ea, ga, fa, va, eb, gb, fb, fc, vc, G;
-    DBuf<int> atm_cnt, work;
+    DBuf<int> atm_cnt, work, sid_in, sid;
+    DBuf<SG> sg_dev;
     DBuf<float4> xs32;
     DBuf<float> w32, dw32, Y32;
     DBuf<long long> atm_off;
@@ -950,13 +980,18 @@ struct Engine {
     static constexpr int NEV = 8;
     cudaEvent_t ev[NEV] = {};
     bool have_events = false;
+    struct OccCache {
+        const void *fn = nullptr;
+        size_t sm = 0;
+        int blocks = 1;
+    } atm_occ_cache[2];
 
     ~Engine() {
         DBuf<double> *ds[] = {&t_cnref, &t_c6, &t_r0, &t_rcov, &t_r2r4, &t_pairA, &pos_in, &cn, &w, &dw, &Y, &e2,
                               &g2, &f2, &v2, &ea, &ga, &fa, &va, &eb, &gb, &fb, &fc, &vc, &G, &out};
         for (auto *d : ds) d->release();
         DBuf<int> *is[] = {&type_in, &bin_in, &bin_cnt, &bin_start, &bin_fill, &order, &bin_s, &orig, &sorted_of,
-                           &atm_cnt, &work};
+                           &atm_cnt, &work, &sid_in, &sid};
         for (auto *d : is) d->release();
         shift_in.release();
         shift.release();
@@ -969,6 +1004,7 @@ struct Engine {
         atm_off.release();
         atm_ent.release();
         st_dev.release();
+        sg_dev.release();
         status.release();
         counters.release();
         for (auto &x : ev)
@@ -976,6 +1012,9 @@ struct Engine {
         if (stream) cudaStreamDestroy(stream);
     }
 };
+
+static void build_structures(Engine *e, int nstruct, const uint64_t *counts, const double *cells,
+                             const float *cells_f);
 
 static const double FUNC_TABLE[7][7] = {
     // s6, s8_zero, s8_bj, sr6, sr8, a1, a2 (src/d3_types.h:46-54)
@@ -1027,8 +1066,29 @@ static void upload_pair_table(Engine *e) {
     D3_CUDA(cudaMemcpy(e->t_pairA.p, pa.data(), sizeof(double) * pa.size(), cudaMemcpyHostToDevice));
 }
 
+struct FullTable {
+    std::vector<float> c6, r0, rcov, r2r4;
+};
+
+static const FullTable &full_table(bool extended) {
+    static FullTable tabs[2];
+    static std::once_flag once[2];
+    const int t = extended ? 1 : 0;
+    std::call_once(once[t], [t]() {
+        const int NE = t ? D3_NE_EXTENDED : D3_NE_ORIGINAL, NR = t ? D3_NREF_EXTENDED : D3_NREF_ORIGINAL;
+        FullTable &f = tabs[t];
+        f.c6.resize((size_t)NE * NE * NR * NR * 3);
+        f.r0.resize((size_t)NE * NE);
+        f.rcov.resize(NE);
+        f.r2r4.resize(NE);
+        d3_synth_fill(D3_SYNTH_SEED, NE, NR, t, f.c6.data(), f.r0.data(), f.rcov.data(), f.r2r4.data());
+    });
+    return tabs[t];
+}
+
 Engine *engine_create(const uint16_t *elements, uint64_t n_elements, uint64_t max_atoms, double rc, double rc_cn,
-                      double rc_atm, bool use_atm, int damping, int functional, bool extended, std::string &err) {
+                      double rc_atm, bool use_atm, int damping, int functional, bool extended, std::string &err,
+                      uint64_t max_structs) {
     Engine *e = nullptr;
     try {
         if (!elements && n_elements) throw std::runtime_error("elements is NULL");
@@ -1054,6 +1114,8 @@ Engine *engine_create(const uint16_t *elements, uint64_t n_elements, uint64_t ma
         if (e->ne == 0) throw std::runtime_error("no elements given");
         if (e->ne > MAX_TYPES) throw std::runtime_error("too many distinct elements for one handle");
         e->max_atoms = max_atoms;
+        if (max_structs == 0 || max_structs > max_atoms) throw std::runtime_error("bad structure capacity");
+        e->max_structs = max_structs;
         e->rc = rc;
         e->rc_cn = rc_cn;
         e->rc_atm = rc_atm;
@@ -1067,9 +1129,10 @@ Engine *engine_create(const uint16_t *elements, uint64_t n_elements, uint64_t ma
         D3_CUDA(cudaGetDevice(&dev));
         D3_CUDA(cudaDeviceGetAttribute(&e->dev_sms, cudaDevAttrMultiProcessorCount, dev));
         D3_CUDA(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
-        // parameter tables: full synthetic table, gathered for this handle's elements
-        std::vector<float> c6((size_t)NE * NE * NR * NR * 3), r0((size_t)NE * NE), rcv(NE), rr(NE);
-        d3_synth_fill(D3_SYNTH_SEED, NE, NR, extended ? 1 : 0, c6.data(), r0.data(), rcv.data(), rr.data());
+        // parameter tables: full synthetic table (generated once per process and layout),
+        // gathered for this handle's elements
+        const FullTable &tab = full_table(extended);
+        const std::vector<float> &c6 = tab.c6, &r0 = tab.r0, &rcv = tab.rcov, &rr = tab.r2r4;
         const int ne = e->ne;
         std::vector<double> cnref((size_t)ne * MAX_NREF, -1.0), c6m((size_t)ne * ne * NR * NR, 0.0),
             r0m((size_t)ne * ne), rcovm(ne), r2r4m(ne);
@@ -1148,11 +1211,14 @@ Engine *engine_create(const uint16_t *elements, uint64_t n_elements, uint64_t ma
         e->atm_cnt.ensure(N);
         e->atm_off.ensure(N + 1);
         e->work.ensure(1);
-        e->out.ensure(1 + 3 * N + 9);
+        e->sid_in.ensure(N);
+        e->sid.ensure(N);
+        e->sg_dev.ensure(max_structs);
+        e->out.ensure(10 * max_structs + 3 * N);
         e->status.ensure(1);
         e->counters.ensure(4);
         for (auto &x : e->ev) D3_CUDA(cudaEventCreate(&x));
-        e->host_out.resize(1 + 3 * N + 9);
+        e->host_out.resize(10 * max_structs + 3 * N);
         return e;
     } catch (const std::exception &ex) {
         err = ex.what();
@@ -1167,7 +1233,16 @@ void engine_destroy(Engine *e) {
     delete e;
 }
 
-void engine_set_options(Engine *e, const Options &o) { e->opt = o; }
+void engine_set_options(Engine *e, const Options &o) {
+    const bool regrid = o.bin_divisor != e->opt.bin_divisor;
+    e->opt = o;
+    if (regrid && e->cell_set && e->nstruct > 0) {
+        const std::vector<uint64_t> c = e->counts;
+        const std::vector<double> cl = e->cells;
+        const std::vector<float> cf = e->cells_f;
+        build_structures(e, e->nstruct, c.data(), cl.data(), cf.data());
+    }
+}
 Options engine_get_options(const Engine *e) { return e->opt; }
 void engine_set_functional_params(Engine *e, const FuncParams &p) {
     e->fp = p;
@@ -1176,24 +1251,99 @@ void engine_set_functional_params(Engine *e, const FuncParams &p) {
 uint64_t engine_num_atoms(const Engine *e) { return e->n; }
 const double *engine_device_results(const Engine *e) { return e->out.p; }
 
+static std::vector<int> map_types(const Engine *e, const uint16_t *Z, uint64_t n) {
+    std::vector<int> types(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        auto it = std::lower_bound(e->elements.begin(), e->elements.end(), (int)Z[i]);
+        if (it == e->elements.end() || *it != (int)Z[i])
+            throw std::runtime_error("element " + std::to_string(Z[i]) + " was not given when the handle was created");
+        types[i] = (int)(it - e->elements.begin());
+    }
+    return types;
+}
+
+// Geometry of every structure: reference image box and workload decision, bin grid,
+// stencils; uploads the records, the stencil rows and the per-atom structure index.
+static void build_structures(Engine *e, int nstruct, const uint64_t *counts, const double *cells,
+                             const float *cells_f) {
+    std::vector<SG> sg(nstruct);
+    std::vector<CellGeom> geoms(nstruct);
+    std::vector<int4> rows;
+    std::vector<int> sid;
+    int bin_base = 0, atom_base = 0;
+    const double rmin = std::min(e->rc_cn, e->use_atm ? std::min(e->rc, e->rc_atm) : e->rc);
+    const double target = std::max(rmin / e->opt.bin_divisor, 1.0);
+    for (int k = 0; k < nstruct; ++k) {
+        for (int i = 0; i < 9; ++i)
+            if (!std::isfinite(cells[9 * k + i])) throw std::runtime_error("cell has a non-finite entry");
+        CellGeom g = make_geom(cells + 9 * k);
+        if (!(std::fabs(g.volume) > 1e-12) || !std::isfinite(g.volume)) throw std::runtime_error("degenerate cell");
+        geoms[k] = g;
+        SG &r = sg[k];
+        memset(&r, 0, sizeof(SG));
+        for (int i = 0; i < 9; ++i) {
+            r.h[i] = g.h[i];
+            r.inv[i] = g.inv[i];
+        }
+        r.vol = g.volume;
+        int64_t mcb[3];
+        r.box_mode = reference_box(cells_f + 9 * k, e->rc_f, e->rc_cn_f, mcb) ? 1 : 0;
+        for (int i = 0; i < 3; ++i) r.half[i] = (int)(mcb[i] / 2);
+        const int64_t max_bins = std::max<int64_t>(64, (int64_t)std::max<uint64_t>(counts[k], 1) * 2);
+        choose_bins(g, target, max_bins, r.nb);
+        r.nbins = r.nb[0] * r.nb[1] * r.nb[2];
+        r.bin_base = bin_base;
+        bin_base += r.nbins;
+        r.atom_base = atom_base;
+        r.natoms = (int)counts[k];
+        atom_base += (int)counts[k];
+        auto add = [&](double rc, int &off, int &cnt) {
+            auto st = build_stencil(g, r.nb, rc);
+            off = (int)rows.size();
+            cnt = (int)st.size();
+            for (auto &x : st) rows.push_back(make_int4(x.dy, x.dz, x.dxlo, x.dxhi));
+        };
+        add(e->rc, r.st2_off, r.st2_n);
+        add(e->rc_cn, r.stc_off, r.stc_n);
+        if (e->use_atm) add(e->rc_atm, r.sta_off, r.sta_n);
+        sid.insert(sid.end(), counts[k], k);
+    }
+    e->sg = sg;
+    e->geoms = geoms;
+    e->counts.assign(counts, counts + nstruct);
+    e->cells.assign(cells, cells + 9 * (size_t)nstruct);
+    e->cells_f.assign(cells_f, cells_f + 9 * (size_t)nstruct);
+    e->stencil_rows = rows;
+    e->nstruct = nstruct;
+    e->nbins_total = bin_base;
+    e->sg_dev.ensure(nstruct);
+    D3_CUDA(cudaMemcpy(e->sg_dev.p, sg.data(), sizeof(SG) * nstruct, cudaMemcpyHostToDevice));
+    e->st_dev.ensure(rows.size());
+    if (!rows.empty())
+        D3_CUDA(cudaMemcpy(e->st_dev.p, rows.data(), sizeof(int4) * rows.size(), cudaMemcpyHostToDevice));
+    e->bin_cnt.ensure(bin_base);
+    e->bin_fill.ensure(bin_base);
+    e->bin_start.ensure(bin_base + 1);
+    if (!sid.empty()) D3_CUDA(cudaMemcpy(e->sid_in.p, sid.data(), sizeof(int) * sid.size(), cudaMemcpyHostToDevice));
+}
+
 int engine_set_atoms(Engine *e, const double *pos_bohr, const uint16_t *Z, uint64_t n, std::string &err) {
     try {
         if (n > e->max_atoms)
             throw std::runtime_error("length " + std::to_string(n) + " exceeds the handle capacity " +
                                      std::to_string(e->max_atoms));
         if (n == 0) throw std::runtime_error("no atoms given");
-        std::vector<int> types(n);
-        for (uint64_t i = 0; i < n; ++i) {
-            auto it = std::lower_bound(e->elements.begin(), e->elements.end(), (int)Z[i]);
-            if (it == e->elements.end() || *it != (int)Z[i])
-                throw std::runtime_error("element " + std::to_string(Z[i]) + " was not given when the handle was created");
-            types[i] = (int)(it - e->elements.begin());
-        }
+        std::vector<int> types = map_types(e, Z, n);
         D3_CUDA(cudaMemcpyAsync(e->pos_in.p, pos_bohr, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, e->stream));
         D3_CUDA(cudaMemcpyAsync(e->type_in.p, types.data(), sizeof(int) * n, cudaMemcpyHostToDevice, e->stream));
         D3_CUDA(cudaStreamSynchronize(e->stream));
+        const bool recount = e->n != n;
         e->n = n;
         e->atoms_set = true;
+        if (e->cell_set && (recount || e->nstruct != 1)) {
+            const uint64_t c = n;
+            build_structures(e, 1, &c, e->first_cell, e->first_cell_f);
+        }
         return 0;
     } catch (const std::exception &ex) {
         err = ex.what();
@@ -1203,28 +1353,41 @@ int engine_set_atoms(Engine *e, const double *pos_bohr, const uint16_t *Z, uint6
 
 int engine_set_cell(Engine *e, const double cell[9], const float cell_f[9], std::string &err) {
     try {
-        for (int i = 0; i < 9; ++i)
-            if (!std::isfinite(cell[i])) throw std::runtime_error("cell has a non-finite entry");
-        CellGeom g = make_geom(cell);
-        if (!(std::fabs(g.volume) > 1e-12) || !std::isfinite(g.volume)) throw std::runtime_error("degenerate cell");
-        e->geom = g;
-        e->box_mode = reference_box(cell_f, e->rc_f, e->rc_cn_f, e->mcb);
-        const double rmin = std::min(e->rc_cn, e->use_atm ? std::min(e->rc, e->rc_atm) : e->rc);
-        const double target = std::max(rmin / 6.0, 1.0);
-        const int64_t max_bins = std::max<int64_t>(64, (int64_t)std::max<uint64_t>(e->max_atoms, 1) * 2);
-        choose_bins(g, target, max_bins, e->nb);
-        e->st2 = build_stencil(g, e->nb, e->rc);
-        e->stc = build_stencil(g, e->nb, e->rc_cn);
-        e->sta = e->use_atm ? build_stencil(g, e->nb, e->rc_atm) : std::vector<StencilRow>();
-        std::vector<int4> all;
-        for (auto *v : {&e->st2, &e->stc, &e->sta})
-            for (auto &r : *v) all.push_back(make_int4(r.dy, r.dz, r.dxlo, r.dxhi));
-        e->st_dev.ensure(all.size());
-        D3_CUDA(cudaMemcpy(e->st_dev.p, all.data(), sizeof(int4) * all.size(), cudaMemcpyHostToDevice));
-        const int nbins = e->nb[0] * e->nb[1] * e->nb[2];
-        e->bin_cnt.ensure(nbins);
-        e->bin_fill.ensure(nbins);
-        e->bin_start.ensure(nbins + 1);
+        for (int i = 0; i < 9; ++i) {
+            e->first_cell[i] = cell[i];
+            e->first_cell_f[i] = cell_f[i];
+        }
+        const uint64_t c = e->n;
+        build_structures(e, 1, &c, cell, cell_f);
+        e->cell_set = true;
+        return 0;
+    } catch (const std::exception &ex) {
+        e->cell_set = false;
+        err = ex.what();
+        return 1;
+    }
+}
+
+int engine_set_batch(Engine *e, uint64_t nstruct, const uint64_t *counts, const double *pos_bohr, const uint16_t *Z,
+                     const double *cells_bohr, const float *cells_f, std::string &err) {
+    try {
+        if (nstruct == 0 || nstruct > e->max_structs)
+            throw std::runtime_error("structure count " + std::to_string(nstruct) + " outside 1.." +
+                                     std::to_string(e->max_structs));
+        uint64_t n = 0;
+        for (uint64_t k = 0; k < nstruct; ++k) {
+            if (counts[k] == 0) throw std::runtime_error("structure without atoms");
+            n += counts[k];
+        }
+        if (n > e->max_atoms)
+            throw std::runtime_error(std::to_string(n) + " atoms exceed the handle capacity " + std::to_string(e->max_atoms));
+        std::vector<int> types = map_types(e, Z, n);
+        build_structures(e, (int)nstruct, counts, cells_bohr, cells_f);
+        D3_CUDA(cudaMemcpyAsync(e->pos_in.p, pos_bohr, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, e->stream));
+        D3_CUDA(cudaMemcpyAsync(e->type_in.p, types.data(), sizeof(int) * n, cudaMemcpyHostToDevice, e->stream));
+        D3_CUDA(cudaStreamSynchronize(e->stream));
+        e->n = n;
+        e->atoms_set = true;
         e->cell_set = true;
         return 0;
     } catch (const std::exception &ex) {
@@ -1233,23 +1396,41 @@ int engine_set_cell(Engine *e, const double cell[9], const float cell_f[9], std:
     }
 }
 
+__global__ void k_set_positions(double *pos_in, const double *coords_ang, int n3) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n3) pos_in[i] = coords_ang[i] * ANG2BOHR;
+}
+
+int engine_set_positions_device(Engine *e, const double *coords_ang_dev, cudaStream_t stream) {
+    if (!e->atoms_set) return 1;
+    const int n3 = (int)(3 * e->n);
+    k_set_positions<<<(n3 + 255) / 256, 256, 0, stream ? stream : e->stream>>>(e->pos_in.p, coords_ang_dev, n3);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+int engine_num_structures(const Engine *e) { return e->nstruct; }
+
+void engine_fetch_results(Engine *e, double *energies, double *forces, double *stresses) {
+    const size_t S = e->nstruct, n = e->n;
+    std::vector<double> h(10 * S + 3 * n);
+    D3_CUDA(cudaMemcpy(h.data(), e->out.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+    if (energies) memcpy(energies, h.data(), sizeof(double) * S);
+    if (forces) memcpy(forces, h.data() + S, sizeof(double) * 3 * n);
+    if (stresses) memcpy(stresses, h.data() + S + 3 * n, sizeof(double) * 9 * S);
+}
+
 static KP make_kp(Engine *e) {
     KP p;
     memset(&p, 0, sizeof(p));
     p.n = (int)e->n;
+    p.nstruct = e->nstruct;
+    p.nbins_total = e->nbins_total;
     p.ne = e->ne;
     p.nref = e->nref;
-    for (int i = 0; i < 9; ++i) {
-        p.h[i] = e->geom.h[i];
-        p.inv[i] = e->geom.inv[i];
-    }
-    p.vol = e->geom.volume;
-    for (int k = 0; k < 3; ++k) {
-        p.nb[k] = e->nb[k];
-        p.half[k] = (int)(e->mcb[k] / 2);
-    }
-    p.nbins = e->nb[0] * e->nb[1] * e->nb[2];
-    p.box_mode = e->box_mode ? 1 : 0;
+    p.sg = e->sg_dev.p;
+    p.sid_in = e->sid_in.p;
+    p.sid = e->sid.p;
+    p.stencils = e->st_dev.p;
     // cutoffs: the reference compares squared distances against rc*rc of its float cutoff
     p.rc2 = e->rc * e->rc;
     p.rcn2 = e->rc_cn * e->rc_cn;
@@ -1316,16 +1497,24 @@ static KP make_kp(Engine *e) {
     p.atm_ent = e->atm_ent.p;
     p.atm_cap = e->atm_cap;
     p.work = e->work.p;
-    p.st2 = e->st_dev.p;
-    p.nst2 = (int)e->st2.size();
-    p.stc = e->st_dev.p + e->st2.size();
-    p.nstc = (int)e->stc.size();
-    p.sta = e->st_dev.p + e->st2.size() + e->stc.size();
-    p.nsta = (int)e->sta.size();
     p.out = e->out.p;
     p.status = e->status.p;
     p.counters = e->counters.p;
     return p;
+}
+
+// dynamic shared memory attribute and occupancy of an ATM kernel, cached per kernel and
+// size so that evaluations inside a CUDA-graph capture make no such host calls
+static int atm_occupancy(Engine *e, int which, size_t sm, const void *fn) {
+    auto &c = e->atm_occ_cache[which];
+    if (c.fn == fn && c.sm == sm) return c.blocks;
+    D3_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int blocks = 0;
+    D3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, ATM_THREADS, sm));
+    c.fn = fn;
+    c.sm = sm;
+    c.blocks = std::max(1, blocks);
+    return c.blocks;
 }
 
 template <int NR>
@@ -1338,12 +1527,12 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     cudaEvent_t *ev = e->ev;
     D3_CUDA(cudaEventRecord(ev[0], s));
     D3_CUDA(cudaMemsetAsync(p.counters, 0, sizeof(unsigned long long) * 4, s));
-    D3_CUDA(cudaMemsetAsync(p.bin_cnt, 0, sizeof(int) * p.nbins, s));
-    D3_CUDA(cudaMemsetAsync(p.bin_fill, 0, sizeof(int) * p.nbins, s));
+    D3_CUDA(cudaMemsetAsync(p.bin_cnt, 0, sizeof(int) * p.nbins_total, s));
+    D3_CUDA(cudaMemsetAsync(p.bin_fill, 0, sizeof(int) * p.nbins_total, s));
     k_bin<<<gb, T, 0, s>>>(p);
-    k_scan<int, int><<<1, 1024, 0, s>>>(p.bin_cnt, p.bin_start, p.nbins);
+    k_scan<int, int><<<1, 1024, 0, s>>>(p.bin_cnt, p.bin_start, p.nbins_total);
     k_scatter<<<gb, T, 0, s>>>(p);
-    k_binsort<<<(p.nbins + T - 1) / T, T, 0, s>>>(p);
+    k_binsort<<<(p.nbins_total + T - 1) / T, T, 0, s>>>(p);
     k_gather<<<gb, T, 0, s>>>(p);
     D3_CUDA(cudaEventRecord(ev[1], s));
     if (p.precision)
@@ -1376,24 +1565,24 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
             const size_t fixed = (size_t)p.ne * NR * sizeof(double) + ((p.ne * p.ne + 1) & ~1) * sizeof(float) +
                                  ATM_PERM_CAP * sizeof(unsigned short) + 16;
             const size_t per = sizeof(Partner32) + (size_t)p.ne * NR * sizeof(float);
-            const int tile = (int)std::max<size_t>(8, std::min<size_t>(128, (100 * 1024 - fixed) / per)) & ~1;
+            const int tmax = (int)std::max<size_t>(8, std::min<size_t>(256, (100 * 1024 - fixed) / per)) & ~1;
+            const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(8, e->opt.atm_tile & ~1)) : std::min(tmax, 128);
             const size_t sm = (size_t)tile * per + fixed;
-            D3_CUDA(cudaFuncSetAttribute(k_atm32<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            int blocks_per_sm = 0;
-            D3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_atm32<NR>, ATM_THREADS, sm));
-            const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, blocks_per_sm)));
+            const int blocks_per_sm = atm_occupancy(e, 1, sm, (const void *)k_atm32<NR>);
+            const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
+            const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, per_sm)));
             k_atm32<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
         } else {
             // partner tile: as many entries as fit in ~160 KB next to the apex tables
             const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double) +
                                  ATM_PERM_CAP * sizeof(unsigned short);
             const size_t per = sizeof(Partner) + (size_t)p.ne * NR * sizeof(double);
-            const int tile = (int)std::max<size_t>(8, std::min<size_t>(128, (160 * 1024 - fixed) / per));
+            const int tmax = (int)std::max<size_t>(8, std::min<size_t>(256, (160 * 1024 - fixed) / per));
+            const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(8, e->opt.atm_tile)) : std::min(tmax, 128);
             const size_t sm = (size_t)tile * per + fixed;
-            D3_CUDA(cudaFuncSetAttribute(k_atm<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            int blocks_per_sm = 0;
-            D3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_atm<NR>, ATM_THREADS, sm));
-            const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, blocks_per_sm)));
+            const int blocks_per_sm = atm_occupancy(e, 0, sm, (const void *)k_atm<NR>);
+            const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
+            const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, per_sm)));
             k_atm<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
         }
     }
@@ -1405,7 +1594,7 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
         k_chain<<<gw, T, 0, s>>>(p, e->G.p);
     D3_CUDA(cudaEventRecord(ev[6], s));
     k_forces_out<<<gb, T, 0, s>>>(p);
-    k_reduce<<<1, 1024, 0, s>>>(p);
+    k_reduce<<<p.nstruct, 256, 0, s>>>(p);
     D3_CUDA(cudaEventRecord(ev[7], s));
     e->have_events = true;
     D3_CUDA(cudaGetLastError());
@@ -1511,10 +1700,15 @@ uint16_t engine_compute(Engine *e, double *energy, double *forces, double *stres
     try {
         const uint64_t n = e->n;
         if (e->use_atm && e->atm_cap == 0) {
-            // initial list capacity from the density of the half sphere, with margin
-            const double rho = (double)n / std::fabs(e->geom.volume);
-            const double k_half = 0.5 * rho * 4.18879020478639 * e->rc_atm * e->rc_atm * e->rc_atm;
-            e->atm_cap = (long long)(n * (k_half * 1.25 + 64.0));
+            // initial list capacity from each structure's density over the half sphere
+            double cap = 0.0;
+            for (int k = 0; k < e->nstruct; ++k) {
+                const double nk = (double)e->sg[k].natoms;
+                const double rho = nk / std::fabs(e->geoms[k].volume);
+                const double k_half = 0.5 * rho * 4.18879020478639 * e->rc_atm * e->rc_atm * e->rc_atm;
+                cap += nk * (k_half * 1.25 + 64.0);
+            }
+            e->atm_cap = (long long)cap + 1024;
             e->atm_ent.ensure((size_t)e->atm_cap);
         }
         for (int attempt = 0; attempt < 4; ++attempt) {
@@ -1535,12 +1729,14 @@ uint16_t engine_compute(Engine *e, double *energy, double *forces, double *stres
                 e->atm_ent.ensure((size_t)e->atm_cap);
                 continue;
             }
-            const size_t nout = 1 + 3 * n + 9;
+            const size_t S = e->nstruct;
+            const size_t nout = 10 * S + 3 * n;
             D3_CUDA(cudaMemcpyAsync(e->host_out.data(), e->out.p, sizeof(double) * nout, cudaMemcpyDeviceToHost, s));
             D3_CUDA(cudaStreamSynchronize(s));
-            if (energy) *energy = e->host_out[0];
-            if (forces) memcpy(forces, e->host_out.data() + 1, sizeof(double) * 3 * n);
-            if (stress) memcpy(stress, e->host_out.data() + 1 + 3 * n, sizeof(double) * 9);
+            // energies [S], forces [3n], stresses [9S]
+            if (energy) memcpy(energy, e->host_out.data(), sizeof(double) * S);
+            if (forces) memcpy(forces, e->host_out.data() + S, sizeof(double) * 3 * n);
+            if (stress) memcpy(stress, e->host_out.data() + S + 3 * n, sizeof(double) * 9 * S);
             return (uint16_t)st;
         }
         return ST_LIST_OVERFLOW;
@@ -1617,7 +1813,7 @@ int engine_debug_bins(Engine *e, int64_t *wrap_shift, int64_t *bin_index, int nb
         if (bin_index) bin_index[i] = b[i];
     }
     if (nb_out)
-        for (int k = 0; k < 3; ++k) nb_out[k] = e->nb[k];
+        for (int k = 0; k < 3; ++k) nb_out[k] = e->sg.empty() ? 0 : e->sg[0].nb[k];
     return 0;
 }
 

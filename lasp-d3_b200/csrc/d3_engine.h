@@ -44,25 +44,39 @@ struct Options {
     bool smooth_cn = false;        // tanh^3 CN cutoff (reference SMOOTH_CUTOFF_CN)
     int precision = 0;             // 0: FP64 plain form; 1: FP32 pair/triplet arithmetic with
                                    // FP64 weights, dE/dCN and reductions (precision form)
+    // tunables (set by the autotuner or the caller)
+    double bin_divisor = 6.0;      // bin width = smallest cutoff / bin_divisor
+    int atm_tile = 0;              // ATM partner tile entries (0: largest that fits, <= 128)
+    int atm_ctas_per_sm = 0;       // persistent ATM CTAs per SM (0: occupancy limit)
 };
 
 struct Engine;
 
 Engine *engine_create(const uint16_t *elements, uint64_t n_elements, uint64_t max_atoms, double rc, double rc_cn,
-                      double rc_atm, bool use_atm, int damping, int functional, bool extended, std::string &err);
+                      double rc_atm, bool use_atm, int damping, int functional, bool extended, std::string &err,
+                      uint64_t max_structs = 1);
 void engine_destroy(Engine *e);
 int engine_set_atoms(Engine *e, const double *pos_bohr, const uint16_t *Z, uint64_t n, std::string &err);
 int engine_set_cell(Engine *e, const double cell_bohr[9], const float cell_bohr_f[9], std::string &err);
+// many independent structures in one handle: counts[k] atoms each, concatenated
+// positions (bohr), elements and cells (bohr, 9 per structure)
+int engine_set_batch(Engine *e, uint64_t nstruct, const uint64_t *counts, const double *pos_bohr, const uint16_t *Z,
+                     const double *cells_bohr, const float *cells_f, std::string &err);
+// replace positions from device memory (Angstrom, caller order; same atoms), stream-ordered
+int engine_set_positions_device(Engine *e, const double *coords_ang_dev, cudaStream_t stream);
+int engine_num_structures(const Engine *e);
+// copy the device results of the last evaluation (caller synchronises its stream first)
+void engine_fetch_results(Engine *e, double *energies, double *forces, double *stresses);
 void engine_set_options(Engine *e, const Options &o);
 Options engine_get_options(const Engine *e);
 void engine_set_functional_params(Engine *e, const FuncParams &p);
 // Runs the whole evaluation on `stream` (the engine's own stream when null) and,
-// when sync is true, waits and copies results to the host outputs (eV, eV/A, eV/A^3,
-// caller's atom order). Returns the status word.
+// when sync is true, waits and copies results to the host outputs: energies [S] (eV),
+// forces [3n] (eV/A, caller order), stresses [9S] (eV/A^3). Returns the status word.
 uint16_t engine_compute(Engine *e, double *energy_ev, double *forces_ev_a, double *stress_ev_a3,
                         cudaStream_t stream, bool sync);
 // device-resident results of the last evaluation (eV units, caller order)
-const double *engine_device_results(const Engine *e); // [1 + 3n + 9]
+const double *engine_device_results(const Engine *e); // [S energies, 3n forces, 9S stresses]
 uint64_t engine_num_atoms(const Engine *e);
 
 // per-pass device times (ms) of the last evaluation, from CUDA events on its stream:

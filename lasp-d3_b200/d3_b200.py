@@ -22,6 +22,7 @@ HEADER = os.path.join(HERE, "..", "include", "d3.h")
 
 ZERO_DAMPING, BJ_DAMPING = 0, 1
 OPT_ATM_FORCE_SCALED, OPT_SMOOTH_CN, OPT_PRECISION = 1, 2, 3
+OPT_BIN_DIVISOR, OPT_ATM_TILE, OPT_ATM_CTAS_PER_SM = 4, 5, 6
 TABLE_5REF, TABLE_7REF = 0, 1
 
 _lib = None
@@ -71,6 +72,18 @@ def load_library(path=None):
     lib.d3_compute_async.argtypes = [vp, vp]
     lib.d3_device_results.restype = vp
     lib.d3_device_results.argtypes = [vp]
+    lib.d3_init_batch.restype = vp
+    lib.d3_init_batch.argtypes = [vp, u64, u64, u64, f64, f64, f64, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    lib.d3_set_batch_f64.restype = ctypes.c_int
+    lib.d3_set_batch_f64.argtypes = [vp, u64, vp, vp, vp, vp]
+    lib.d3_compute_batch_f64.restype = ctypes.c_uint16
+    lib.d3_compute_batch_f64.argtypes = [vp, vp, vp, vp]
+    lib.d3_fetch_results.restype = ctypes.c_int
+    lib.d3_fetch_results.argtypes = [vp, vp, vp, vp]
+    lib.d3_num_structures.restype = ctypes.c_int
+    lib.d3_num_structures.argtypes = [vp]
+    lib.d3_set_positions_device.restype = ctypes.c_int
+    lib.d3_set_positions_device.argtypes = [vp, vp, vp]
     lib.d3_pass_times.restype = ctypes.c_int
     lib.d3_pass_times.argtypes = [vp, vp, ctypes.c_int, vp]
     lib.d3_launches_per_eval.restype = ctypes.c_int
@@ -161,6 +174,12 @@ class D3:
             raise RuntimeError("d3_compute_f64 status %d: %s" % (st, self.lib.d3_last_error().decode()))
         return float(e[0]), f, s.reshape(3, 3)
 
+    def set_positions_device(self, ptr, stream_ptr=None):
+        """Positions from device memory (double [n,3], Angstrom), stream-ordered."""
+        if self.lib.d3_set_positions_device(self.h, ctypes.c_void_p(ptr),
+                                            ctypes.c_void_p(stream_ptr) if stream_ptr else None):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+
     def pass_times(self):
         """Device ms per pass of the last evaluation and the work counters."""
         ms = np.zeros(8, np.float32)
@@ -175,6 +194,15 @@ class D3:
     def compute_async(self, stream_ptr=None):
         """Enqueue one evaluation on a CUDA stream (int handle or None); no host sync."""
         return int(self.lib.d3_compute_async(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def fetch_results(self):
+        """Results of the last (asynchronous) evaluation; synchronise its stream first."""
+        e = np.zeros(1)
+        f = np.zeros((self.n, 3))
+        s = np.zeros(9)
+        if self.lib.d3_fetch_results(self.h, _ptr(e), _ptr(f), _ptr(s)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+        return float(e[0]), f, s.reshape(3, 3)
 
     def device_results_ptr(self):
         return self.lib.d3_device_results(self.h)
@@ -196,6 +224,67 @@ class D3:
         nb = np.zeros(3, np.int32)
         self.lib.d3_debug_bins(self.h, _ptr(sh), _ptr(b), _ptr(nb))
         return sh, b, nb
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.free_d3_handle(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class D3Batch:
+    """Many independent periodic structures in one handle (batching form)."""
+
+    def __init__(self, elements, max_structures, max_total_atoms, rc=95.0, rc_cn=40.0, rc_atm=None,
+                 damping=BJ_DAMPING, functional=0, table=TABLE_5REF):
+        self.lib = load_library()
+        el = np.ascontiguousarray(sorted(set(int(z) for z in elements)), np.uint16)
+        self.h = self.lib.d3_init_batch(_ptr(el), len(el), int(max_structures), int(max_total_atoms), float(rc),
+                                        float(rc_cn), float(rc_atm) if rc_atm else 0.0, int(damping),
+                                        int(functional), int(table))
+        if not self.h:
+            raise RuntimeError("d3_init_batch failed: %s" % self.lib.d3_last_error().decode())
+        self.counts = None
+
+    def set_option(self, opt, value):
+        if self.lib.d3_set_option(self.h, int(opt), int(value)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+
+    def set_structures(self, structures):
+        """structures: list of dicts with pos [n,3], Z [n], cell [3,3] (Angstrom)."""
+        counts = np.array([len(s["Z"]) for s in structures], np.uint64)
+        pos = np.ascontiguousarray(np.concatenate([s["pos"] for s in structures]), np.float64)
+        z = np.ascontiguousarray(np.concatenate([s["Z"] for s in structures]), np.uint16)
+        cells = np.ascontiguousarray(np.stack([np.asarray(s["cell"], np.float64).reshape(9) for s in structures]))
+        if self.lib.d3_set_batch_f64(self.h, len(counts), _ptr(counts), _ptr(pos), _ptr(z), _ptr(cells)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+        self.counts = counts
+
+    def compute(self, check=True):
+        S, n = len(self.counts), int(self.counts.sum())
+        e = np.zeros(S)
+        f = np.zeros((n, 3))
+        s = np.zeros((S, 9))
+        st = self.lib.d3_compute_batch_f64(self.h, _ptr(e), _ptr(f), _ptr(s))
+        if check and st != 0:
+            raise RuntimeError("d3_compute_batch_f64 status %d: %s" % (st, self.lib.d3_last_error().decode()))
+        off = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        return e, [f[off[k]:off[k + 1]] for k in range(S)], s.reshape(S, 3, 3)
+
+    def compute_async(self, stream_ptr=None):
+        return int(self.lib.d3_compute_async(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def pass_times(self):
+        ms = np.zeros(8, np.float32)
+        cnt = np.zeros(4, np.uint64)
+        k = self.lib.d3_pass_times(self.h, _ptr(ms), 8, _ptr(cnt))
+        names = ["bin", "cn", "twobody", "atm_list", "atm", "chain", "finalize"]
+        return dict(zip(names, ms[:k].tolist())), cnt
 
     def close(self):
         if getattr(self, "h", None):
