@@ -128,8 +128,14 @@ def random_box(n, cell, composition=MIX_HCNOCU, seed=1, rmin=1.0, chunk=None):
         cand = cand[~drop]
         acc = np.concatenate([acc, cand[: n - len(acc)]])
     pos = acc @ cell
-    counts = [int(round(frac * n)) for _, frac in composition]
-    counts[0] += n - sum(counts)
+    # largest-remainder apportionment of n atoms over the composition fractions
+    frac = np.array([f for _, f in composition], float)
+    frac = frac / frac.sum()
+    raw = frac * n
+    counts = np.floor(raw).astype(int)
+    for k in np.argsort(-(raw - counts))[: n - counts.sum()]:
+        counts[k] += 1
+    counts = counts.tolist()
     Z = np.concatenate([np.full(c, Z_OF[s]) for (s, _), c in zip(composition, counts)])
     rng.shuffle(Z)
     return {"pos": pos, "Z": Z, "cell": cell}

@@ -36,11 +36,14 @@ def test_batch_equals_single_handles(precision):
     b.set_structures(sts)
     e, f, st = b.compute()
     b.close()
+    # FP64: equal to rounding; FP32 arithmetic: lane assignment of the ATM entries varies
+    # between launches, so FP32 partial sums differ in their last bits
+    etol, ftol, stol = (1e-12, 1e-11, 1e-12) if precision == 0 else (1e-8, 1e-7, 1e-9)
     for k, s in enumerate(sts):
         e1, f1, s1 = single(s, precision)
-        assert abs(e[k] - e1) <= 1e-12 * abs(e1) + 1e-14
-        assert np.abs(f[k] - f1).max() <= 1e-11
-        assert np.abs(st[k] - s1).max() <= 1e-12
+        assert abs(e[k] - e1) <= etol * abs(e1) + 1e-14
+        assert np.abs(f[k] - f1).max() <= ftol
+        assert np.abs(st[k] - s1).max() <= stol
 
 
 def test_batch_matches_oracle():

@@ -48,9 +48,11 @@ def test_graph_replay_matches_direct_evaluation(precision):
         e, f, s = d.fetch_results()
         ref.set_atoms(cur, sys_["Z"])
         e1, f1, s1 = ref.compute()
-        assert abs(e - e1) <= 1e-11 * abs(e1)
-        assert np.abs(f - f1).max() <= 1e-10
-        assert np.abs(s - s1).max() <= 1e-12
+        # FP64: equal to rounding; FP32 arithmetic: last-bit differences of partial sums
+        etol, ftol, stol = (1e-11, 1e-10, 1e-12) if precision == 0 else (1e-8, 1e-7, 1e-9)
+        assert abs(e - e1) <= etol * abs(e1)
+        assert np.abs(f - f1).max() <= ftol
+        assert np.abs(s - s1).max() <= stol
     del graph
     ref.close()
     d.close()
