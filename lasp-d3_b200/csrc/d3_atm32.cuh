@@ -1,34 +1,41 @@
 // ATM three-body kernel, precision form: the per-visit triplet arithmetic in FP32.
 // Same enumeration, schedule, weights and mirror-symmetric accumulation as k_atm
 // (d3_atm.cuh); per-entry set-up (C6 of the apex pairs, damping ratios) is done in FP64
-// and rounded once. Per-visit sums are kept in FP32 within one partner tile and carried
-// across tiles in FP64 (blocked summation, error ~ sqrt(tile) * eps_32 per block); the
-// dE/dCN sum is accumulated in FP64 per visit.
+// and rounded once. Per-visit sums, dE/dCN included, are kept in FP32 within one
+// partner tile and carried across tiles in FP64 (blocked summation, error
+// ~ sqrt(tile) * eps_32 per block).
+//
+// Layout for few instructions per visit: partner records as two float4 and one int2
+// (three wide shared-memory loads), C6 rows padded to 8 floats (two 16-byte loads),
+// 32-bit in-range masks over tiles padded to a multiple of 32 with far-away dummies.
 
-struct Partner32 {
-    float vx, vy, vz, d2, ir, id2, s, g;
-    int j, t;
-};
+constexpr int ATM32_NRP = 8; // padded C6 row length (NR <= 7)
 
 template <int NR>
 __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) unsigned char smem32[];
     const int ne = p.ne;
-    Partner32 *ptile = reinterpret_cast<Partner32 *>(smem);
-    float *ytile = reinterpret_cast<float *>(ptile + tile);    // [tile][ne][NR]
-    double *yapex = reinterpret_cast<double *>(ytile + (((size_t)tile * ne * NR + 1) & ~(size_t)1)); // [ne][NR]
+    const int tilep = (tile + 31) & ~31;
+    float4 *pA = reinterpret_cast<float4 *>(smem32);       // [tilep] vx vy vz d2
+    float4 *pB = pA + tilep;                                // [tilep] ir id2 s g
+    int2 *pC = reinterpret_cast<int2 *>(pB + tilep);        // [tilep] j t
+    float4 *ytile = reinterpret_cast<float4 *>(pC + tilep); // [tilep][ne][2]: C6 row, padded to 8
+    double *yapex = reinterpret_cast<double *>(ytile + (size_t)tilep * ne * 2); // [ne][NR]
     float *r0sq = reinterpret_cast<float *>(yapex + ne * NR); // [ne][ne]
-    unsigned short *perm = reinterpret_cast<unsigned short *>(r0sq + ((ne * ne + 1) & ~1)); // [ATM_PERM_CAP]
+    unsigned short *perm = reinterpret_cast<unsigned short *>(r0sq + ((ne * ne + 3) & ~3)); // [ATM_PERM_CAP]
+    // per-thread FP64 carries of the entry sums, touched once per partner tile, kept in
+    // shared memory to save registers: [11][blockDim]
+    double *carry = reinterpret_cast<double *>(perm + ATM_PERM_CAP);
     __shared__ int s_item;
     __shared__ int shell_cnt[ATM_SHELLS], shell_off[ATM_SHELLS];
     __shared__ double red[ATM_THREADS / 32][12];
     const int tid = threadIdx.x;
     if (p.atm_off[p.n] > p.atm_cap) return; // list overflowed: the host grows it and re-runs
     for (int k = tid; k < ne * ne; k += blockDim.x) r0sq[k] = (float)(p.r0ab[k] * p.r0ab[k]);
-    const double x16c_d = 4294967296.0 / 43046721.0; // (4/3)^16
-    const float x16c = (float)x16c_d;
+    const float x16c = (float)(4294967296.0 / 43046721.0); // (4/3)^16
     const float third = 1.0f / 3.0f;
     const float ratm2f = (float)p.ratm2;
+    const bool force_scaled = p.atm_force_scaled != 0;
     const double inv_rc = 1.0 / sqrt(p.ratm2);
     unsigned long long visits = 0;
     while (true) {
@@ -81,15 +88,19 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
             }
         }
         __syncthreads();
-        double ea = 0, ga = 0, fax = 0, fay = 0, faz = 0;
-        double vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+        const int B = blockDim.x;
+        double apex[11];
+#pragma unroll
+        for (int k = 0; k < 11; ++k) apex[k] = 0.0;
         for (int q0 = 0; q0 < m; q0 += blockDim.x) {
             const int qi = q0 + tid;
             const bool active = qi < m;
             const int q = active ? (sorted ? (int)perm[qi] : qi) : -1;
             double vqx_d = 0, vqy_d = 0, vqz_d = 0, lam_qa = 0, lam_aq = 0;
             float vqx = 0.f, vqy = 0.f, vqz = 1e30f, d1 = 1.f, ir1 = 1.f, id1 = 1.f, sq = 0.f, gq = 0.f;
-            float wq[NR], dwq[NR];
+            float wq[ATM32_NRP], dwq[ATM32_NRP];
+#pragma unroll
+            for (int b = 0; b < ATM32_NRP; ++b) wq[b] = dwq[b] = 0.f;
             int jq = -1, tq = 0;
             if (active) {
                 const int2 ent = p.atm_ent[e0 + q];
@@ -130,15 +141,20 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
                 lam_aq = dca / c6;
                 lam_qa = dcq / c6;
                 gq = (float)pow((double)r0sq[ta * ne + tq] / d1d, 8.0 / 3.0);
-            } else {
-#pragma unroll
-                for (int b = 0; b < NR; ++b) wq[b] = dwq[b] = 0.f;
             }
-            double Esum = 0, Dsum = 0, Ssum = 0, Ux = 0, Uy = 0, Uz = 0, Fsum = 0, Wx = 0, Wy = 0, Wz = 0, Asum = 0;
+            const bool qa = (jq == a);
+#pragma unroll
+            for (int k = 0; k < 11; ++k) carry[k * B + tid] = 0.0;
             for (int p0 = 0; p0 < m; p0 += tile) {
                 const int cnt = min(tile, m - p0);
+                const int cntp = (cnt + 31) & ~31;
                 __syncthreads();
-                for (int k = tid; k < cnt; k += blockDim.x) {
+                for (int k = tid; k < cntp; k += blockDim.x) {
+                    if (k >= cnt) {
+                        // padding: far-away dummies fail every distance test
+                        pA[k] = make_float4(1e30f, 1e30f, 1e30f, 1.f);
+                        continue;
+                    }
                     const int pi = p0 + k;
                     const int2 ent = p.atm_ent[e0 + (sorted ? (int)perm[pi] : pi)];
                     const int jp = ent.x;
@@ -153,138 +169,140 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
                     double c6 = 0;
 #pragma unroll
                     for (int b = 0; b < NR; ++b) c6 += ya[b] * p.w[(size_t)jp * NR + b];
-                    Partner32 pr;
-                    pr.vx = (float)vx;
-                    pr.vy = (float)vy;
-                    pr.vz = (float)vz;
-                    pr.d2 = (float)d2;
-                    pr.ir = (float)(1.0 / sqrt(d2));
-                    pr.id2 = (float)(1.0 / d2);
-                    pr.s = (float)sqrt(c6);
-                    pr.g = (float)pow((double)r0sq[ta * ne + tp] / d2, 8.0 / 3.0);
-                    pr.j = jp;
-                    pr.t = tp;
-                    ptile[k] = pr;
+                    pA[k] = make_float4((float)vx, (float)vy, (float)vz, (float)d2);
+                    pB[k] = make_float4((float)(1.0 / sqrt(d2)), (float)(1.0 / d2), (float)sqrt(c6),
+                                        (float)pow((double)r0sq[ta * ne + tp] / d2, 8.0 / 3.0));
+                    pC[k] = make_int2(jp, tp);
                     const float *ysrc = p.Y32 + (size_t)jp * ne * NR;
-                    float *ydst = ytile + (size_t)k * ne * NR;
-                    for (int u2 = 0; u2 < ne * NR; ++u2) ydst[u2] = ysrc[u2];
+                    float *ydst = reinterpret_cast<float *>(ytile + (size_t)k * ne * 2);
+                    for (int t = 0; t < ne; ++t)
+#pragma unroll
+                        for (int b = 0; b < ATM32_NRP; ++b) ydst[t * ATM32_NRP + b] = b < NR ? ysrc[t * NR + b] : 0.f;
                 }
                 __syncthreads();
-                float tE = 0.f, tS = 0.f, tUx = 0.f, tUy = 0.f, tUz = 0.f, tF = 0.f, tWx = 0.f, tWy = 0.f, tWz = 0.f,
-                      tA = 0.f;
-                for (int s0 = 0; s0 < cnt; s0 += 64) {
-                    unsigned long long mask = 0ull;
-                    const int sc = min(64, cnt - s0);
-                    for (int k = 0; k < sc; ++k) {
-                        const Partner32 &pr = ptile[s0 + k];
-                        const float dx = vqx - pr.vx, dy = vqy - pr.vy, dz = vqz - pr.vz;
+                float tE = 0.f, tD = 0.f, tS = 0.f, tUx = 0.f, tUy = 0.f, tUz = 0.f, tF = 0.f, tWx = 0.f, tWy = 0.f,
+                      tWz = 0.f, tA = 0.f;
+                for (int s0 = 0; s0 < cntp; s0 += 32) {
+                    // in-range mask over 32 partners (upper bound only; the exact test is below)
+                    unsigned mask = 0u;
+#pragma unroll 4
+                    for (int k = 0; k < 32; ++k) {
+                        const float4 pa = pA[s0 + k];
+                        const float dx = vqx - pa.x, dy = vqy - pa.y, dz = vqz - pa.z;
                         const float d3 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        if (d3 <= ratm2f && d3 >= 1e-12f) mask |= 1ull << k;
+                        mask |= (d3 <= ratm2f) ? (1u << k) : 0u;
                     }
-                    while (__any_sync(0xffffffffu, mask != 0ull)) {
-                        if (mask == 0ull) continue;
-                        const int k = s0 + __ffsll((long long)mask) - 1;
-                        mask &= mask - 1ull;
-                        const Partner32 &pr = ptile[k];
-                        ++visits;
-                        const float rx = vqx - pr.vx, ry = vqy - pr.vy, rz = vqz - pr.vz;
+                    while (__any_sync(0xffffffffu, mask != 0u)) {
+                        if (mask == 0u) continue;
+                        const int k = s0 + __ffs(mask) - 1;
+                        mask &= mask - 1u;
+                        const float4 pa = pA[k];
+                        const float rx = vqx - pa.x, ry = vqy - pa.y, rz = vqz - pa.z;
                         const float d3 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+                        if (d3 < 1e-12f) continue; // the entry itself
+                        ++visits;
+                        const float4 pb = pB[k];
+                        const int2 pc = pC[k];
                         const float ir3 = rsqrtf(d3);
                         const float id3 = ir3 * ir3;
-                        const float *yp = ytile + ((size_t)k * ne + tq) * NR;
-                        float c6 = 0.f, dc6 = 0.f;
-#pragma unroll
-                        for (int b = 0; b < NR; ++b) {
-                            const float y = yp[b];
-                            c6 = fmaf(y, wq[b], c6);
-                            dc6 = fmaf(y, dwq[b], dc6);
+                        const float4 *yr = ytile + ((size_t)k * ne + tq) * 2;
+                        const float4 y0 = yr[0], y1 = yr[1];
+                        float c6 = y0.x * wq[0];
+                        float dc6 = y0.x * dwq[0];
+                        c6 = fmaf(y0.y, wq[1], c6);
+                        dc6 = fmaf(y0.y, dwq[1], dc6);
+                        c6 = fmaf(y0.z, wq[2], c6);
+                        dc6 = fmaf(y0.z, dwq[2], dc6);
+                        c6 = fmaf(y0.w, wq[3], c6);
+                        dc6 = fmaf(y0.w, dwq[3], dc6);
+                        c6 = fmaf(y1.x, wq[4], c6);
+                        dc6 = fmaf(y1.x, dwq[4], dc6);
+                        if (NR > 5) {
+                            c6 = fmaf(y1.y, wq[5], c6);
+                            dc6 = fmaf(y1.y, dwq[5], dc6);
+                            c6 = fmaf(y1.z, wq[6], c6);
+                            dc6 = fmaf(y1.z, dwq[6], dc6);
                         }
                         const float is3 = rsqrtf(c6);
                         const float s3 = c6 * is3;
                         const float lam_xy = dc6 * is3 * is3;
-                        const float u = r0sq[tq * ne + pr.t] * id3;
+                        const float u = r0sq[tq * ne + pc.y] * id3;
                         const float g3 = u * u * u * exp2f(__log2f(u) * (-1.0f / 3.0f));
-                        const bool same = (jq == pr.j), qa = (jq == a), pa = (pr.j == a);
-                        float w, wf;
-                        if (same) {
-                            w = qa ? third : 1.0f;
-                            wf = 2.0f;
-                        } else if (qa || pa) {
-                            w = 0.5f;
-                            wf = 1.0f;
-                        } else {
-                            w = 1.0f;
-                            wf = 1.0f;
-                        }
-                        if (p.atm_force_scaled) wf = w;
-                        const float d2 = pr.d2;
-                        const float irsq = id1 * pr.id2 * id3;
-                        const float ir9 = irsq * ir1 * pr.ir * ir3;
+                        // reference scale factors (src/d3_kernel.cu:1282-1290) as pair weights
+                        const bool same = (jq == pc.x);
+                        const bool apex_img = qa | (pc.x == a);
+                        const float w = same ? (qa ? third : 1.0f) : (apex_img ? 0.5f : 1.0f);
+                        const float wf = force_scaled ? w : (same ? 2.0f : 1.0f);
+                        const float d2 = pa.w;
+                        const float irsq = id1 * pb.y * id3;
+                        const float ir9 = irsq * ir1 * pb.x * ir3;
                         const float t1 = d1 + d2 - d3, t2 = d1 - d2 + d3, t3 = -d1 + d2 + d3;
                         const float t12 = t1 * t2, t13 = t1 * t3, t23 = t2 * t3;
                         const float P = t12 * t3;
                         const float A = fmaf(0.375f * P, irsq, 1.0f) * ir9;
                         const float q52 = ir9 * irsq;
                         const float Q3 = 3.0f * d1 * d2 * d3;
-                        const float dang1 = q52 * fmaf(-0.75f * d1, t23 + t13 - t12, fmaf(1.875f, P, Q3));
-                        const float dang3 = q52 * fmaf(-0.75f * d3, t13 + t12 - t23, fmaf(1.875f, P, Q3));
-                        const float x16 = x16c * gq * pr.g * g3;
+                        const float base = fmaf(1.875f, P, Q3);
+                        const float dang1 = q52 * fmaf(-0.75f * d1, t23 + t13 - t12, base);
+                        const float dang3 = q52 * fmaf(-0.75f * d3, t13 + t12 - t23, base);
+                        const float x16 = x16c * gq * pb.w * g3;
                         const float fd = __fdividef(1.0f, fmaf(6.0f, x16, 1.0f));
                         const float dfd = 32.0f * x16 * fd * fd;
-                        const float C9 = -sq * pr.s * s3;
+                        const float C9 = -sq * pb.z * s3;
                         const float Et = C9 * A * fd;
                         const float Adfd = A * dfd;
                         const float f1 = -C9 * fmaf(dang1, fd, -Adfd) * id1;
                         const float f3 = -C9 * fmaf(dang3, fd, -Adfd) * id3;
                         const float wE = w * Et;
                         tE += wE;
-                        Dsum = fma((double)wE, (double)lam_xy, Dsum);
+                        tD = fmaf(wE, lam_xy, tD);
                         const float w3 = w * f3;
                         tS = fmaf(w, f1 + f3, tS);
-                        tUx = fmaf(w3, pr.vx, tUx);
-                        tUy = fmaf(w3, pr.vy, tUy);
-                        tUz = fmaf(w3, pr.vz, tUz);
+                        tUx = fmaf(w3, pa.x, tUx);
+                        tUy = fmaf(w3, pa.y, tUy);
+                        tUz = fmaf(w3, pa.z, tUz);
                         const float ff3 = wf * f3;
                         tF = fmaf(wf, f1 + f3, tF);
-                        tWx = fmaf(ff3, pr.vx, tWx);
-                        tWy = fmaf(ff3, pr.vy, tWy);
-                        tWz = fmaf(ff3, pr.vz, tWz);
+                        tWx = fmaf(ff3, pa.x, tWx);
+                        tWy = fmaf(ff3, pa.y, tWy);
+                        tWz = fmaf(ff3, pa.z, tWz);
                         tA = fmaf(wf, f1, tA);
                     }
                 }
                 // carry the tile's FP32 partial sums in FP64
-                Esum += tE;
-                Ssum += tS;
-                Ux += tUx;
-                Uy += tUy;
-                Uz += tUz;
-                Fsum += tF;
-                Wx += tWx;
-                Wy += tWy;
-                Wz += tWz;
-                Asum += tA;
+                const float tv[11] = {tE, tD, tS, tUx, tUy, tUz, tF, tWx, tWy, tWz, tA};
+#pragma unroll
+                for (int k = 0; k < 11; ++k) carry[k * B + tid] += (double)tv[k];
             }
             if (active) {
+                const double Esum = carry[0 * B + tid], Dsum = carry[1 * B + tid], Ssum = carry[2 * B + tid];
+                const double Ux = carry[3 * B + tid], Uy = carry[4 * B + tid], Uz = carry[5 * B + tid];
+                const double Fsum = carry[6 * B + tid], Wx = carry[7 * B + tid], Wy = carry[8 * B + tid],
+                             Wz = carry[9 * B + tid], Asum = carry[10 * B + tid];
                 const double third_d = 1.0 / 3.0;
                 atomicAdd(&p.eb[jq], Esum * third_d);
                 atomicAdd(&p.gb[jq], 0.5 * (lam_qa * Esum + Dsum));
                 atomicAdd(&p.fb[3 * jq], Fsum * vqx_d - Wx);
                 atomicAdd(&p.fb[3 * jq + 1], Fsum * vqy_d - Wy);
                 atomicAdd(&p.fb[3 * jq + 2], Fsum * vqz_d - Wz);
-                ea += 0.5 * Esum * third_d;
-                ga += 0.5 * lam_aq * Esum;
-                fax -= Asum * vqx_d;
-                fay -= Asum * vqy_d;
-                faz -= Asum * vqz_d;
-                vxx += Ssum * vqx_d * vqx_d - Ux * vqx_d;
-                vyy += Ssum * vqy_d * vqy_d - Uy * vqy_d;
-                vzz += Ssum * vqz_d * vqz_d - Uz * vqz_d;
-                vxy += Ssum * vqx_d * vqy_d - 0.5 * (Ux * vqy_d + Uy * vqx_d);
-                vxz += Ssum * vqx_d * vqz_d - 0.5 * (Ux * vqz_d + Uz * vqx_d);
-                vyz += Ssum * vqy_d * vqz_d - 0.5 * (Uy * vqz_d + Uz * vqy_d);
+                const double av[11] = {0.5 * Esum * third_d,
+                                       0.5 * lam_aq * Esum,
+                                       -Asum * vqx_d,
+                                       -Asum * vqy_d,
+                                       -Asum * vqz_d,
+                                       Ssum * vqx_d * vqx_d - Ux * vqx_d,
+                                       Ssum * vqy_d * vqy_d - Uy * vqy_d,
+                                       Ssum * vqz_d * vqz_d - Uz * vqz_d,
+                                       Ssum * vqx_d * vqy_d - 0.5 * (Ux * vqy_d + Uy * vqx_d),
+                                       Ssum * vqx_d * vqz_d - 0.5 * (Ux * vqz_d + Uz * vqx_d),
+                                       Ssum * vqy_d * vqz_d - 0.5 * (Uy * vqz_d + Uz * vqy_d)};
+#pragma unroll
+                for (int k = 0; k < 11; ++k) apex[k] += av[k];
             }
         }
-        double vals[11] = {ea, ga, fax, fay, faz, vxx, vyy, vzz, vxy, vxz, vyz};
+        double vals[11];
+#pragma unroll
+        for (int k = 0; k < 11; ++k) vals[k] = apex[k];
         const int lane = tid & 31, wid = tid >> 5;
 #pragma unroll
         for (int k = 0; k < 11; ++k) {

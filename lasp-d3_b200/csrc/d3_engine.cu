@@ -1562,11 +1562,11 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     if (e->use_atm) {
         D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
         if (p.precision) {
-            const size_t fixed = (size_t)p.ne * NR * sizeof(double) + ((p.ne * p.ne + 1) & ~1) * sizeof(float) +
-                                 ATM_PERM_CAP * sizeof(unsigned short) + 16;
-            const size_t per = sizeof(Partner32) + (size_t)p.ne * NR * sizeof(float);
-            const int tmax = (int)std::max<size_t>(8, std::min<size_t>(256, (100 * 1024 - fixed) / per)) & ~1;
-            const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(8, e->opt.atm_tile & ~1)) : std::min(tmax, 128);
+            const size_t fixed = (size_t)p.ne * NR * sizeof(double) + ((p.ne * p.ne + 3) & ~3) * sizeof(float) +
+                                 ATM_PERM_CAP * sizeof(unsigned short) + 11 * ATM_THREADS * sizeof(double);
+            const size_t per = 2 * sizeof(float4) + sizeof(int2) + (size_t)p.ne * 2 * sizeof(float4);
+            const int tmax = (int)std::max<size_t>(32, std::min<size_t>(256, (100 * 1024 - fixed) / per)) & ~31;
+            const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(32, e->opt.atm_tile & ~31)) : std::min(tmax, 128);
             const size_t sm = (size_t)tile * per + fixed;
             const int blocks_per_sm = atm_occupancy(e, 1, sm, (const void *)k_atm32<NR>);
             const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
