@@ -195,6 +195,65 @@ int d3_coordination_numbers_noalloc(const double *coords, const uint16_t *elemen
                                     const double cell[9], double cn_cutoff, int table, double *cn,
                                     void *cuda_stream);
 
+/* ---- Learned ATM surrogate (no counterpart in the reference) ----------------------
+   Per-atom ATM energy from an ensemble of MLPs over per-atom descriptors:
+     G_i[c][k] = sum over neighbours j of channel c within rc_ATM of
+                 C6_ij exp(-(r_ij - mu_k)^2 / (2 sigma^2)) (1 + cos(pi r_ij / rc_ATM)) / 2
+   with 32 centres mu_k uniform in 0.8 .. 21 A, sigma = 0.7 A, C6_ij the exact
+   CN-dependent coefficient. Network input: (G - mean) * inv_std, then a one-hot of the
+   atom's own channel. Each member: in -> 128 -> 128 -> 128 -> 1, SiLU, BF16 hidden
+   weights on the tensor cores, FP32 accumulation. E_i (eV) = e_scale * mean over members
+   + e_shift[channel of i]. Atoms whose ensemble standard deviation (population, eV)
+   exceeds the threshold (default 2e-4 eV) take their exact share instead: all triplets
+   through them, each weighted 1/3, by the exact ATM kernel. Forces, stress and dE/dCN
+   are the analytic derivatives of that energy (forces = -dE/dx, so repeated-index
+   triplets are force-scaled in the fallback share).
+
+   Parameter vector of one member (FP32, d3_mlp_layout gives the offsets):
+     W1[in_pad][128] b1[128] W2[128][128] b2[128] W3[128][128] b3[128] w4[128] b4
+   with in_pad = 16-aligned (33 * nch), W[in][out] (row = input). */
+#define D3_OPT_ATM_SURROGATE 7 /* d3_set_option value 1: evaluate ATM through the surrogate */
+int d3_set_surrogate(d3_handle_t *handle, const int *channel_z, int n_channels, int members, const float *params,
+                     const float *mean, const float *inv_std, const float *e_shift, float e_scale);
+int d3_set_surrogate_threshold(d3_handle_t *handle, double std_threshold_ev);
+/* atoms that took the exact fallback in the last evaluation */
+int d3_surrogate_flagged(d3_handle_t *handle);
+/* After an evaluation: descriptors of the handle's atoms for the given channels, in
+   the caller's atom order, into device memory: G_dev [n][32 * n_channels] (float),
+   center_dev [n] (channel of each atom, -1 if none), e_atm_dev [n] (double, eV: the
+   per-atom ATM energy of the last evaluation, one third of every triplet through the
+   atom). Any output may be NULL. */
+int d3_surrogate_descriptors(d3_handle_t *handle, const int *channel_z, int n_channels, float *G_dev,
+                             int *center_dev, double *e_atm_dev, void *cuda_stream);
+
+/* Network kernels on caller device buffers (training and standalone evaluation).
+   d3_mlp_layout: out[12] = in_dim, in_pad, oW1, ob1, oW2, ob2, oW3, ob3, ow4, ob4,
+   nparam (floats per member), packed (BF16 elements per member of the packed copy).
+   d3_mlp_pack: BF16 packed copy of the FP32 parameters [members][nparam].
+   d3_mlp_forward: E_dev [members][rows] network outputs; dX_dev (may be NULL)
+   [rows][32 * n_channels] = sum over members of dE/dG.
+   d3_mlp_train_batch: forward, backward and weight gradients of one mini-batch of
+   B rows (a multiple of 128) per member, member m reading rows idx_dev[m * B + r];
+   target_dev holds normalised targets; loss = mean squared error per member. Writes
+   E_dev [members][B], the partial gradients partial_dev [members][B/128][nparam] and
+   loss_dev [members][B/128] (summed squared errors per 128-row split); acts_dev is
+   scratch of d3_mlp_acts_elems(n_channels, B) BF16 elements per member.
+   d3_mlp_adam: sums the partial gradients, Adam step (step counts from 1) with
+   decoupled weight decay on the weight matrices, refreshes the packed copy. */
+int d3_mlp_layout(int n_channels, uint64_t *out);
+uint64_t d3_mlp_acts_elems(int n_channels, int B);
+int d3_mlp_pack(int n_channels, int members, const float *params_dev, uint16_t *packed_dev, void *cuda_stream);
+int d3_mlp_forward(int n_channels, int members, const float *params_dev, const uint16_t *packed_dev,
+                   const float *mean_dev, const float *inv_std_dev, const float *G_dev, const int *center_dev,
+                   int rows, float *E_dev, float *dX_dev, void *cuda_stream);
+int d3_mlp_train_batch(int n_channels, int members, const float *params_dev, const uint16_t *packed_dev,
+                       const float *mean_dev, const float *inv_std_dev, const float *G_dev, const int *center_dev,
+                       const float *target_dev, const int *idx_dev, int B, float *E_dev, uint16_t *acts_dev,
+                       float *partial_dev, float *loss_dev, void *cuda_stream);
+int d3_mlp_adam(int n_channels, int members, float *params_dev, uint16_t *packed_dev, float *m1_dev, float *m2_dev,
+                const float *partial_dev, int splits, float lr, float beta1, float beta2, float eps,
+                float weight_decay, int step, void *cuda_stream);
+
 /* Last error message of this thread ("" if none). */
 const char *d3_last_error(void);
 

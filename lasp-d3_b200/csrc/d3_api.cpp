@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "d3_engine.h"
+#include "d3_mlp.h"
 
 namespace {
 
@@ -238,6 +239,7 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
         break;
     case D3_OPT_ATM_TILE: o.atm_tile = value < 0 ? 0 : value; break;
     case D3_OPT_ATM_CTAS_PER_SM: o.atm_ctas_per_sm = value < 0 ? 0 : value; break;
+    case D3_OPT_ATM_SURROGATE: o.atm_surrogate = value != 0; break;
     case D3_OPT_PRECISION:
         if (value != 0 && value != 1) {
             set_error("D3_OPT_PRECISION takes 0 (FP64) or 1 (FP32 pair/triplet arithmetic)");
@@ -410,6 +412,162 @@ int d3_debug_bins(d3_handle_t *handle, int64_t *wrap_shift, int64_t *bin_index, 
     if (!handle) return 1;
     try {
         return d3::engine_debug_bins(H(handle)->engine, wrap_shift, bin_index, num_bins);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+// ---- learned ATM surrogate ---------------------------------------------------------
+int d3_set_surrogate(d3_handle_t *handle, const int *channel_z, int n_channels, int members, const float *params,
+                     const float *mean, const float *inv_std, const float *e_shift, float e_scale) {
+    if (!handle || !channel_z || !params || !mean || !inv_std || !e_shift || n_channels < 1 || members < 1) {
+        set_error("invalid argument in d3_set_surrogate");
+        return 1;
+    }
+    try {
+        const d3mlp::Layout L = d3mlp::make_layout(n_channels);
+        d3::SurrogateModel m;
+        m.channel_z.assign(channel_z, channel_z + n_channels);
+        m.members = members;
+        m.master.assign(params, params + (size_t)members * L.nparam);
+        const size_t nf = (size_t)n_channels * d3mlp::NRBF;
+        m.mean.assign(mean, mean + nf);
+        m.inv_std.assign(inv_std, inv_std + nf);
+        m.e_shift.assign(e_shift, e_shift + n_channels);
+        m.e_scale = e_scale;
+        std::string err;
+        if (d3::engine_set_surrogate(H(handle)->engine, m, err)) {
+            set_error(err);
+            return 1;
+        }
+        return 0;
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+int d3_set_surrogate_threshold(d3_handle_t *handle, double std_threshold_ev) {
+    if (!handle || !(std_threshold_ev >= 0.0)) {
+        set_error("invalid argument in d3_set_surrogate_threshold");
+        return 1;
+    }
+    d3::engine_set_surrogate_threshold(H(handle)->engine, std_threshold_ev);
+    return 0;
+}
+
+int d3_surrogate_flagged(d3_handle_t *handle) {
+    if (!handle) return -1;
+    try {
+        return d3::engine_surrogate_flagged(H(handle)->engine);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return -1;
+    }
+}
+
+int d3_surrogate_descriptors(d3_handle_t *handle, const int *channel_z, int n_channels, float *G_dev,
+                             int *center_dev, double *e_atm_dev, void *cuda_stream) {
+    if (!handle || !channel_z) {
+        set_error("invalid argument in d3_surrogate_descriptors");
+        return 1;
+    }
+    std::string err;
+    if (d3::engine_surrogate_descriptors(H(handle)->engine, channel_z, n_channels, G_dev, center_dev, e_atm_dev,
+                                         (cudaStream_t)cuda_stream, err)) {
+        set_error(err);
+        return 1;
+    }
+    return 0;
+}
+
+int d3_mlp_layout(int n_channels, uint64_t *out) {
+    try {
+        const d3mlp::Layout L = d3mlp::make_layout(n_channels);
+        const uint64_t v[12] = {(uint64_t)L.in_dim, (uint64_t)L.in_pad, L.oW1, L.ob1, L.oW2, L.ob2,
+                                L.oW3, L.ob3, L.ow4, L.ob4, L.nparam, L.packed};
+        for (int k = 0; k < 12; ++k) out[k] = v[k];
+        return 0;
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+uint64_t d3_mlp_acts_elems(int n_channels, int B) {
+    try {
+        return d3mlp::acts_elems(d3mlp::make_layout(n_channels), B);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 0;
+    }
+}
+
+static d3mlp::Net mlp_net(int n_channels, int members, const float *params, const uint16_t *packed, const float *mean,
+                          const float *inv_std) {
+    d3mlp::Net net;
+    net.L = d3mlp::make_layout(n_channels);
+    net.members = members;
+    net.master = params;
+    net.packed = packed;
+    net.mean = mean;
+    net.inv_std = inv_std;
+    return net;
+}
+
+static int sm_count() {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+int d3_mlp_pack(int n_channels, int members, const float *params_dev, uint16_t *packed_dev, void *cuda_stream) {
+    try {
+        d3mlp::pack(d3mlp::make_layout(n_channels), members, params_dev, packed_dev, (cudaStream_t)cuda_stream);
+        return 0;
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+int d3_mlp_forward(int n_channels, int members, const float *params_dev, const uint16_t *packed_dev,
+                   const float *mean_dev, const float *inv_std_dev, const float *G_dev, const int *center_dev,
+                   int rows, float *E_dev, float *dX_dev, void *cuda_stream) {
+    try {
+        d3mlp::infer(mlp_net(n_channels, members, params_dev, packed_dev, mean_dev, inv_std_dev), G_dev, center_dev,
+                     rows, E_dev, dX_dev, sm_count(), (cudaStream_t)cuda_stream);
+        return 0;
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+int d3_mlp_train_batch(int n_channels, int members, const float *params_dev, const uint16_t *packed_dev,
+                       const float *mean_dev, const float *inv_std_dev, const float *G_dev, const int *center_dev,
+                       const float *target_dev, const int *idx_dev, int B, float *E_dev, uint16_t *acts_dev,
+                       float *partial_dev, float *loss_dev, void *cuda_stream) {
+    try {
+        const d3mlp::Net net = mlp_net(n_channels, members, params_dev, packed_dev, mean_dev, inv_std_dev);
+        d3mlp::train_fwdbwd(net, G_dev, center_dev, target_dev, idx_dev, B, E_dev, acts_dev, partial_dev, loss_dev,
+                            (cudaStream_t)cuda_stream);
+        d3mlp::wgrad(net, acts_dev, B, partial_dev, (cudaStream_t)cuda_stream);
+        return 0;
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+int d3_mlp_adam(int n_channels, int members, float *params_dev, uint16_t *packed_dev, float *m1_dev, float *m2_dev,
+                const float *partial_dev, int splits, float lr, float beta1, float beta2, float eps,
+                float weight_decay, int step, void *cuda_stream) {
+    try {
+        d3mlp::adam(d3mlp::make_layout(n_channels), members, params_dev, packed_dev, m1_dev, m2_dev, partial_dev,
+                    splits, lr, beta1, beta2, eps, weight_decay, step, (cudaStream_t)cuda_stream);
+        return 0;
     } catch (const std::exception &ex) {
         set_error(ex.what());
         return 1;

@@ -77,7 +77,9 @@ constexpr int ATM_THREADS = 128;
 constexpr int ATM_PERM_CAP = 8192; // longest list whose entries are re-ordered by distance
 constexpr int ATM_SHELLS = 32;
 
-template <int NR>
+// CENTER: centre mode of the surrogate fallback (apexes from p.atm_apex, full lists,
+// every triplet weighted 1/3 for energy and forces alike)
+template <int NR, bool CENTER>
 __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
     extern __shared__ double smem[];
     const int ne = p.ne;
@@ -103,8 +105,8 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
         if (tid < ATM_SHELLS) shell_cnt[tid] = 0;
         __syncthreads();
         const int item = s_item;
-        if (item >= p.n) break;
-        const int a = p.sorted_of[p.n - 1 - item];
+        if (item >= (CENTER ? *p.atm_napex : p.n)) break;
+        const int a = CENTER ? p.atm_apex[item] : p.sorted_of[p.n - 1 - item];
         const long long e0 = p.atm_off[a];
         const int m = (int)(p.atm_off[a + 1] - e0);
         const double4 xa = p.xs[a];
@@ -296,6 +298,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm(KP p, int tile) {
                             wf = 1.0;
                         }
                         if (p.atm_force_scaled) wf = w;
+                        if (CENTER) w = wf = third;
                         // angular term A = (1 + 3 cos cos cos) / (r1 r2 r3)^3 and its side
                         // derivatives: with t1..t3 the cosine numerators, P = t1 t2 t3 and
                         // Q = d1 d2 d3, -r_k dA/dr_k = Q^(-5/2) (3Q - 3/4 d_k dP/dd_k + 15/8 P)

@@ -11,7 +11,7 @@
 
 constexpr int ATM32_NRP = 8; // padded C6 row length (NR <= 7)
 
-template <int NR>
+template <int NR, bool CENTER>
 __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
     extern __shared__ __align__(16) unsigned char smem32[];
     const int ne = p.ne;
@@ -36,6 +36,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
     const float third = 1.0f / 3.0f;
     const float ratm2f = (float)p.ratm2;
     const bool force_scaled = p.atm_force_scaled != 0;
+    const bool center = CENTER;
     const double inv_rc = 1.0 / sqrt(p.ratm2);
     unsigned long long visits = 0;
     while (true) {
@@ -44,8 +45,8 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
         if (tid < ATM_SHELLS) shell_cnt[tid] = 0;
         __syncthreads();
         const int item = s_item;
-        if (item >= p.n) break;
-        const int a = p.sorted_of[p.n - 1 - item];
+        if (item >= (CENTER ? *p.atm_napex : p.n)) break;
+        const int a = CENTER ? p.atm_apex[item] : p.sorted_of[p.n - 1 - item];
         const long long e0 = p.atm_off[a];
         const int m = (int)(p.atm_off[a + 1] - e0);
         const double4 xa = p.xs[a];
@@ -231,8 +232,8 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
                         // reference scale factors (src/d3_kernel.cu:1282-1290) as pair weights
                         const bool same = (jq == pc.x);
                         const bool apex_img = qa | (pc.x == a);
-                        const float w = same ? (qa ? third : 1.0f) : (apex_img ? 0.5f : 1.0f);
-                        const float wf = force_scaled ? w : (same ? 2.0f : 1.0f);
+                        const float w = center ? third : (same ? (qa ? third : 1.0f) : (apex_img ? 0.5f : 1.0f));
+                        const float wf = (force_scaled || center) ? w : (same ? 2.0f : 1.0f);
                         const float d2 = pa.w;
                         const float irsq = id1 * pb.y * id3;
                         const float ir9 = irsq * ir1 * pb.x * ir3;

@@ -31,6 +31,7 @@
 #include <mutex>
 #include <stdexcept>
 
+#include "d3_mlp.h"
 #include "d3_synth_params.h"
 
 namespace d3 {
@@ -101,6 +102,12 @@ struct KP {
     int2 *atm_ent;
     long long atm_cap;
     int *work;
+    // centre mode (surrogate fallback): full lists of the flagged atoms only, the apexes
+    // taken from atm_apex[0 .. *atm_napex), every triplet weighted 1/3
+    int atm_center;
+    const int *atm_apex;
+    const int *atm_napex;
+    const unsigned char *surr_flag;
     // outputs: [0, S) energies (eV), [S, S+3n) forces (eV/A, caller order),
     // [S+3n, S+3n+9S) stresses (eV/A^3, row-major per structure)
     double *out;
@@ -517,9 +524,14 @@ __global__ void k_atm_list(KP p) {
     if (FILL) pos = p.atm_off[a];
     int count = 0;
     bool range_err = false;
+    if (p.atm_center && !p.surr_flag[a]) {
+        if (!FILL && lane == 0) p.atm_cnt[a] = 0;
+        return;
+    }
+    const bool full = p.atm_center != 0;
     traverse(p, g, p.bin_s[a], p.stencils + g.sta_off, g.sta_n, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         bool keep = false;
-        if (act && p.orig[j] <= oa && in_box(g, sa, p.shift[j], Tx, Ty, Tz)) {
+        if (act && (full || p.orig[j] <= oa) && in_box(g, sa, p.shift[j], Tx, Ty, Tz)) {
             const double4 xj = p.xs[j];
             const double dx = xa.x - (xj.x + sh.x), dy = xa.y - (xj.y + sh.y), dz = xa.z - (xj.z + sh.z);
             const double d2 = dx * dx + dy * dy + dz * dz;
@@ -794,6 +806,72 @@ __global__ void k_chain32(KP p, const double *Gd) {
 
 #include "d3_atm.cuh"
 #include "d3_atm32.cuh"
+#include "d3_surrogate.cuh"
+
+// ------------------------------------------------------------------------------------
+// learned ATM surrogate: ensemble mean / spread, fallback flags, dE/dG in engine units
+// ------------------------------------------------------------------------------------
+// Radial basis: 32 Gaussians, centres 0.8 .. 21 A, width 0.7 A (bohr here)
+constexpr double SURR_MU0_A = 0.8, SURR_MU1_A = 21.0, SURR_SIGMA_A = 0.7;
+
+struct SurrComb {
+    const float *E;        // [members][n] network outputs
+    float *dX;             // [n][nfeat]: sum_m dE_m/dG in, dE/dG (engine energy units) out
+    const int *center;     // [n]
+    const float *e_shift;  // [nch] eV
+    float e_scale;         // eV per network unit
+    int members, nfeat;
+    double thr;            // ensemble standard deviation threshold, eV
+    unsigned char *flag;   // [n] 1: exact fallback
+    int *apex, *napex;     // flagged atoms (centre-mode ATM apexes)
+};
+
+// One warp per atom: ensemble mean and population standard deviation; unflagged atoms
+// keep the surrogate energy as their ATM apex share and scale their input gradient to
+// the engine's convention (hartree, stored sign); flagged atoms get zero of both and are
+// queued for the exact centre-mode pass.
+__global__ void k_surr_combine(KP p, SurrComb c) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= p.n) return;
+    const int cen = c.center[i];
+    double mean = 0.0, var = 0.0;
+    for (int m = 0; m < c.members; ++m) mean += (double)c.E[(size_t)m * p.n + i];
+    mean /= c.members;
+    for (int m = 0; m < c.members; ++m) {
+        const double d = (double)c.E[(size_t)m * p.n + i] - mean;
+        var += d * d;
+    }
+    var /= c.members;
+    const double sd = sqrt(var) * (double)c.e_scale;
+    const bool fl = cen < 0 || !(sd <= c.thr);
+    if (lane == 0) {
+        c.flag[i] = fl ? 1 : 0;
+        const double e_ev = mean * (double)c.e_scale + (cen >= 0 ? (double)c.e_shift[cen] : 0.0);
+        p.ea[i] = fl ? 0.0 : -e_ev / HARTREE_EV;
+        if (fl) {
+            c.apex[atomicAdd(c.napex, 1)] = i;
+            if (p.counters) atomicAdd(p.counters + 3, 1ull);
+        }
+    }
+    const float f = fl ? 0.f : (float)(-(double)c.e_scale / ((double)c.members * HARTREE_EV));
+    float *row = c.dX + (size_t)i * c.nfeat;
+    for (int k = lane; k < c.nfeat; k += 32) row[k] *= f;
+}
+
+// descriptors, centre channels and per-atom ATM energies (eV) to caller order
+__global__ void k_surr_export(KP p, const float *G, const int *center, int nfeat, float *Go, int *co, double *eo) {
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= p.n) return;
+    const int o = p.orig[i];
+    if (Go)
+        for (int k = lane; k < nfeat; k += 32) Go[(size_t)o * nfeat + k] = G[(size_t)i * nfeat + k];
+    if (lane == 0) {
+        if (co) co[o] = center[i];
+        if (eo) eo[o] = -(p.ea[i] + p.eb[i]) * HARTREE_EV;
+    }
+}
 
 // ------------------------------------------------------------------------------------
 // chain rule (src/d3_kernel.cu:1511-1698): F_i += (dE/dCN_i + dE/dCN_j) dCN_ij/dr r_hat
@@ -925,6 +1003,27 @@ struct DBuf {
     }
 };
 
+// learned ATM surrogate: model on the device and its per-evaluation work arrays
+struct SurrState {
+    bool loaded = false;
+    d3mlp::Layout L;
+    int members = 0;
+    float e_scale = 1.0f;
+    double thr_ev = 2e-4;
+    DBuf<int> chan, center, apex, napex, xchan, xcenter;
+    DBuf<float> master, mean, inv_std, e_shift, G, E, dX, xG;
+    DBuf<uint16_t> packed;
+    DBuf<unsigned char> flag;
+    void release() {
+        DBuf<int> *is[] = {&chan, &center, &apex, &napex, &xchan, &xcenter};
+        for (auto *d : is) d->release();
+        DBuf<float> *fs[] = {&master, &mean, &inv_std, &e_shift, &G, &E, &dX, &xG};
+        for (auto *d : fs) d->release();
+        packed.release();
+        flag.release();
+    }
+};
+
 struct Engine {
     // configuration
     int nref = 5;
@@ -984,7 +1083,8 @@ struct Engine {
         const void *fn = nullptr;
         size_t sm = 0;
         int blocks = 1;
-    } atm_occ_cache[2];
+    } atm_occ_cache[4];
+    SurrState surr;
 
     ~Engine() {
         DBuf<double> *ds[] = {&t_cnref, &t_c6, &t_r0, &t_rcov, &t_r2r4, &t_pairA, &pos_in, &cn, &w, &dw, &Y, &e2,
@@ -1007,6 +1107,7 @@ struct Engine {
         sg_dev.release();
         status.release();
         counters.release();
+        surr.release();
         for (auto &x : ev)
             if (x) cudaEventDestroy(x);
         if (stream) cudaStreamDestroy(stream);
@@ -1517,6 +1618,31 @@ static int atm_occupancy(Engine *e, int which, size_t sm, const void *fn) {
     return c.blocks;
 }
 
+static SurrDesc surr_desc(const int *chan, int nch, float *G, const float *dEdG, int *center) {
+    SurrDesc sd{};
+    sd.chan = chan;
+    sd.nch = nch;
+    sd.mu0 = (float)(SURR_MU0_A * ANG2BOHR);
+    sd.dmu = (float)((SURR_MU1_A - SURR_MU0_A) / (SURR_NRBF - 1) * ANG2BOHR);
+    const double sig = SURR_SIGMA_A * ANG2BOHR;
+    sd.inv2s2 = (float)(1.0 / (2.0 * sig * sig));
+    sd.G = G;
+    sd.dEdG = dEdG;
+    sd.center = center;
+    return sd;
+}
+
+static d3mlp::Net surr_net(const SurrState &S) {
+    d3mlp::Net net;
+    net.L = S.L;
+    net.members = S.members;
+    net.master = S.master.p;
+    net.packed = S.packed.p;
+    net.mean = S.mean.p;
+    net.inv_std = S.inv_std.p;
+    return net;
+}
+
 template <int NR>
 static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     KP p = p0;
@@ -1553,10 +1679,39 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
     D3_CUDA(cudaMemsetAsync(p.eb, 0, sizeof(double) * n, s));
     D3_CUDA(cudaMemsetAsync(p.gb, 0, sizeof(double) * n, s));
     D3_CUDA(cudaMemsetAsync(p.fb, 0, sizeof(double) * 3 * n, s));
+    // learned surrogate: descriptors -> ensemble -> fallback flags; the exact ATM pass
+    // below then runs in centre mode over the flagged atoms only
+    const bool surr = e->use_atm && e->opt.atm_surrogate && e->surr.loaded;
+    KP pc = p;
+    SurrDesc sd{};
+    if (surr) {
+        SurrState &S = e->surr;
+        sd = surr_desc(S.chan.p, S.L.nch, S.G.p, S.dX.p, S.center.p);
+        k_desc_fwd<NR><<<gw, T, 0, s>>>(p, sd);
+        d3mlp::infer(surr_net(S), S.G.p, S.center.p, n, S.E.p, S.dX.p, e->dev_sms, s);
+        D3_CUDA(cudaMemsetAsync(S.napex.p, 0, sizeof(int), s));
+        SurrComb c{};
+        c.E = S.E.p;
+        c.dX = S.dX.p;
+        c.center = S.center.p;
+        c.e_shift = S.e_shift.p;
+        c.e_scale = S.e_scale;
+        c.members = S.members;
+        c.nfeat = S.L.nch * SURR_NRBF;
+        c.thr = S.thr_ev;
+        c.flag = S.flag.p;
+        c.apex = S.apex.p;
+        c.napex = S.napex.p;
+        k_surr_combine<<<gw, T, 0, s>>>(p, c);
+        pc.atm_center = 1;
+        pc.atm_apex = S.apex.p;
+        pc.atm_napex = S.napex.p;
+        pc.surr_flag = S.flag.p;
+    }
     if (e->use_atm) {
-        k_atm_list<false><<<gw, T, 0, s>>>(p);
+        k_atm_list<false><<<gw, T, 0, s>>>(pc);
         k_scan<long long, int><<<1, 1024, 0, s>>>(p.atm_cnt, p.atm_off, n);
-        k_atm_list<true><<<gw, T, 0, s>>>(p);
+        k_atm_list<true><<<gw, T, 0, s>>>(pc);
     }
     D3_CUDA(cudaEventRecord(ev[4], s));
     if (e->use_atm) {
@@ -1568,10 +1723,14 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
             const int tmax = (int)std::max<size_t>(32, std::min<size_t>(256, (100 * 1024 - fixed) / per)) & ~31;
             const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(32, e->opt.atm_tile & ~31)) : std::min(tmax, 128);
             const size_t sm = (size_t)tile * per + fixed;
-            const int blocks_per_sm = atm_occupancy(e, 1, sm, (const void *)k_atm32<NR>);
+            const void *fn = surr ? (const void *)k_atm32<NR, true> : (const void *)k_atm32<NR, false>;
+            const int blocks_per_sm = atm_occupancy(e, surr ? 3 : 1, sm, fn);
             const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
             const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, per_sm)));
-            k_atm32<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
+            if (surr)
+                k_atm32<NR, true><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
+            else
+                k_atm32<NR, false><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
         } else {
             // partner tile: as many entries as fit in ~160 KB next to the apex tables
             const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double) +
@@ -1580,11 +1739,16 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
             const int tmax = (int)std::max<size_t>(8, std::min<size_t>(256, (160 * 1024 - fixed) / per));
             const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(8, e->opt.atm_tile)) : std::min(tmax, 128);
             const size_t sm = (size_t)tile * per + fixed;
-            const int blocks_per_sm = atm_occupancy(e, 0, sm, (const void *)k_atm<NR>);
+            const void *fn = surr ? (const void *)k_atm<NR, true> : (const void *)k_atm<NR, false>;
+            const int blocks_per_sm = atm_occupancy(e, surr ? 2 : 0, sm, fn);
             const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
             const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, per_sm)));
-            k_atm<NR><<<grid, ATM_THREADS, sm, s>>>(p, tile);
+            if (surr)
+                k_atm<NR, true><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
+            else
+                k_atm<NR, false><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
         }
+        if (surr) k_desc_bwd<NR><<<gw, T, 0, s>>>(p, sd);
     }
     D3_CUDA(cudaEventRecord(ev[5], s));
     k_sum_g<<<gb, T, 0, s>>>(p, e->G.p);
@@ -1609,7 +1773,10 @@ int engine_pass_times(Engine *e, float *ms, int cap, unsigned long long *counter
     return k;
 }
 
-int engine_launches_per_eval(const Engine *e) { return e->use_atm ? 16 : 12; }
+int engine_launches_per_eval(const Engine *e) {
+    if (!e->use_atm) return 12;
+    return (e->opt.atm_surrogate && e->surr.loaded) ? 20 : 16;
+}
 
 // Accuracy check of the Newton-refined helpers used by the ATM kernel against CUDA's
 // double-precision 1/sqrt, 1/x and cbrt over log-spaced inputs in [1e-12, 1e14].
@@ -1815,6 +1982,120 @@ int engine_debug_bins(Engine *e, int64_t *wrap_shift, int64_t *bin_index, int nb
     if (nb_out)
         for (int k = 0; k < 3; ++k) nb_out[k] = e->sg.empty() ? 0 : e->sg[0].nb[k];
     return 0;
+}
+
+// ------------------------------------------------------------------------------------
+// learned ATM surrogate: host side
+// ------------------------------------------------------------------------------------
+static std::vector<int> channel_map(const Engine *e, const int *channel_z, int nch) {
+    std::vector<int> chan(e->ne, -1);
+    for (int t = 0; t < e->ne; ++t)
+        for (int c = 0; c < nch; ++c)
+            if (channel_z[c] == e->elements[t]) chan[t] = c;
+    return chan;
+}
+
+int engine_set_surrogate(Engine *e, const SurrogateModel &m, std::string &err) {
+    try {
+        const int nch = (int)m.channel_z.size();
+        if (nch < 1 || nch > SURR_MAXCH) {
+            err = "surrogate: 1 to " + std::to_string(SURR_MAXCH) + " channels supported";
+            return -1;
+        }
+        const d3mlp::Layout L = d3mlp::make_layout(nch);
+        const size_t nfeat = (size_t)nch * SURR_NRBF;
+        if (m.members < 1 || m.master.size() != (size_t)m.members * L.nparam || m.mean.size() != nfeat ||
+            m.inv_std.size() != nfeat || m.e_shift.size() != (size_t)nch) {
+            err = "surrogate: model arrays do not match its channel and member counts";
+            return -1;
+        }
+        const std::vector<int> chan = channel_map(e, m.channel_z.data(), nch);
+        for (int t = 0; t < e->ne; ++t)
+            if (chan[t] < 0) {
+                err = "surrogate: element Z=" + std::to_string(e->elements[t]) + " of the handle is not a model channel";
+                return -1;
+            }
+        SurrState &S = e->surr;
+        S.loaded = false;
+        S.L = L;
+        S.members = m.members;
+        S.e_scale = m.e_scale;
+        S.chan.ensure(e->ne);
+        S.master.ensure(m.master.size());
+        S.mean.ensure(nfeat);
+        S.inv_std.ensure(nfeat);
+        S.e_shift.ensure(nch);
+        S.packed.ensure((size_t)m.members * L.packed);
+        D3_CUDA(cudaMemcpy(S.chan.p, chan.data(), sizeof(int) * e->ne, cudaMemcpyHostToDevice));
+        D3_CUDA(cudaMemcpy(S.master.p, m.master.data(), sizeof(float) * m.master.size(), cudaMemcpyHostToDevice));
+        D3_CUDA(cudaMemcpy(S.mean.p, m.mean.data(), sizeof(float) * nfeat, cudaMemcpyHostToDevice));
+        D3_CUDA(cudaMemcpy(S.inv_std.p, m.inv_std.data(), sizeof(float) * nfeat, cudaMemcpyHostToDevice));
+        D3_CUDA(cudaMemcpy(S.e_shift.p, m.e_shift.data(), sizeof(float) * nch, cudaMemcpyHostToDevice));
+        d3mlp::pack(L, m.members, S.master.p, S.packed.p, e->stream);
+        const size_t na = std::max<uint64_t>(e->max_atoms, 1);
+        S.G.ensure(na * nfeat);
+        S.dX.ensure(na * nfeat);
+        S.E.ensure(na * m.members);
+        S.center.ensure(na);
+        S.apex.ensure(na);
+        S.flag.ensure(na);
+        S.napex.ensure(1);
+        D3_CUDA(cudaStreamSynchronize(e->stream));
+        S.loaded = true;
+        return 0;
+    } catch (const std::exception &ex) {
+        err = ex.what();
+        return -1;
+    }
+}
+
+void engine_set_surrogate_threshold(Engine *e, double ev) { e->surr.thr_ev = ev; }
+
+int engine_surrogate_flagged(Engine *e) {
+    if (!e->surr.loaded) return 0;
+    int k = 0;
+    D3_CUDA(cudaStreamSynchronize(e->stream));
+    D3_CUDA(cudaDeviceSynchronize());
+    D3_CUDA(cudaMemcpy(&k, e->surr.napex.p, sizeof(int), cudaMemcpyDeviceToHost));
+    return k;
+}
+
+int engine_surrogate_descriptors(Engine *e, const int *channel_z, int nch, float *G_dev, int *center_dev,
+                                 double *e_atm_dev, cudaStream_t stream, std::string &err) {
+    try {
+        if (!e->have_events || !e->atoms_set) {
+            err = "surrogate descriptors: no evaluation yet";
+            return -1;
+        }
+        if (nch < 1 || nch > SURR_MAXCH) {
+            err = "surrogate descriptors: 1 to " + std::to_string(SURR_MAXCH) + " channels supported";
+            return -1;
+        }
+        cudaStream_t s = stream ? stream : e->stream;
+        const std::vector<int> chan = channel_map(e, channel_z, nch);
+        SurrState &S = e->surr;
+        const size_t n = e->n, nfeat = (size_t)nch * SURR_NRBF;
+        S.xchan.ensure(e->ne);
+        S.xG.ensure(std::max<size_t>(n, 1) * nfeat);
+        S.xcenter.ensure(std::max<size_t>(n, 1));
+        D3_CUDA(cudaMemcpy(S.xchan.p, chan.data(), sizeof(int) * e->ne, cudaMemcpyHostToDevice));
+        if (n == 0) return 0;
+        KP p = make_kp(e);
+        const SurrDesc sd = surr_desc(S.xchan.p, nch, S.xG.p, nullptr, S.xcenter.p);
+        const int T = 256;
+        const int gw = (int)(((long long)n * 32 + T - 1) / T);
+        if (e->nref == 5)
+            k_desc_fwd<5><<<gw, T, 0, s>>>(p, sd);
+        else
+            k_desc_fwd<7><<<gw, T, 0, s>>>(p, sd);
+        k_surr_export<<<gw, T, 0, s>>>(p, S.xG.p, S.xcenter.p, (int)nfeat, G_dev, center_dev, e_atm_dev);
+        D3_CUDA(cudaGetLastError());
+        D3_CUDA(cudaStreamSynchronize(s));
+        return 0;
+    } catch (const std::exception &ex) {
+        err = ex.what();
+        return -1;
+    }
 }
 
 } // namespace d3

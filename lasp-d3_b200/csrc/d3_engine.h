@@ -48,6 +48,21 @@ struct Options {
     double bin_divisor = 6.0;      // bin width = smallest cutoff / bin_divisor
     int atm_tile = 0;              // ATM partner tile entries (0: largest that fits, <= 128)
     int atm_ctas_per_sm = 0;       // persistent ATM CTAs per SM (0: occupancy limit)
+    bool atm_surrogate = false;    // learned ATM surrogate with exact fallback (needs a model)
+};
+
+// Learned ATM surrogate: network parameters and normalisation (network in d3_mlp.h).
+// Per-atom ATM energy (eV) of atom i = e_scale * mean_m(net_m(x_i)) + e_shift[channel(i)];
+// atoms whose ensemble standard deviation (population, eV) exceeds the threshold take
+// their exact share instead (all triplets through them, weight 1/3 each).
+struct SurrogateModel {
+    std::vector<int> channel_z;   // atomic number of each neighbour/centre channel
+    int members = 0;
+    std::vector<float> master;    // [members][nparam] FP32 parameters
+    std::vector<float> mean;      // [nch*32] descriptor normalisation
+    std::vector<float> inv_std;   // [nch*32]
+    std::vector<float> e_shift;   // [nch] eV
+    float e_scale = 1.0f;         // eV per network unit
 };
 
 struct Engine;
@@ -90,6 +105,18 @@ int engine_selftest_math(double max_rel[6]);
 // measured FMA throughput of the FP64 (fp64 = 1) or FP32 pipe, TFLOP/s
 double engine_peak_probe(int fp64);
 
+// learned ATM surrogate: load a model (every element of the handle must be a channel),
+// set the fallback threshold (eV; default 2e-4), number of atoms that took the exact
+// fallback in the last evaluation
+int engine_set_surrogate(Engine *e, const SurrogateModel &m, std::string &err);
+void engine_set_surrogate_threshold(Engine *e, double ev);
+int engine_surrogate_flagged(Engine *e);
+// descriptors of the current atoms (valid after an evaluation) for the given channels,
+// written to device memory in caller order: G[n][nch*32], centre channel [n] (-1: not a
+// channel) and the per-atom ATM energy of the last evaluation (eV, E/3 share of each
+// triplet), each output skipped when null
+int engine_surrogate_descriptors(Engine *e, const int *channel_z, int nch, float *G_dev, int *center_dev,
+                                 double *e_atm_dev, cudaStream_t stream, std::string &err);
 // diagnostics for tests: coordination numbers, dE/dCN, per-atom energies (hartree),
 // in the caller's atom order; ATM list (caller indices and reference lattice shifts)
 int engine_debug_atom_arrays(Engine *e, double *cn, double *dedcn, double *energy_atoms);

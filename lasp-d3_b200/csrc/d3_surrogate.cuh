@@ -1,0 +1,204 @@
+// Descriptors of the learned ATM surrogate and their backward pass.
+// Included by d3_engine.cu after the kernel parameter block and the traversal helper.
+//
+// For atom i, neighbour-element channel c and radial function k (32 per channel):
+//     G_i[c][k] = sum_{j,T: 0 < r_ij <= rc_ATM, chan(j) = c} C6_ij psi_k(r_ij)
+//     psi_k(r) = exp(-(r - mu_k)^2 / (2 sigma^2)) fc(r),  fc(r) = (1 + cos(pi r / rc)) / 2
+// with mu_k uniform in [0.8, 21] A and sigma = 0.7 A (in bohr here), C6_ij the exact
+// CN-dependent coefficient of the pair. The smooth cutoff keeps energies continuous.
+//
+// Backward, given dE/dG for every atom (E = sum_i E_i(G_i), E in the engine's stored sign):
+//     a_ij = C6_ij sum_k dE_i/dG_i[c_j][k] psi_k'(r),   b_ij = sum_k dE_i/dG_i[c_j][k] psi_k(r)
+//     force (gradient) on i:  sum_j (a_ij + a_ji) (x_i - x_j) / r_ij
+//     dE/dCN_i:               sum_j (b_ij + b_ji) dC6_ij/dCN_i
+//     virial:                 -(x_i - x_j) (x) (x_i - x_j) (a_ij + a_ji) / (2 V r) per ordered pair
+// One warp per atom, one lane per radial function; neighbours found by the rc_ATM stencil.
+
+constexpr int SURR_NRBF = 32;
+constexpr int SURR_MAXCH = 8;
+
+struct SurrDesc {
+    const int *chan;   // channel of each handle type (-1: not covered)
+    int nch;
+    float mu0, dmu;    // bohr
+    float inv2s2;      // 1 / (2 sigma^2), bohr^-2
+    float *G;          // [n][nch][32], binned order
+    const float *dEdG; // [n][nch][32], binned order (backward input)
+    int *center;       // [n] channel of each atom (binned order), -1: not a channel
+};
+
+template <int NR>
+__global__ void k_desc_fwd(KP p, SurrDesc sd) {
+    __shared__ float Gs[8][SURR_MAXCH][SURR_NRBF];
+    const int warp_in_block = threadIdx.x >> 5;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= p.n) return;
+    const SG &g = p.sg[p.sid[i]];
+    float(*Gw)[SURR_NRBF] = Gs[warp_in_block];
+    for (int c = 0; c < SURR_MAXCH; ++c) Gw[c][lane] = 0.0f;
+    __syncwarp();
+    const double4 xi = p.xs[i];
+    const int4 si = p.shift[i];
+    const int ti = (int)xi.w;
+    if (lane == 0) sd.center[i] = sd.chan[ti];
+    double wi[NR];
+#pragma unroll
+    for (int a = 0; a < NR; ++a) wi[a] = p.w[(size_t)i * NR + a];
+    const float mu_k = sd.mu0 + sd.dmu * lane;
+    const double rc = sqrt(p.ratm2);
+    const double pirc = 3.14159265358979323846 / rc;
+    traverse(p, g, p.bin_s[i], p.stencils + g.sta_off, g.sta_n,
+             [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+                 float r = 0.f, c6fc = 0.f;
+                 int ch = -1;
+                 bool keep = false;
+                 if (act && in_box(g, si, p.shift[j], Tx, Ty, Tz)) {
+                     const double4 xj = p.xs[j];
+                     const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
+                     const double d2 = dx * dx + dy * dy + dz * dz;
+                     ch = sd.chan[(int)xj.w];
+                     if (d2 <= p.ratm2 && d2 > 0.0 && ch >= 0) {
+                         const double rr = sqrt(d2);
+                         const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
+                         double c6 = 0.0;
+#pragma unroll
+                         for (int b = 0; b < NR; ++b) c6 += yj[b] * wi[b];
+                         r = (float)rr;
+                         c6fc = (float)(c6 * 0.5 * (1.0 + cos(pirc * rr)));
+                         keep = true;
+                     }
+                 }
+                 unsigned m = __ballot_sync(0xffffffffu, keep);
+                 while (m) {
+                     const int b = __ffs(m) - 1;
+                     m &= m - 1u;
+                     const float rb = __shfl_sync(0xffffffffu, r, b);
+                     const float cb = __shfl_sync(0xffffffffu, c6fc, b);
+                     const int chb = __shfl_sync(0xffffffffu, ch, b);
+                     const float d = rb - mu_k;
+                     Gw[chb][lane] += cb * __expf(-d * d * sd.inv2s2);
+                 }
+             });
+    __syncwarp();
+    float *out = sd.G + (size_t)i * sd.nch * SURR_NRBF;
+    for (int c = 0; c < sd.nch; ++c) out[c * SURR_NRBF + lane] = Gw[c][lane];
+}
+
+template <int NR>
+__global__ void k_desc_bwd(KP p, SurrDesc sd) {
+    __shared__ float Ds[8][SURR_MAXCH][SURR_NRBF];
+    const int warp_in_block = threadIdx.x >> 5;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= p.n) return;
+    const SG &g = p.sg[p.sid[i]];
+    float(*Dw)[SURR_NRBF] = Ds[warp_in_block];
+    const float *din = sd.dEdG + (size_t)i * sd.nch * SURR_NRBF;
+    for (int c = 0; c < sd.nch; ++c) Dw[c][lane] = din[c * SURR_NRBF + lane];
+    __syncwarp();
+    const double4 xi = p.xs[i];
+    const int4 si = p.shift[i];
+    const int ti = (int)xi.w;
+    const int chi = sd.chan[ti];
+    double wi[NR], dwi[NR];
+#pragma unroll
+    for (int a = 0; a < NR; ++a) {
+        wi[a] = p.w[(size_t)i * NR + a];
+        dwi[a] = p.dw[(size_t)i * NR + a];
+    }
+    const float mu_k = sd.mu0 + sd.dmu * lane;
+    const double rc = sqrt(p.ratm2);
+    const double pirc = 3.14159265358979323846 / rc;
+    double fx = 0, fy = 0, fz = 0, gcn = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+    traverse(p, g, p.bin_s[i], p.stencils + g.sta_off, g.sta_n,
+             [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+                 double dx = 0, dy = 0, dz = 0, rr = 1, c6 = 0, dc6 = 0, fc = 0, dfc = 0;
+                 int ch = -1;
+                 bool keep = false;
+                 if (act && chi >= 0 && in_box(g, si, p.shift[j], Tx, Ty, Tz)) {
+                     const double4 xj = p.xs[j];
+                     dx = xi.x - (xj.x + sh.x);
+                     dy = xi.y - (xj.y + sh.y);
+                     dz = xi.z - (xj.z + sh.z);
+                     const double d2 = dx * dx + dy * dy + dz * dz;
+                     ch = sd.chan[(int)xj.w];
+                     if (d2 <= p.ratm2 && d2 > 0.0 && ch >= 0) {
+                         rr = sqrt(d2);
+                         const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
+#pragma unroll
+                         for (int b = 0; b < NR; ++b) {
+                             c6 += yj[b] * wi[b];
+                             dc6 += yj[b] * dwi[b]; // dC6_ij/dCN_i
+                         }
+                         fc = 0.5 * (1.0 + cos(pirc * rr));
+                         dfc = -0.5 * pirc * sin(pirc * rr);
+                         keep = true;
+                     }
+                 }
+                 unsigned m = __ballot_sync(0xffffffffu, keep);
+                 while (m) {
+                     const int b = __ffs(m) - 1;
+                     m &= m - 1u;
+                     const double rb = __shfl_sync(0xffffffffu, rr, b);
+                     const int chb = __shfl_sync(0xffffffffu, ch, b);
+                     const int jb = __shfl_sync(0xffffffffu, j, b);
+                     const float fcb = (float)__shfl_sync(0xffffffffu, fc, b);
+                     const float dfcb = (float)__shfl_sync(0xffffffffu, dfc, b);
+                     const float d = (float)rb - mu_k;
+                     const float ph = __expf(-d * d * sd.inv2s2);
+                     const float psi = ph * fcb;
+                     const float dpsi = ph * (dfcb - 2.0f * d * sd.inv2s2 * fcb);
+                     const float gi = Dw[chb][lane];
+                     const float gj = sd.dEdG[((size_t)jb * sd.nch + chi) * SURR_NRBF + lane];
+                     // reduce sum_k of (gi + gj) psi' and (gi + gj) psi over the 32 radial functions
+                     float sa = (gi + gj) * dpsi, sb = (gi + gj) * psi;
+#pragma unroll
+                     for (int o = 16; o > 0; o >>= 1) {
+                         sa += __shfl_xor_sync(0xffffffffu, sa, o);
+                         sb += __shfl_xor_sync(0xffffffffu, sb, o);
+                     }
+                     if (lane == b) {
+                         // lane b owns the pair's geometry and C6
+                         const double a = c6 * (double)sa; // a_ij + a_ji
+                         const double fs = a / rr;
+                         fx += fs * dx;
+                         fy += fs * dy;
+                         fz += fs * dz;
+                         vxx += fs * dx * dx;
+                         vyy += fs * dy * dy;
+                         vzz += fs * dz * dz;
+                         vxy += fs * dx * dy;
+                         vxz += fs * dx * dz;
+                         vyz += fs * dy * dz;
+                         gcn += (double)sb * dc6; // (b_ij + b_ji) dC6/dCN_i
+                     }
+                 }
+             });
+    fx = warp_sum(fx);
+    fy = warp_sum(fy);
+    fz = warp_sum(fz);
+    gcn = warp_sum(gcn);
+    vxx = warp_sum(vxx);
+    vyy = warp_sum(vyy);
+    vzz = warp_sum(vzz);
+    vxy = warp_sum(vxy);
+    vxz = warp_sum(vxz);
+    vyz = warp_sum(vyz);
+    if (lane == 0) {
+        // the surrogate's share enters through the ATM apex arrays (entry arrays stay zero
+        // for atoms the surrogate covers)
+        p.fa[3 * i] += fx;
+        p.fa[3 * i + 1] += fy;
+        p.fa[3 * i + 2] += fz;
+        p.ga[i] += gcn;
+        const double sc = -1.0 / (2.0 * g.vol);
+        double *v = p.va + 6 * (size_t)i;
+        v[0] += vxx * sc;
+        v[1] += vyy * sc;
+        v[2] += vzz * sc;
+        v[3] += vxy * sc;
+        v[4] += vxz * sc;
+        v[5] += vyz * sc;
+    }
+}

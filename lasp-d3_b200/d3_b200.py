@@ -23,6 +23,7 @@ HEADER = os.path.join(HERE, "..", "include", "d3.h")
 ZERO_DAMPING, BJ_DAMPING = 0, 1
 OPT_ATM_FORCE_SCALED, OPT_SMOOTH_CN, OPT_PRECISION = 1, 2, 3
 OPT_BIN_DIVISOR, OPT_ATM_TILE, OPT_ATM_CTAS_PER_SM = 4, 5, 6
+OPT_ATM_SURROGATE = 7
 TABLE_5REF, TABLE_7REF = 0, 1
 
 _lib = None
@@ -100,6 +101,27 @@ def load_library(path=None):
     lib.d3_debug_atm_pairs.argtypes = [vp, vp, i64]
     lib.d3_debug_bins.restype = ctypes.c_int
     lib.d3_debug_bins.argtypes = [vp, vp, vp, vp]
+    ci = ctypes.c_int
+    lib.d3_set_surrogate.restype = ci
+    lib.d3_set_surrogate.argtypes = [vp, vp, ci, ci, vp, vp, vp, vp, f32]
+    lib.d3_set_surrogate_threshold.restype = ci
+    lib.d3_set_surrogate_threshold.argtypes = [vp, f64]
+    lib.d3_surrogate_flagged.restype = ci
+    lib.d3_surrogate_flagged.argtypes = [vp]
+    lib.d3_surrogate_descriptors.restype = ci
+    lib.d3_surrogate_descriptors.argtypes = [vp, vp, ci, vp, vp, vp, vp]
+    lib.d3_mlp_layout.restype = ci
+    lib.d3_mlp_layout.argtypes = [ci, vp]
+    lib.d3_mlp_acts_elems.restype = u64
+    lib.d3_mlp_acts_elems.argtypes = [ci, ci]
+    lib.d3_mlp_pack.restype = ci
+    lib.d3_mlp_pack.argtypes = [ci, ci, vp, vp, vp]
+    lib.d3_mlp_forward.restype = ci
+    lib.d3_mlp_forward.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, ci, vp, vp, vp]
+    lib.d3_mlp_train_batch.restype = ci
+    lib.d3_mlp_train_batch.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, ci, vp, vp, vp, vp, vp]
+    lib.d3_mlp_adam.restype = ci
+    lib.d3_mlp_adam.argtypes = [ci, ci, vp, vp, vp, vp, vp, ci, f32, f32, f32, f32, f32, ci, vp]
     if path is None:
         _lib = lib
     return lib
@@ -131,7 +153,42 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-class D3:
+class _Surrogate:
+    """Learned ATM surrogate methods shared by D3 and D3Batch (model: d3_surrogate.Model)."""
+
+    def set_surrogate(self, model, threshold_ev=None, enable=True):
+        cz = np.ascontiguousarray(model.channel_z, np.int32)
+        params = np.ascontiguousarray(model.params, np.float32)
+        mean = np.ascontiguousarray(model.mean, np.float32)
+        istd = np.ascontiguousarray(model.inv_std, np.float32)
+        shift = np.ascontiguousarray(model.e_shift, np.float32)
+        if self.lib.d3_set_surrogate(self.h, _ptr(cz), len(cz), int(model.members), _ptr(params), _ptr(mean),
+                                     _ptr(istd), _ptr(shift), float(model.e_scale)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+        if threshold_ev is not None:
+            self.set_surrogate_threshold(threshold_ev)
+        self.set_option(OPT_ATM_SURROGATE, 1 if enable else 0)
+
+    def set_surrogate_threshold(self, threshold_ev):
+        if self.lib.d3_set_surrogate_threshold(self.h, float(threshold_ev)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+
+    def surrogate_flagged(self):
+        return int(self.lib.d3_surrogate_flagged(self.h))
+
+    def surrogate_descriptors(self, channel_z, G_ptr=None, center_ptr=None, e_atm_ptr=None, stream_ptr=None):
+        """Descriptors of the current atoms into device buffers (caller order); see
+        d3_surrogate_descriptors in include/d3.h."""
+        cz = np.ascontiguousarray(channel_z, np.int32)
+        vp = ctypes.c_void_p
+        if self.lib.d3_surrogate_descriptors(self.h, _ptr(cz), len(cz), vp(G_ptr) if G_ptr else None,
+                                             vp(center_ptr) if center_ptr else None,
+                                             vp(e_atm_ptr) if e_atm_ptr else None,
+                                             vp(stream_ptr) if stream_ptr else None):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+
+
+class D3(_Surrogate):
     """One engine handle (FP64 path)."""
 
     def __init__(self, elements, max_atoms, rc=95.0, rc_cn=40.0, rc_atm=None, damping=BJ_DAMPING, functional=0,
@@ -237,7 +294,7 @@ class D3:
             pass
 
 
-class D3Batch:
+class D3Batch(_Surrogate):
     """Many independent periodic structures in one handle (batching form)."""
 
     def __init__(self, elements, max_structures, max_total_atoms, rc=95.0, rc_cn=40.0, rc_atm=None,

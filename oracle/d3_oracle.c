@@ -616,3 +616,171 @@ void oracle_grid_assign(const float *cell_f, int64_t n, const float *pos_f, cons
         grid_index[i] = (int64_t)(g[0] + g[1] * num_grid[0] + g[2] * num_grid[0] * num_grid[1]);
     }
 }
+
+/*
+ * Learned ATM surrogate (no reference counterpart: the checker of the engine's
+ * surrogate descriptors and of its force / stress chain).
+ *
+ * Descriptor of atom i, channel c, radial function k:
+ *     G[i][c*nrbf + k] = sum over (j, T) with 0 < r^2 <= rc_atm^2 and chan[types[j]] = c of
+ *                        C6_ij exp(-(r - mu0 - k dmu)^2 inv2s2) (1 + cos(pi r / rc_atm)) / 2
+ * with this oracle's CN and C6. Given dEdG (derivative of an energy E = sum_i E_i(G_i),
+ * hartree, the oracle's sign), accumulates the gradient +dE/dx into forces[n][3], the
+ * virial (divided by V) into virial[9] and dE/dCN into dedcn[n], then applies the CN
+ * chain rule. Any output may be NULL; dEdG NULL skips the backward part.
+ */
+int oracle_surrogate(const oracle_params *p, int64_t n, const double *pos, const int *types, const double *cell,
+                     const int64_t *mcb, const int *chan, int nch, int nrbf, double mu0, double dmu, double inv2s2,
+                     double *G, const double *dEdG, double *forces, double *virial, double *cn_out, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    image_set im;
+    make_images(cell, mcb, &im);
+    const double V = cell_volume(cell);
+    const double rcn2 = p->rc_cn * p->rc_cn, ra2 = p->rc_atm * p->rc_atm;
+    const double rca = p->rc_atm, pi = 3.14159265358979323846;
+    const int nf = nch * nrbf;
+    double *cn = (double *)calloc((size_t)n, sizeof(double));
+    double *dedcn = (double *)calloc((size_t)n, sizeof(double));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t i = 0; i < n; ++i) {
+        double acc = 0, ri = p->rcov[types[i]];
+        for (int64_t j = 0; j < n; ++j) {
+            double rs = ri + p->rcov[types[j]];
+            for (int64_t b = 0; b < im.n_img; ++b) {
+                double dx = pos[3 * i] - (pos[3 * j] + im.shift[3 * b]);
+                double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im.shift[3 * b + 1]);
+                double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im.shift[3 * b + 2]);
+                double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 <= rcn2 && d2 > 0.0) {
+                    double dd;
+                    acc += cn_term(p, sqrt(d2), rs, &dd);
+                }
+            }
+        }
+        cn[i] = acc;
+    }
+    if (cn_out) memcpy(cn_out, cn, sizeof(double) * n);
+    atom_weights *aw = NULL;
+    if (p->c6_mode == 1) {
+        aw = (atom_weights *)malloc(sizeof(atom_weights) * n);
+        for (int64_t i = 0; i < n; ++i) atom_weights_of(p, types[i], cn[i], &aw[i]);
+    }
+    c6_ctx cc = {p, aw, types, cn};
+    int nth = 1;
+#ifdef _OPENMP
+    nth = omp_get_max_threads();
+#endif
+    double *th_v = (double *)calloc((size_t)nth * 9, sizeof(double));
+    if (G) memset(G, 0, sizeof(double) * n * nf);
+    if (forces) memset(forces, 0, sizeof(double) * 3 * n);
+#pragma omp parallel
+    {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        double *Vv = th_v + (size_t)tid * 9;
+#pragma omp for schedule(dynamic, 4)
+        for (int64_t i = 0; i < n; ++i) {
+            const int ci = chan[types[i]];
+            double f_acc[3] = {0, 0, 0}, v_acc[9] = {0}, g_acc = 0;
+            for (int64_t j = 0; j < n; ++j) {
+                const int cj = chan[types[j]];
+                if (cj < 0) continue;
+                double c6 = 0, d1 = 0, d2c = 0;
+                int have_c6 = 0;
+                for (int64_t b = 0; b < im.n_img; ++b) {
+                    double dx = pos[3 * i] - (pos[3 * j] + im.shift[3 * b]);
+                    double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im.shift[3 * b + 1]);
+                    double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im.shift[3 * b + 2]);
+                    double d2 = dx * dx + dy * dy + dz * dz;
+                    if (!(d2 <= ra2 && d2 > 0.0)) continue;
+                    if (!have_c6) {
+                        pair_c6(&cc, i, j, &c6, &d1, &d2c);
+                        have_c6 = 1;
+                    }
+                    const double r = sqrt(d2);
+                    const double fc = 0.5 * (1.0 + cos(pi * r / rca));
+                    const double dfc = -0.5 * (pi / rca) * sin(pi * r / rca);
+                    double sa = 0, sb = 0;
+                    for (int k = 0; k < nrbf; ++k) {
+                        const double u = r - (mu0 + k * dmu);
+                        const double ph = exp(-u * u * inv2s2);
+                        const double psi = ph * fc;
+                        if (G && ci >= 0) G[(size_t)i * nf + (size_t)cj * nrbf + k] += c6 * psi;
+                        if (dEdG && ci >= 0) {
+                            const double dpsi = ph * (dfc - 2.0 * u * inv2s2 * fc);
+                            const double gg = dEdG[(size_t)i * nf + (size_t)cj * nrbf + k] +
+                                              dEdG[(size_t)j * nf + (size_t)ci * nrbf + k];
+                            sa += gg * dpsi;
+                            sb += gg * psi;
+                        }
+                    }
+                    if (dEdG && ci >= 0) {
+                        const double a = c6 * sa / r; /* dE/dr_ij / r over both descriptors */
+                        const double d[3] = {dx, dy, dz};
+                        for (int k = 0; k < 3; ++k) {
+                            f_acc[k] += a * d[k];
+                            for (int l = 0; l < 3; ++l) v_acc[k * 3 + l] += -d[k] * a * d[l] / 2.0;
+                        }
+                        g_acc += sb * d1; /* dE/dC6_ij dC6_ij/dCN_i */
+                    }
+                }
+            }
+            if (forces)
+                for (int k = 0; k < 3; ++k) forces[3 * i + k] += f_acc[k];
+            dedcn[i] = g_acc;
+            for (int k = 0; k < 9; ++k) Vv[k] += v_acc[k] / V;
+        }
+    }
+    if (dEdG) {
+        /* CN chain rule: (dE/dCN_i + dE/dCN_j) dCN_ij/dr over CN pairs */
+#pragma omp parallel
+        {
+            int tid = 0;
+#ifdef _OPENMP
+            tid = omp_get_thread_num();
+#endif
+            double *Vv = th_v + (size_t)tid * 9;
+#pragma omp for schedule(dynamic, 4)
+            for (int64_t i = 0; i < n; ++i) {
+                double ri = p->rcov[types[i]], gi = dedcn[i];
+                double f_acc[3] = {0, 0, 0}, v_acc[9] = {0};
+                for (int64_t j = 0; j < n; ++j) {
+                    double rs = ri + p->rcov[types[j]], g = gi + dedcn[j];
+                    for (int64_t b = 0; b < im.n_img; ++b) {
+                        double dx = pos[3 * i] - (pos[3 * j] + im.shift[3 * b]);
+                        double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im.shift[3 * b + 1]);
+                        double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im.shift[3 * b + 2]);
+                        double d2r = dx * dx + dy * dy + dz * dz;
+                        if (!(d2r <= rcn2 && d2r > 0.0)) continue;
+                        double dcn;
+                        cn_term(p, sqrt(d2r), rs, &dcn);
+                        double dE = g * dcn;
+                        double d[3] = {dx, dy, dz};
+                        for (int k = 0; k < 3; ++k) {
+                            f_acc[k] += dE * d[k];
+                            for (int l = 0; l < 3; ++l) v_acc[k * 3 + l] += (-1.0 * d[k] * dE * d[l]) / 2.0;
+                        }
+                    }
+                }
+                if (forces)
+                    for (int k = 0; k < 3; ++k) forces[3 * i + k] += f_acc[k];
+                for (int k = 0; k < 9; ++k) Vv[k] += v_acc[k] / V;
+            }
+        }
+    }
+    if (virial) {
+        memset(virial, 0, sizeof(double) * 9);
+        for (int t = 0; t < nth; ++t)
+            for (int k = 0; k < 9; ++k) virial[k] += th_v[t * 9 + k];
+    }
+    free(th_v);
+    free(cn);
+    free(dedcn);
+    free(aw);
+    free(im.shift);
+    return 0;
+}
