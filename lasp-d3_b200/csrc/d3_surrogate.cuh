@@ -12,7 +12,8 @@
 //     force (gradient) on i:  sum_j (a_ij + a_ji) (x_i - x_j) / r_ij
 //     dE/dCN_i:               sum_j (b_ij + b_ji) dC6_ij/dCN_i
 //     virial:                 -(x_i - x_j) (x) (x_i - x_j) (a_ij + a_ji) / (2 V r) per ordered pair
-// One warp per atom, one lane per radial function; neighbours found by the rc_ATM stencil.
+// Forward: one warp per atom, one lane per radial function; backward: one lane per
+// neighbour. Neighbours come from the rc_ATM stencil.
 
 constexpr int SURR_NRBF = 32;
 constexpr int SURR_MAXCH = 8;
@@ -85,17 +86,25 @@ __global__ void k_desc_fwd(KP p, SurrDesc sd) {
     for (int c = 0; c < sd.nch; ++c) out[c * SURR_NRBF + lane] = Gw[c][lane];
 }
 
+// Backward, one warp per atom and one neighbour per lane. With phi_k = exp(-(r - mu_k)^2
+// / (2 sigma^2)), psi_k = phi_k fc and g_k = dE/dG_i[c_j][k] + dE/dG_j[c_i][k]:
+//     sum_k g_k psi_k  = fc S0,   sum_k g_k psi_k' = dfc S0 - 2 fc S1 / (2 sigma^2)
+//     S0 = sum_k g_k phi_k,       S1 = sum_k g_k phi_k (r - mu_k)
+// so each neighbour costs 32 exponentials and two FMAs per radial function; the atom's own
+// dE/dG rows sit in shared memory (rows padded to 33 floats: lanes reading different
+// channels at the same k hit different banks), the neighbour's row is read as 8 float4.
 template <int NR>
-__global__ void k_desc_bwd(KP p, SurrDesc sd) {
-    __shared__ float Ds[8][SURR_MAXCH][SURR_NRBF];
+__global__ void __launch_bounds__(256, 2) k_desc_bwd(KP p, SurrDesc sd) {
+    constexpr int PITCH = SURR_NRBF + 1;
+    __shared__ float Ds[8][SURR_MAXCH * PITCH];
     const int warp_in_block = threadIdx.x >> 5;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= p.n) return;
     const SG &g = p.sg[p.sid[i]];
-    float(*Dw)[SURR_NRBF] = Ds[warp_in_block];
+    float *Dw = Ds[warp_in_block];
     const float *din = sd.dEdG + (size_t)i * sd.nch * SURR_NRBF;
-    for (int c = 0; c < sd.nch; ++c) Dw[c][lane] = din[c * SURR_NRBF + lane];
+    for (int c = 0; c < sd.nch; ++c) Dw[c * PITCH + lane] = din[c * SURR_NRBF + lane];
     __syncwarp();
     const double4 xi = p.xs[i];
     const int4 si = p.shift[i];
@@ -107,73 +116,56 @@ __global__ void k_desc_bwd(KP p, SurrDesc sd) {
         wi[a] = p.w[(size_t)i * NR + a];
         dwi[a] = p.dw[(size_t)i * NR + a];
     }
-    const float mu_k = sd.mu0 + sd.dmu * lane;
     const double rc = sqrt(p.ratm2);
     const double pirc = 3.14159265358979323846 / rc;
+    const float a2 = sd.inv2s2;
     double fx = 0, fy = 0, fz = 0, gcn = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
     traverse(p, g, p.bin_s[i], p.stencils + g.sta_off, g.sta_n,
              [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
-                 double dx = 0, dy = 0, dz = 0, rr = 1, c6 = 0, dc6 = 0, fc = 0, dfc = 0;
-                 int ch = -1;
-                 bool keep = false;
-                 if (act && chi >= 0 && in_box(g, si, p.shift[j], Tx, Ty, Tz)) {
-                     const double4 xj = p.xs[j];
-                     dx = xi.x - (xj.x + sh.x);
-                     dy = xi.y - (xj.y + sh.y);
-                     dz = xi.z - (xj.z + sh.z);
-                     const double d2 = dx * dx + dy * dy + dz * dz;
-                     ch = sd.chan[(int)xj.w];
-                     if (d2 <= p.ratm2 && d2 > 0.0 && ch >= 0) {
-                         rr = sqrt(d2);
-                         const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
+                 if (!act || chi < 0 || !in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
+                 const double4 xj = p.xs[j];
+                 const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
+                 const double d2 = dx * dx + dy * dy + dz * dz;
+                 const int ch = sd.chan[(int)xj.w];
+                 if (!(d2 <= p.ratm2 && d2 > 0.0) || ch < 0) return;
+                 const double rr = sqrt(d2);
+                 const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
+                 double c6 = 0.0, dc6 = 0.0;
 #pragma unroll
-                         for (int b = 0; b < NR; ++b) {
-                             c6 += yj[b] * wi[b];
-                             dc6 += yj[b] * dwi[b]; // dC6_ij/dCN_i
-                         }
-                         fc = 0.5 * (1.0 + cos(pirc * rr));
-                         dfc = -0.5 * pirc * sin(pirc * rr);
-                         keep = true;
+                 for (int b = 0; b < NR; ++b) {
+                     c6 += yj[b] * wi[b];
+                     dc6 += yj[b] * dwi[b]; // dC6_ij/dCN_i
+                 }
+                 const double fc = 0.5 * (1.0 + cos(pirc * rr));
+                 const double dfc = -0.5 * pirc * sin(pirc * rr);
+                 const float r = (float)rr;
+                 const float4 *gj = reinterpret_cast<const float4 *>(sd.dEdG + ((size_t)j * sd.nch + chi) * SURR_NRBF);
+                 const float *gi = Dw + ch * PITCH;
+                 float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+                 for (int q = 0; q < SURR_NRBF / 4; ++q) {
+                     const float4 v = __ldg(gj + q);
+                     const float gv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                     for (int t = 0; t < 4; ++t) {
+                         const int k = 4 * q + t;
+                         const float u = r - (sd.mu0 + sd.dmu * k);
+                         const float w = (gv[t] + gi[k]) * __expf(-u * u * a2);
+                         s0 += w;
+                         s1 = fmaf(w, u, s1);
                      }
                  }
-                 unsigned m = __ballot_sync(0xffffffffu, keep);
-                 while (m) {
-                     const int b = __ffs(m) - 1;
-                     m &= m - 1u;
-                     const double rb = __shfl_sync(0xffffffffu, rr, b);
-                     const int chb = __shfl_sync(0xffffffffu, ch, b);
-                     const int jb = __shfl_sync(0xffffffffu, j, b);
-                     const float fcb = (float)__shfl_sync(0xffffffffu, fc, b);
-                     const float dfcb = (float)__shfl_sync(0xffffffffu, dfc, b);
-                     const float d = (float)rb - mu_k;
-                     const float ph = __expf(-d * d * sd.inv2s2);
-                     const float psi = ph * fcb;
-                     const float dpsi = ph * (dfcb - 2.0f * d * sd.inv2s2 * fcb);
-                     const float gi = Dw[chb][lane];
-                     const float gj = sd.dEdG[((size_t)jb * sd.nch + chi) * SURR_NRBF + lane];
-                     // reduce sum_k of (gi + gj) psi' and (gi + gj) psi over the 32 radial functions
-                     float sa = (gi + gj) * dpsi, sb = (gi + gj) * psi;
-#pragma unroll
-                     for (int o = 16; o > 0; o >>= 1) {
-                         sa += __shfl_xor_sync(0xffffffffu, sa, o);
-                         sb += __shfl_xor_sync(0xffffffffu, sb, o);
-                     }
-                     if (lane == b) {
-                         // lane b owns the pair's geometry and C6
-                         const double a = c6 * (double)sa; // a_ij + a_ji
-                         const double fs = a / rr;
-                         fx += fs * dx;
-                         fy += fs * dy;
-                         fz += fs * dz;
-                         vxx += fs * dx * dx;
-                         vyy += fs * dy * dy;
-                         vzz += fs * dz * dz;
-                         vxy += fs * dx * dy;
-                         vxz += fs * dx * dz;
-                         vyz += fs * dy * dz;
-                         gcn += (double)sb * dc6; // (b_ij + b_ji) dC6/dCN_i
-                     }
-                 }
+                 const double fs = c6 * (dfc * (double)s0 - 2.0 * (double)a2 * fc * (double)s1) / rr; // dE/dr / r
+                 fx += fs * dx;
+                 fy += fs * dy;
+                 fz += fs * dz;
+                 vxx += fs * dx * dx;
+                 vyy += fs * dy * dy;
+                 vzz += fs * dz * dz;
+                 vxy += fs * dx * dy;
+                 vxz += fs * dx * dz;
+                 vyz += fs * dy * dz;
+                 gcn += fc * (double)s0 * dc6; // dE/dC6_ij dC6_ij/dCN_i
              });
     fx = warp_sum(fx);
     fy = warp_sum(fy);
