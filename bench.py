@@ -43,11 +43,34 @@ ATM_FLOP_PER_TRIPLET = 345
 L2_FLUSH_BYTES = 256 << 20
 
 
-def workload_config(n, form):
+# Algorithmic FLOPs of one in-range ordered two-body pair as the reference writes it
+# (src/d3_kernel.cu:1105-1154): distance 8, r powers 6, BJ damping terms 12, energy 6,
+# dE/dr and dE/dCN 12, force 6, half of the 3x3 stress 10; C6 interpolation excluded.
+TWOBODY_FLOP_PER_PAIR = 60
+
+
+def system_for(args, seed):
+    import d3_systems as S
+
+    if args.system == "water":
+        return S.water_box(seed=0)
+    return S.triclinic_box(args.atoms, seed=seed)
+
+
+def workload_config(n, form, args=None):
+    water = args is not None and args.system == "water"
+    table = 7 if (args is not None and args.table == 7) else 5
+    atm = not (args is not None and args.no_atm)
+    if water:
+        box = ("32 rigid H2O (96 atoms) in a cubic 9.86 A cell, O on a jittered 4x4x2 grid, random "
+               "orientations (seed 0)")
+    else:
+        box = ("%d-atom triclinic periodic box (a=(58,0,0) b=(5,58,0) c=(3,4,58) A, scaled for other sizes), "
+               "H40/C30/N10/O15/Cu5 %%, 1.0 A min-image rejection" % n)
     return {
-        "workload": "%d-atom triclinic periodic box (a=(58,0,0) b=(5,58,0) c=(3,4,58) A, scaled for other sizes), "
-                    "H40/C30/N10/O15/Cu5 %%, 1.0 A min-image rejection; PBE-D3(BJ)+ATM, 5-reference synthetic "
-                    "table, rc 95 / rc_CN 40 / rc_ATM 40 bohr; energy+forces+stress" % n,
+        "workload": "%s; PBE-D3(BJ)%s, %d-reference synthetic table, rc 95 / rc_CN 40%s bohr; "
+                    "energy+forces+stress" % (box, "+ATM" if atm else " (two-body + CN, no ATM)", table,
+                                               " / rc_ATM 40" if atm else ""),
         "atoms_per_gpu": n,
         "form": form,
         "l2": "flushed between timed steps (256 MiB device write)",
@@ -115,7 +138,7 @@ def dist_setup():
     return world, rank, local
 
 
-def run_cpu_baseline(sys_, sample=48, seed=7):
+def run_cpu_baseline(sys_, sample=48, seed=7, rc_atm=RC_ATM, extended=False):
     """FP64 oracle (C/OpenMP, all host threads) on a bounded sample: CN for every atom,
     then two-body, ATM (as apex) and chain rule for `sample` random central atoms."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -123,9 +146,11 @@ def run_cpu_baseline(sys_, sample=48, seed=7):
 
     n = len(sys_["Z"])
     rng = np.random.default_rng(seed)
+    sample = min(sample, n)
     sub = np.sort(rng.choice(n, size=sample, replace=False))
     cores = os.cpu_count() or 1
-    kw = dict(rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0, c6_mode=1, nthreads=cores)
+    kw = dict(rc=RC, rc_cn=RC_CN, rc_atm=rc_atm, damping=1, functional=0, c6_mode=1, nthreads=cores,
+              extended=extended)
     t0 = time.perf_counter()
     oracle.compute(sys_["pos"], sys_["Z"], sys_["cell"], subset=np.zeros(0, np.int64), **kw)
     t_cn = time.perf_counter() - t0
@@ -185,7 +210,7 @@ def engine_arm(args, world, rank, local):
     import torch
 
     import d3_systems as S
-    from d3_b200 import D3, OPT_PRECISION, peak_probe
+    from d3_b200 import D3, OPT_PRECISION, TABLE_5REF, TABLE_7REF, peak_probe
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -202,15 +227,17 @@ def engine_arm(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
 
-    n = args.atoms
-    sys_ = S.triclinic_box(n, seed=1 + rank)
+    sys_ = system_for(args, 1 + rank)
+    n = len(sys_["Z"])
+    rc_atm = None if args.no_atm else RC_ATM
+    table = TABLE_7REF if args.table == 7 else TABLE_5REF
     stream = torch.cuda.Stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     forms = {}
     sampler = ClockSampler(local)
     sampler.start()
     for form, prec in (("plain", 0), ("precision", 1)):
-        d = D3(sys_["Z"], n, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
+        d = D3(sys_["Z"], n, rc=RC, rc_cn=RC_CN, rc_atm=rc_atm, damping=1, functional=0, table=table)
         d.set_option(OPT_PRECISION, prec)
         d.set_cell(sys_["cell"])
         d.set_atoms(sys_["pos"], sys_["Z"])
@@ -220,6 +247,7 @@ def engine_arm(args, world, rank, local):
         ms_per_step = total_ms / args.steps
         forms[form] = {"value": world * n / (ms_per_step * 1e-3), "ms_per_step": ms_per_step,
                        "atm_ms": statistics.mean(atm_ms), "counters": counters,
+                       "twobody_ms": statistics.mean(p["twobody"] for p in passes),
                        "passes_ms": {k: statistics.mean(p[k] for p in passes) for k in passes[0]},
                        "energy": energy, "forces": forces, "stress": stress,
                        "launches": d.launches_per_eval()}
@@ -244,7 +272,13 @@ def engine_arm(args, world, rank, local):
     z16 = np.ascontiguousarray(sys_["Z"], np.uint16)
     posf = np.ascontiguousarray(sys_["pos"], np.float32)
     cellf = np.ascontiguousarray(sys_["cell"], np.float32)
-    h = lib.init_d3_handle_with_atm(z16.ctypes.data, n, n, RC, RC_CN, RC_ATM, 1, 0)
+    if table == TABLE_7REF:
+        el = np.ascontiguousarray(sorted(set(int(z) for z in sys_["Z"])), np.uint16)
+        h = lib.d3_init_handle_ex(el.ctypes.data, len(el), n, RC, RC_CN, rc_atm or 0.0, 1, 0, table)
+    elif rc_atm:
+        h = lib.init_d3_handle_with_atm(z16.ctypes.data, n, n, RC, RC_CN, RC_ATM, 1, 0)
+    else:
+        h = lib.init_d3_handle(z16.ctypes.data, n, n, RC, RC_CN, 1, 0)
     lib.d3_set_option(h, OPT_PRECISION, 1 if chosen == "precision" else 0)
     lib.set_cell(h, cellf.ctypes.data)
     ef = np.zeros(1, np.float32)
@@ -266,25 +300,32 @@ def engine_arm(args, world, rank, local):
            "path": "set_atoms(float coords) + compute_dispersion_energy_from_handle_status, host buffers, %s form"
                    % chosen}
 
-    # roofline of the dominant kernel (ATM triplets) of the chosen form
-    triplets = int(ch["counters"][0]) // 2
-    atm_s = ch["atm_ms"] * 1e-3
-    achieved = triplets * ATM_FLOP_PER_TRIPLET / atm_s / 1e12
+    # roofline of the dominant kernel of the chosen form (ATM triplets; two-body pairs
+    # when ATM is off)
     fp64 = chosen == "plain"
     peak = peak_probe(fp64)
+    triplets = int(ch["counters"][0]) // 2
+    pairs = int(ch["counters"][1])
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
-    if os.path.exists(tfile):
-        traffic = json.load(open(tfile)).get("atm_fp64_bytes_per_launch" if fp64 else "atm_fp32_bytes_per_launch")
-    roofline = {"bound": "fp64" if fp64 else "fp32",
-                "kernel": "k_atm (ATM triplets, FP64)" if fp64 else "k_atm32 (ATM triplets, FP32 arithmetic)",
+    if rc_atm:
+        achieved = triplets * ATM_FLOP_PER_TRIPLET / (ch["atm_ms"] * 1e-3) / 1e12
+        tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+        if os.path.exists(tfile) and args.system == "triclinic" and n == N_ATOMS and table == TABLE_5REF:
+            traffic = json.load(open(tfile)).get("atm_fp64_bytes_per_launch" if fp64 else "atm_fp32_bytes_per_launch")
+        kernel = "k_atm (ATM triplets, FP64)" if fp64 else "k_atm32 (ATM triplets, FP32 arithmetic)"
+        algorithmic = "%d in-range triplets x %d FLOP per launch" % (triplets, ATM_FLOP_PER_TRIPLET)
+    else:
+        achieved = pairs * TWOBODY_FLOP_PER_PAIR / (ch["twobody_ms"] * 1e-3) / 1e12
+        kernel = "k_twobody (FP64)" if fp64 else "k_twobody32 (FP32 pair arithmetic)"
+        algorithmic = "%d in-range ordered pairs x %d FLOP per launch" % (pairs, TWOBODY_FLOP_PER_PAIR)
+    roofline = {"bound": "fp64" if fp64 else "fp32", "kernel": kernel,
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                 "peak_source": "measured %s FMA throughput of this GPU by d3_peak_probe (MEASURED_PEAKS.json has no "
                                "FP64/FP32 figure)" % ("FP64" if fp64 else "FP32"),
-                "algorithmic": "%d in-range triplets x %d FLOP per launch" % (triplets, ATM_FLOP_PER_TRIPLET)}
+                "algorithmic": algorithmic}
     model_path = os.path.join(ROOT, "lasp-d3_b200", "surrogate", "atm_hcnosicu.d3s")
     sur = None
-    if os.path.exists(model_path):
+    if os.path.exists(model_path) and rc_atm and table == TABLE_5REF and args.system == "triclinic":
         import d3_surrogate as SU
 
         sur = surrogate_form(sys_, SU.Model.load(model_path), args, flush, stream, barrier, forms["plain"])
@@ -302,13 +343,13 @@ def engine_arm(args, world, rank, local):
             "vs_baseline": None, "dtype": "f64" if fp64 else "f32", "data": "synthetic",
             "config": workload_config(n, "%s form (%s)" % (chosen, "FP64 throughout" if fp64 else
                                                          "FP32 pair/triplet arithmetic, FP64 C6 weights, dE/dCN "
-                                                         "and reductions")),
+                                                         "and reductions"), args),
             "chosen_form": chosen, "forms": forms_out,
             "roofline": roofline, "e2e": e2e, "gpu_launches": ch["launches"] * args.steps, "clocks": clocks,
             "counters": {"atm_triplets": triplets, "twobody_ordered_pairs": int(ch["counters"][1]),
                          "cn_ordered_pairs": int(ch["counters"][2])}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = run_cpu_baseline(sys_)
+        line["cpu_baseline"] = run_cpu_baseline(sys_, rc_atm=rc_atm, extended=table == TABLE_7REF)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -326,13 +367,18 @@ def reference_arm(args, world, rank, local):
 
     import d3_systems as S
 
-    if not ref_lib.available():
+    ext = args.table == 7
+    if not ref_lib.available(ext):
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libd3_ref.so is missing"}))
         return
-    n = args.ref_atoms
-    sys_ = S.triclinic_box(n, seed=1)
+    if args.system == "water":
+        sys_ = S.water_box(seed=0)
+    else:
+        sys_ = S.triclinic_box(args.ref_atoms, seed=1)
+    n = len(sys_["Z"])
     # the reference's compute call is synchronous (src/d3.cu:201): wall clock around it
-    h = ref_lib.RefHandle(sys_["Z"], n, RC, RC_CN, RC_ATM, damping=1, functional=0)
+    h = ref_lib.RefHandle(sys_["Z"], n, RC, RC_CN, None if args.no_atm else RC_ATM, damping=1, functional=0,
+                          extended=ext)
     h.set_system(sys_["pos"], sys_["Z"], sys_["cell"])
     for _ in range(args.warmup):
         h.compute()
@@ -347,14 +393,16 @@ def reference_arm(args, world, rank, local):
     h.close()
     sec = statistics.mean(times)
     value = n / sec
+    full_n = 96 if args.system == "water" else args.atoms
     sample = ("reference CUDA build (LASP-D3 sources, sm_100a, synthetic table) through "
               "compute_dispersion_energy_from_handle_status on the same generator at %d atoms (cell scaled to "
-              "density); its cost per atom grows with N (all-pairs ATM), so this overstates its throughput at %d "
-              "atoms" % (n, N_ATOMS))
+              "density)%s" % (n, "" if n == full_n else "; its cost per atom grows with N (all-pairs ATM), so this "
+                              "overstates its throughput at %d atoms" % full_n))
     line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": workload_config(N_ATOMS, "reference CUDA build, bounded sample of %d atoms" % n),
+            "config": workload_config(full_n, "reference CUDA build%s" % (
+                "" if n == full_n else ", bounded sample of %d atoms" % n), args),
             "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "clocks": clocks, "energy_ev": e}
@@ -383,12 +431,21 @@ def batch_mode(args):
                                   "H/C/N/O/Si/Cu; PBE-D3(BJ)+ATM, rc 95 / 40 / 40 bohr" % (len(sts), ntot)},
            "forms": {}}
     stream = torch.cuda.Stream()
+    # the autotuner times candidates on a subset of the structures (same generator, so the
+    # same per-structure sizes and densities) and the result is applied to the whole batch
+    sub = sts[:min(len(sts), args.tune_structs)]
+    nsub = sum(len(s["Z"]) for s in sub)
     for form, prec in (("plain", 0), ("precision", 1)):
+        t = D3Batch(elements, len(sub), nsub, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
+        t.set_option(OPT_PRECISION, prec)
+        t.set_structures(sub)
+        key = d3_autotune.workload_key(ntot / len(sts), vol / len(sts), RC, RC_CN, RC_ATM, prec) + "|batch"
+        tuned = d3_autotune.tune(t, key, repeats=1)
+        t.close()
         b = D3Batch(elements, len(sts), ntot, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
         b.set_option(OPT_PRECISION, prec)
         b.set_structures(sts)
-        key = d3_autotune.workload_key(ntot / len(sts), vol / len(sts), RC, RC_CN, RC_ATM, prec) + "|batch"
-        tuned = d3_autotune.tune(b, key, repeats=1)
+        d3_autotune.apply(b, tuned)
         e, _, _ = b.compute()
         with torch.cuda.stream(stream):
             for _ in range(args.warmup):
@@ -405,6 +462,7 @@ def batch_mode(args):
         pt, cnt = b.pass_times()
         out["forms"][form] = {"value": ntot / (statistics.mean(ms) * 1e-3), "ms_per_step": statistics.mean(ms),
                               "passes_ms": pt, "autotuned": {k: v for k, v in tuned.items() if k != "trials"},
+                              "tuned_on_structures": len(sub),
                               "energy_sum_ev": float(np.sum(e))}
         b.close()
     out["value"] = out["forms"]["precision"]["value"]
@@ -554,16 +612,23 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
-    ap.add_argument("--atoms", type=int, default=N_ATOMS)
+    ap.add_argument("--atoms", type=int, default=None,
+                    help="atoms per box (default 20,000; 100,000 in --mode surrogate)")
     ap.add_argument("--ref-atoms", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", choices=["single", "batch", "md", "surrogate"], default="single")
+    ap.add_argument("--system", choices=["triclinic", "water"], default="triclinic")
+    ap.add_argument("--table", type=int, choices=[5, 7], default=5)
+    ap.add_argument("--no-atm", action="store_true", help="two-body + CN only")
     ap.add_argument("--model", default=os.path.join(ROOT, "lasp-d3_b200", "surrogate", "atm_hcnosicu.d3s"))
     ap.add_argument("--seed", type=int, default=77)
     ap.add_argument("--batch", type=int, default=2048)
+    ap.add_argument("--tune-structs", type=int, default=128)
     ap.add_argument("--md-steps", type=int, default=200)
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.mode in ("batch", "md"):
+        args.atoms = args.atoms or N_ATOMS
     if args.mode == "batch":
         batch_mode(args)
         return
@@ -571,10 +636,10 @@ def main():
         md_mode(args)
         return
     if args.mode == "surrogate":
-        if args.atoms == N_ATOMS:
-            args.atoms = 100000
+        args.atoms = args.atoms or 100000
         surrogate_mode(args)
         return
+    args.atoms = args.atoms or N_ATOMS
     if args.impl == "reference":
         reference_arm(args, world, rank, local)
     else:
