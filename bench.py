@@ -312,7 +312,8 @@ def engine_arm(args, world, rank, local):
         tfile = os.path.join(ROOT, "profiles", "ncu_traffic.json")
         if os.path.exists(tfile) and args.system == "triclinic" and n == N_ATOMS and table == TABLE_5REF:
             traffic = json.load(open(tfile)).get("atm_fp64_bytes_per_launch" if fp64 else "atm_fp32_bytes_per_launch")
-        kernel = "k_atm (ATM triplets, FP64)" if fp64 else "k_atm32 (ATM triplets, FP32 arithmetic)"
+        kernel = ("k_atm (ATM triplets, FP64)" if fp64 else
+                  "k_atm32b + k_atm32 (ATM triplets, FP32 arithmetic; block pairs, lists over 4,096 entries mirrored)")
         algorithmic = "%d in-range triplets x %d FLOP per launch" % (triplets, ATM_FLOP_PER_TRIPLET)
     else:
         achieved = pairs * TWOBODY_FLOP_PER_PAIR / (ch["twobody_ms"] * 1e-3) / 1e12

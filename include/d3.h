@@ -115,7 +115,9 @@ enum {
                                     reductions (precision form) */
     D3_OPT_BIN_DIVISOR = 4,      /* cell-list bin width = smallest cutoff / value (1..32, default 6) */
     D3_OPT_ATM_TILE = 5,         /* ATM partner tile entries (0 = automatic) */
-    D3_OPT_ATM_CTAS_PER_SM = 6   /* persistent ATM CTAs per SM (0 = occupancy limit) */
+    D3_OPT_ATM_CTAS_PER_SM = 6,  /* persistent ATM CTAs per SM (0 = occupancy limit) */
+    D3_OPT_ATM_SCHEDULE = 8      /* precision-form ATM: 0 (default) block pairs, each triplet
+                                    visited once; 1 mirror-symmetric, each triplet twice */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);
 

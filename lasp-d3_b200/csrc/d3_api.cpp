@@ -240,6 +240,13 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
     case D3_OPT_ATM_TILE: o.atm_tile = value < 0 ? 0 : value; break;
     case D3_OPT_ATM_CTAS_PER_SM: o.atm_ctas_per_sm = value < 0 ? 0 : value; break;
     case D3_OPT_ATM_SURROGATE: o.atm_surrogate = value != 0; break;
+    case D3_OPT_ATM_SCHEDULE:
+        if (value != 0 && value != 1) {
+            set_error("D3_OPT_ATM_SCHEDULE takes 0 (block pairs) or 1 (mirror-symmetric)");
+            return 1;
+        }
+        o.atm_schedule = value;
+        break;
     case D3_OPT_PRECISION:
         if (value != 0 && value != 1) {
             set_error("D3_OPT_PRECISION takes 0 (FP64) or 1 (FP32 pair/triplet arithmetic)");

@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
         const int a = CENTER ? p.atm_apex[item] : p.sorted_of[p.n - 1 - item];
         const long long e0 = p.atm_off[a];
         const int m = (int)(p.atm_off[a + 1] - e0);
+        if (!CENTER && m <= p.atm_min_m) continue; // shorter lists: k_atm32b
         const double4 xa = p.xs[a];
         const int ta = (int)xa.w;
         const SG &g = p.sg[p.sid[a]];

@@ -116,6 +116,8 @@ struct KP {
     int precision;
     float4 *xs32;
     float *w32, *dw32, *Y32;
+    float *D32;     // [n][ne][NR]: d/dCN of the own weights through the C6 rows (block-pair ATM)
+    int atm_min_m;  // k_atm32 takes only apexes with longer lists (the rest: k_atm32b)
     // work counters: [0] ATM in-range visits (2 per triplet), [1] two-body in-range
     // ordered pairs, [2] CN in-range ordered pairs
     unsigned long long *counters;
@@ -388,6 +390,7 @@ __global__ void k_weights(KP p) {
             p.dw32[(size_t)i * NR + a] = (float)dwn;
         }
         w[a] = wn;
+        dw[a] = dwn;
     }
     for (int tt = 0; tt < p.ne; ++tt) {
         const double *C = p.c6 + ((size_t)t * p.ne + tt) * NR * NR;
@@ -399,6 +402,12 @@ __global__ void k_weights(KP p) {
             for (int a = 0; a < NR; ++a) acc += w[a] * C[a * NR + b];
             Yo[b] = acc;
             if (p.precision) p.Y32[((size_t)i * p.ne + tt) * NR + b] = (float)acc;
+            if (p.D32) {
+                double dacc = 0.0;
+#pragma unroll
+                for (int a = 0; a < NR; ++a) dacc += dw[a] * C[a * NR + b];
+                p.D32[((size_t)i * p.ne + tt) * NR + b] = (float)dacc;
+            }
         }
     }
 }
@@ -806,6 +815,7 @@ __global__ void k_chain32(KP p, const double *Gd) {
 
 #include "d3_atm.cuh"
 #include "d3_atm32.cuh"
+#include "d3_atm32b.cuh"
 #include "d3_surrogate.cuh"
 
 // ------------------------------------------------------------------------------------
@@ -1065,7 +1075,8 @@ struct Engine {
     DBuf<int> atm_cnt, work, sid_in, sid;
     DBuf<SG> sg_dev;
     DBuf<float4> xs32;
-    DBuf<float> w32, dw32, Y32;
+    DBuf<float> w32, dw32, Y32, D32;
+    DBuf<float4> atmb_scratch;
     DBuf<long long> atm_off;
     DBuf<int2> atm_ent;
     long long atm_cap = 0;
@@ -1083,7 +1094,7 @@ struct Engine {
         const void *fn = nullptr;
         size_t sm = 0;
         int blocks = 1;
-    } atm_occ_cache[4];
+    } atm_occ_cache[5];
     SurrState surr;
 
     ~Engine() {
@@ -1099,6 +1110,8 @@ struct Engine {
         w32.release();
         dw32.release();
         Y32.release();
+        D32.release();
+        atmb_scratch.release();
         xw_in.release();
         xs.release();
         atm_off.release();
@@ -1520,6 +1533,18 @@ void engine_fetch_results(Engine *e, double *energies, double *forces, double *s
     if (stresses) memcpy(stresses, h.data() + S + 3 * n, sizeof(double) * 9 * S);
 }
 
+// warps per CTA of the block-pair ATM kernel for this handle, 0 when it is not used
+// (plain form, surrogate, mirror schedule chosen, or the type count leaves too little
+// shared memory)
+static int blockpair_warps(const Engine *e) {
+    if (!e->use_atm || !e->opt.precision || e->opt.atm_schedule != 0) return 0;
+    if (e->opt.atm_surrogate && e->surr.loaded) return 0;
+    const size_t limit = 227 * 1024 - 1024; // opt-in maximum minus the static arrays
+    const size_t fixed = atmb_smem_fixed(e->ne, e->nref), per = atmb_smem_warp(e->ne);
+    if (fixed + 2 * per > limit) return 0;
+    return (int)std::min<size_t>(ATMB_MAXW, (limit - fixed) / per);
+}
+
 static KP make_kp(Engine *e) {
     KP p;
     memset(&p, 0, sizeof(p));
@@ -1561,6 +1586,13 @@ static KP make_kp(Engine *e) {
     p.w32 = e->w32.p;
     p.dw32 = e->dw32.p;
     p.Y32 = e->Y32.p;
+    p.D32 = nullptr;
+    p.atm_min_m = 0;
+    if (blockpair_warps(e) > 0) {
+        e->D32.ensure((size_t)e->max_atoms * e->ne * e->nref);
+        e->atmb_scratch.ensure((size_t)e->dev_sms * 3 * ATMB_MCAP);
+        p.D32 = e->D32.p;
+    }
     p.atm_force_scaled = e->opt.atm_force_scaled ? 1 : 0;
     p.pos_in = e->pos_in.p;
     p.type_in = e->type_in.p;
@@ -1723,6 +1755,15 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
             const int tmax = (int)std::max<size_t>(32, std::min<size_t>(256, (100 * 1024 - fixed) / per)) & ~31;
             const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(32, e->opt.atm_tile & ~31)) : std::min(tmax, 128);
             const size_t sm = (size_t)tile * per + fixed;
+            const int nwb = blockpair_warps(e);
+            if (nwb > 0 && !surr) {
+                // lists up to ATMB_MCAP entries: block-pair schedule; longer ones below
+                const size_t smb = atmb_smem_fixed(p.ne, NR) + (size_t)nwb * atmb_smem_warp(p.ne);
+                atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR>);
+                k_atm32b<NR><<<e->dev_sms, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
+                D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
+                pc.atm_min_m = ATMB_MCAP;
+            }
             const void *fn = surr ? (const void *)k_atm32<NR, true> : (const void *)k_atm32<NR, false>;
             const int blocks_per_sm = atm_occupancy(e, surr ? 3 : 1, sm, fn);
             const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
@@ -1775,7 +1816,8 @@ int engine_pass_times(Engine *e, float *ms, int cap, unsigned long long *counter
 
 int engine_launches_per_eval(const Engine *e) {
     if (!e->use_atm) return 12;
-    return (e->opt.atm_surrogate && e->surr.loaded) ? 20 : 16;
+    if (e->opt.atm_surrogate && e->surr.loaded) return 20;
+    return blockpair_warps(e) > 0 ? 17 : 16;
 }
 
 // Accuracy check of the Newton-refined helpers used by the ATM kernel against CUDA's

@@ -49,6 +49,8 @@ struct Options {
     int atm_tile = 0;              // ATM partner tile entries (0: largest that fits, <= 128)
     int atm_ctas_per_sm = 0;       // persistent ATM CTAs per SM (0: occupancy limit)
     bool atm_surrogate = false;    // learned ATM surrogate with exact fallback (needs a model)
+    int atm_schedule = 0;          // precision-form ATM: 0 block pairs (each triplet once),
+                                   // 1 mirror-symmetric full square (each triplet twice)
 };
 
 // Learned ATM surrogate: network parameters and normalisation (network in d3_mlp.h).

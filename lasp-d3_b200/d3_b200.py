@@ -24,6 +24,7 @@ ZERO_DAMPING, BJ_DAMPING = 0, 1
 OPT_ATM_FORCE_SCALED, OPT_SMOOTH_CN, OPT_PRECISION = 1, 2, 3
 OPT_BIN_DIVISOR, OPT_ATM_TILE, OPT_ATM_CTAS_PER_SM = 4, 5, 6
 OPT_ATM_SURROGATE = 7
+OPT_ATM_SCHEDULE = 8
 TABLE_5REF, TABLE_7REF = 0, 1
 
 _lib = None

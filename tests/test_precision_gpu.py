@@ -52,3 +52,39 @@ def test_precision_form_scaled_atm_forces():
     r = oracle.compute(sys_["pos"], sys_["Z"], sys_["cell"], atm_force_scaled=True, **kw)
     assert abs(e - r["energy"]) <= 1e-6 * abs(r["energy"])
     assert np.abs(f - r["forces"]).max() <= 1e-4
+
+
+@pytest.mark.parametrize("case", ["tric", "fe", "water"])
+def test_atm_schedules_agree(case):
+    """Block-pair schedule (each triplet once; lists longer than its cap go to the mirror
+    kernel) against the mirror-symmetric schedule (each triplet twice): the same in-range
+    triplets (visit counters equal) and the same energy, forces and stress to FP32 level."""
+    from d3_b200 import OPT_ATM_SCHEDULE
+
+    if case == "tric":
+        sys_, kw = S.triclinic_box(3000, seed=5), dict(rc=95.0, rc_cn=40.0, rc_atm=40.0)
+    elif case == "fe":
+        sys_ = S.gtest_bcc_fe(True)
+        sys_["pos"] = sys_["pos"] + np.random.default_rng(1).uniform(-0.1, 0.1, sys_["pos"].shape)
+        kw = dict(rc=30.0, rc_cn=30.0, rc_atm=30.0)
+    else:
+        sys_, kw = S.water_box(0), dict(rc=95.0, rc_cn=40.0, rc_atm=40.0)
+    out = []
+    for sched in (0, 1):
+        d = D3(sys_["Z"], len(sys_["Z"]), damping=1, functional=0, **kw)
+        d.set_option(OPT_PRECISION, 1)
+        d.set_option(OPT_ATM_SCHEDULE, sched)
+        d.set_cell(sys_["cell"])
+        d.set_atoms(sys_["pos"], sys_["Z"])
+        e, f, s = d.compute()
+        _, cnt = d.pass_times()
+        atm = d.atom_arrays()
+        out.append((e, f, s, int(cnt[0]), atm[2]))
+        d.close()
+    (e0, f0, s0, c0, a0), (e1, f1, s1, c1, a1) = out
+    assert c0 == c1 and c0 > 0
+    assert abs(e0 - e1) <= 1e-7 * abs(e1)
+    assert np.abs(f0 - f1).max() <= 1e-5 * np.abs(f1).max() + 1e-9
+    assert np.abs(s0 - s1).max() <= 1e-6 * np.abs(s1).max() + 1e-12
+    # per-atom energy shares (E/3 of every triplet through the atom) agree as well
+    assert np.abs(a0 - a1).max() <= 1e-6 * np.abs(a1).max()
