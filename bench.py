@@ -11,7 +11,9 @@ list + triplets, dE/dCN chain rule, reductions, E + F + stress):
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
 Multi-GPU (torchrun, one process per GPU): every rank evaluates its own box (different
-seed), no data-path collective; value = all atoms / max-over-ranks time ("weak").
+seed), no data-path collective; value = all atoms / max-over-ranks time ("weak"). With
+--shard the ranks evaluate ONE box together (d3_shard.py: round-robin split of central
+atoms and ATM apexes, NCCL all-reduce of dE/dCN and of the results; "strong").
 The reference arm times the reference's own CUDA build (oracle/_ref) through its C ABI
 on a bounded sample of the same generator (rank 0 only).
 """
@@ -359,6 +361,65 @@ def engine_arm(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def shard_arm(args, world, rank, local):
+    """One structure evaluated by all ranks (strong scaling): every world-th atom / ATM apex
+    per rank, all-reduce of dE/dCN and of the results (NCCL); precision form."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import d3_shard
+    from d3_b200 import D3, OPT_PRECISION
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % (29500 + os.getpid() % 1000), rank=0,
+                                world_size=1)
+    sys_ = system_for(args, 1)
+    n = len(sys_["Z"])
+    d = D3(sys_["Z"], n, rc=RC, rc_cn=RC_CN, rc_atm=None if args.no_atm else RC_ATM, damping=1, functional=0)
+    d.set_option(OPT_PRECISION, 1)
+    d.set_cell(sys_["cell"])
+    d.set_atoms(sys_["pos"], sys_["Z"])
+    ev = d3_shard.ShardedEvaluator(d)
+    for _ in range(args.warmup):
+        ev.compute_device()
+    dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s_ev.record()
+    for _ in range(args.steps):
+        ev.compute_device()
+    e_ev.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = sampler.stop()
+    ms = s_ev.elapsed_time(e_ev)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda" if world > 1 else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    out = ev.out.cpu().numpy()
+    if rank == 0:
+        line = {"metric": METRIC, "value": n * args.steps / (ms * 1e-3), "unit": "atoms/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": dict(workload_config(n, "precision form, sharded", args),
+                               parallelism="shard%d: central atoms and ATM apexes split round-robin over ranks; "
+                                           "all-reduce of dE/dCN (n doubles) and of the results (NCCL)" % world,
+                               l2="not flushed; the inputs are larger than L2 (ATM half lists about 330 MB at "
+                                  "20,000 atoms)"),
+                "energy_ev": float(out[0]), "clocks": clocks, "gpu_launches": d.launches_per_eval() * args.steps}
+        print(json.dumps(line), flush=True)
+    d.close()
+    dist.destroy_process_group()
+
+
 def reference_arm(args, world, rank, local):
     """The reference's own CUDA build (oracle/_ref/libd3_ref.so) through its C ABI."""
     if rank != 0:
@@ -621,6 +682,8 @@ def main():
     ap.add_argument("--system", choices=["triclinic", "water"], default="triclinic")
     ap.add_argument("--table", type=int, choices=[5, 7], default=5)
     ap.add_argument("--no-atm", action="store_true", help="two-body + CN only")
+    ap.add_argument("--shard", action="store_true",
+                    help="one structure over all ranks (strong scaling) instead of one replica per rank")
     ap.add_argument("--model", default=os.path.join(ROOT, "lasp-d3_b200", "surrogate", "atm_hcnosicu.d3s"))
     ap.add_argument("--seed", type=int, default=77)
     ap.add_argument("--batch", type=int, default=2048)
@@ -643,6 +706,8 @@ def main():
     args.atoms = args.atoms or N_ATOMS
     if args.impl == "reference":
         reference_arm(args, world, rank, local)
+    elif args.shard:
+        shard_arm(args, world, rank, local)
     else:
         engine_arm(args, world, rank, local)
 

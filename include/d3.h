@@ -256,6 +256,21 @@ int d3_mlp_adam(int n_channels, int members, float *params_dev, uint16_t *packed
                 const float *partial_dev, int splits, float lr, float beta1, float beta2, float eps,
                 float weight_decay, int step, void *cuda_stream);
 
+/* Sharded evaluation of one structure by `world` cooperating processes, one per GPU (no
+   counterpart in the reference). Every rank holds the same handle contents (atoms, cell,
+   options). d3_shard_begin computes the coordination numbers and C6 weights of every atom
+   and the two-body and ATM terms of this rank's share of the atoms (every world-th one),
+   and writes this rank's part of dE/dCN (d3_shard_length(handle) doubles) to dedcn_dev.
+   The caller sums dedcn_dev over the ranks (an all-reduce); d3_shard_end then runs the
+   dE/dCN chain rule for this rank's share and writes this rank's part of the results
+   (energies [S], forces [n][3], stresses [S][9], double, eV units, the layout of
+   d3_device_results) to results_dev; the sum of results_dev over the ranks is the result.
+   d3_shard_begin synchronises cuda_stream (it checks the neighbour-list capacity); the
+   learned surrogate is not available here. Returns the status word. */
+uint64_t d3_shard_length(d3_handle_t *handle);
+uint16_t d3_shard_begin(d3_handle_t *handle, int rank, int world, double *dedcn_dev, void *cuda_stream);
+uint16_t d3_shard_end(d3_handle_t *handle, const double *dedcn_dev, double *results_dev, void *cuda_stream);
+
 /* Last error message of this thread ("" if none). */
 const char *d3_last_error(void);
 

@@ -581,4 +581,29 @@ int d3_mlp_adam(int n_channels, int members, float *params_dev, uint16_t *packed
     }
 }
 
+// ---- sharded evaluation ---------------------------------------------------------------
+uint64_t d3_shard_length(d3_handle_t *handle) { return handle ? d3::engine_num_atoms(H(handle)->engine) : 0; }
+
+uint16_t d3_shard_begin(d3_handle_t *handle, int rank, int world, double *dedcn_dev, void *cuda_stream) {
+    if (!handle) {
+        set_error("handle is NULL in d3_shard_begin");
+        return 1;
+    }
+    std::string err;
+    const uint16_t st = d3::engine_shard_begin(H(handle)->engine, rank, world, dedcn_dev, (cudaStream_t)cuda_stream, err);
+    if (!err.empty()) set_error(err);
+    return st;
+}
+
+uint16_t d3_shard_end(d3_handle_t *handle, const double *dedcn_dev, double *results_dev, void *cuda_stream) {
+    if (!handle) {
+        set_error("handle is NULL in d3_shard_end");
+        return 1;
+    }
+    std::string err;
+    const uint16_t st = d3::engine_shard_end(H(handle)->engine, dedcn_dev, results_dev, (cudaStream_t)cuda_stream, err);
+    if (!err.empty()) set_error(err);
+    return st;
+}
+
 } // extern "C"

@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
         if (tid == 0) s_item = atomicAdd(p.work, 1);
         if (tid < ATM_SHELLS) shell_cnt[tid] = 0;
         __syncthreads();
-        const int item = s_item;
+        const int item = CENTER ? s_item : s_item * p.shard_world + p.shard_rank;
         if (item >= (CENTER ? *p.atm_napex : p.n)) break;
         const int a = CENTER ? p.atm_apex[item] : p.sorted_of[p.n - 1 - item];
         const long long e0 = p.atm_off[a];

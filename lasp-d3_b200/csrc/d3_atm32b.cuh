@@ -232,7 +232,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         __syncthreads();
         if (tid == 0) s_item = atomicAdd(p.work, 1);
         __syncthreads();
-        const int item = s_item;
+        const int item = s_item * p.shard_world + p.shard_rank;
         if (item >= p.n) break;
         const int a = p.sorted_of[p.n - 1 - item];
         const long long e0 = p.atm_off[a];

@@ -118,6 +118,10 @@ struct KP {
     float *w32, *dw32, *Y32;
     float *D32;     // [n][ne][NR]: d/dCN of the own weights through the C6 rows (block-pair ATM)
     int atm_min_m;  // k_atm32 takes only apexes with longer lists (the rest: k_atm32b)
+    // sharded evaluation: this process computes the two-body and chain-rule terms of central
+    // atoms i = shard_rank + k shard_world (binned order) and the ATM apexes of work items
+    // shard_rank + k shard_world; CN and weights for every atom
+    int shard_rank, shard_world;
     // work counters: [0] ATM in-range visits (2 per triplet), [1] two-body in-range
     // ordered pairs, [2] CN in-range ordered pairs
     unsigned long long *counters;
@@ -128,6 +132,8 @@ __device__ __forceinline__ int floordiv(int a, int b) {
     if ((a % b != 0) && ((a < 0) != (b < 0))) --q;
     return q;
 }
+
+__device__ __forceinline__ int shard_atom(const KP &p, int w) { return w * p.shard_world + p.shard_rank; }
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -417,7 +423,7 @@ __global__ void k_weights(KP p) {
 // ------------------------------------------------------------------------------------
 template <int NR>
 __global__ void k_twobody(KP p) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int i = shard_atom(p, (blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (i >= p.n) return;
     const SG &g = p.sg[p.sid[i]];
     const double4 xi = p.xs[i];
@@ -533,7 +539,8 @@ __global__ void k_atm_list(KP p) {
     if (FILL) pos = p.atm_off[a];
     int count = 0;
     bool range_err = false;
-    if (p.atm_center && !p.surr_flag[a]) {
+    if ((p.atm_center && !p.surr_flag[a]) ||
+        (p.shard_world > 1 && (p.n - 1 - oa) % p.shard_world != p.shard_rank)) {
         if (!FILL && lane == 0) p.atm_cnt[a] = 0;
         return;
     }
@@ -624,7 +631,7 @@ __global__ void k_cn32(KP p) {
 
 template <int NR>
 __global__ void k_twobody32(KP p) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int i = shard_atom(p, (blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (i >= p.n) return;
     const SG &g = p.sg[p.sid[i]];
     const float4 xi = p.xs32[i];
@@ -743,7 +750,7 @@ __global__ void k_twobody32(KP p) {
 }
 
 __global__ void k_chain32(KP p, const double *Gd) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int i = shard_atom(p, (blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (i >= p.n) return;
     const SG &g = p.sg[p.sid[i]];
     const float4 xi = p.xs32[i];
@@ -887,7 +894,7 @@ __global__ void k_surr_export(KP p, const float *G, const int *center, int nfeat
 // chain rule (src/d3_kernel.cu:1511-1698): F_i += (dE/dCN_i + dE/dCN_j) dCN_ij/dr r_hat
 // ------------------------------------------------------------------------------------
 __global__ void k_chain(KP p, const double *G) {
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int i = shard_atom(p, (blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (i >= p.n) return;
     const SG &g = p.sg[p.sid[i]];
     const double4 xi = p.xs[i];
@@ -1096,6 +1103,7 @@ struct Engine {
         int blocks = 1;
     } atm_occ_cache[5];
     SurrState surr;
+    int shard_rank = 0, shard_world = 0; // set by engine_shard_begin
 
     ~Engine() {
         DBuf<double> *ds[] = {&t_cnref, &t_c6, &t_r0, &t_rcov, &t_r2r4, &t_pairA, &pos_in, &cn, &w, &dw, &Y, &e2,
@@ -1548,6 +1556,8 @@ static int blockpair_warps(const Engine *e) {
 static KP make_kp(Engine *e) {
     KP p;
     memset(&p, 0, sizeof(p));
+    p.shard_rank = 0;
+    p.shard_world = 1;
     p.n = (int)e->n;
     p.nstruct = e->nstruct;
     p.nbins_total = e->nbins_total;
@@ -1675,128 +1685,149 @@ static d3mlp::Net surr_net(const SurrState &S) {
     return net;
 }
 
+// stage 0: the whole evaluation; stage 1: everything up to the summed dE/dCN (written to
+// G_ext when given); stage 2: chain rule (dE/dCN read from G_ext), forces and reductions.
+// Stages 1 and 2 with an all-reduce of dE/dCN between them make a sharded evaluation.
 template <int NR>
-static void launch_all(Engine *e, const KP &p0, cudaStream_t s) {
+static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, double *G_ext = nullptr) {
     KP p = p0;
     const int n = p.n;
     const int T = 256;
     const int gb = (n + T - 1) / T;
     const int gw = (int)(((long long)n * 32 + T - 1) / T);
     cudaEvent_t *ev = e->ev;
-    D3_CUDA(cudaEventRecord(ev[0], s));
-    D3_CUDA(cudaMemsetAsync(p.counters, 0, sizeof(unsigned long long) * 4, s));
-    D3_CUDA(cudaMemsetAsync(p.bin_cnt, 0, sizeof(int) * p.nbins_total, s));
-    D3_CUDA(cudaMemsetAsync(p.bin_fill, 0, sizeof(int) * p.nbins_total, s));
-    k_bin<<<gb, T, 0, s>>>(p);
-    k_scan<int, int><<<1, 1024, 0, s>>>(p.bin_cnt, p.bin_start, p.nbins_total);
-    k_scatter<<<gb, T, 0, s>>>(p);
-    k_binsort<<<(p.nbins_total + T - 1) / T, T, 0, s>>>(p);
-    k_gather<<<gb, T, 0, s>>>(p);
-    D3_CUDA(cudaEventRecord(ev[1], s));
-    if (p.precision)
-        k_cn32<<<gw, T, 0, s>>>(p);
-    else
-        k_cn<<<gw, T, 0, s>>>(p);
-    k_weights<NR><<<gb, T, 0, s>>>(p);
-    D3_CUDA(cudaEventRecord(ev[2], s));
-    if (p.precision)
-        k_twobody32<NR><<<gw, T, 0, s>>>(p);
-    else
-        k_twobody<NR><<<gw, T, 0, s>>>(p);
-    D3_CUDA(cudaEventRecord(ev[3], s));
-    D3_CUDA(cudaMemsetAsync(p.ea, 0, sizeof(double) * n, s));
-    D3_CUDA(cudaMemsetAsync(p.ga, 0, sizeof(double) * n, s));
-    D3_CUDA(cudaMemsetAsync(p.fa, 0, sizeof(double) * 3 * n, s));
-    D3_CUDA(cudaMemsetAsync(p.va, 0, sizeof(double) * 6 * n, s));
-    D3_CUDA(cudaMemsetAsync(p.eb, 0, sizeof(double) * n, s));
-    D3_CUDA(cudaMemsetAsync(p.gb, 0, sizeof(double) * n, s));
-    D3_CUDA(cudaMemsetAsync(p.fb, 0, sizeof(double) * 3 * n, s));
-    // learned surrogate: descriptors -> ensemble -> fallback flags; the exact ATM pass
-    // below then runs in centre mode over the flagged atoms only
-    const bool surr = e->use_atm && e->opt.atm_surrogate && e->surr.loaded;
-    KP pc = p;
-    SurrDesc sd{};
-    if (surr) {
-        SurrState &S = e->surr;
-        sd = surr_desc(S.chan.p, S.L.nch, S.G.p, S.dX.p, S.center.p);
-        k_desc_fwd<NR><<<gw, T, 0, s>>>(p, sd);
-        d3mlp::infer(surr_net(S), S.G.p, S.center.p, n, S.E.p, S.dX.p, e->dev_sms, s);
-        D3_CUDA(cudaMemsetAsync(S.napex.p, 0, sizeof(int), s));
-        SurrComb c{};
-        c.E = S.E.p;
-        c.dX = S.dX.p;
-        c.center = S.center.p;
-        c.e_shift = S.e_shift.p;
-        c.e_scale = S.e_scale;
-        c.members = S.members;
-        c.nfeat = S.L.nch * SURR_NRBF;
-        c.thr = S.thr_ev;
-        c.flag = S.flag.p;
-        c.apex = S.apex.p;
-        c.napex = S.napex.p;
-        k_surr_combine<<<gw, T, 0, s>>>(p, c);
-        pc.atm_center = 1;
-        pc.atm_apex = S.apex.p;
-        pc.atm_napex = S.napex.p;
-        pc.surr_flag = S.flag.p;
-    }
-    if (e->use_atm) {
-        k_atm_list<false><<<gw, T, 0, s>>>(pc);
-        k_scan<long long, int><<<1, 1024, 0, s>>>(p.atm_cnt, p.atm_off, n);
-        k_atm_list<true><<<gw, T, 0, s>>>(pc);
-    }
-    D3_CUDA(cudaEventRecord(ev[4], s));
-    if (e->use_atm) {
-        D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
-        if (p.precision) {
-            const size_t fixed = (size_t)p.ne * NR * sizeof(double) + ((p.ne * p.ne + 3) & ~3) * sizeof(float) +
-                                 ATM_PERM_CAP * sizeof(unsigned short) + 11 * ATM_THREADS * sizeof(double);
-            const size_t per = 2 * sizeof(float4) + sizeof(int2) + (size_t)p.ne * 2 * sizeof(float4);
-            const int tmax = (int)std::max<size_t>(32, std::min<size_t>(256, (100 * 1024 - fixed) / per)) & ~31;
-            const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(32, e->opt.atm_tile & ~31)) : std::min(tmax, 128);
-            const size_t sm = (size_t)tile * per + fixed;
-            const int nwb = blockpair_warps(e);
-            if (nwb > 0 && !surr) {
-                // lists up to ATMB_MCAP entries: block-pair schedule; longer ones below
-                const size_t smb = atmb_smem_fixed(p.ne, NR) + (size_t)nwb * atmb_smem_warp(p.ne);
-                atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR>);
-                k_atm32b<NR><<<e->dev_sms, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
-                D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
-                pc.atm_min_m = ATMB_MCAP;
-            }
-            const void *fn = surr ? (const void *)k_atm32<NR, true> : (const void *)k_atm32<NR, false>;
-            const int blocks_per_sm = atm_occupancy(e, surr ? 3 : 1, sm, fn);
-            const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
-            const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, per_sm)));
-            if (surr)
-                k_atm32<NR, true><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
-            else
-                k_atm32<NR, false><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
-        } else {
-            // partner tile: as many entries as fit in ~160 KB next to the apex tables
-            const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double) +
-                                 ATM_PERM_CAP * sizeof(unsigned short);
-            const size_t per = sizeof(Partner) + (size_t)p.ne * NR * sizeof(double);
-            const int tmax = (int)std::max<size_t>(8, std::min<size_t>(256, (160 * 1024 - fixed) / per));
-            const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(8, e->opt.atm_tile)) : std::min(tmax, 128);
-            const size_t sm = (size_t)tile * per + fixed;
-            const void *fn = surr ? (const void *)k_atm<NR, true> : (const void *)k_atm<NR, false>;
-            const int blocks_per_sm = atm_occupancy(e, surr ? 2 : 0, sm, fn);
-            const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
-            const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, per_sm)));
-            if (surr)
-                k_atm<NR, true><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
-            else
-                k_atm<NR, false><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
+    double *Gsum = G_ext ? G_ext : e->G.p;
+    if (stage != 2) {
+        D3_CUDA(cudaEventRecord(ev[0], s));
+        D3_CUDA(cudaMemsetAsync(p.counters, 0, sizeof(unsigned long long) * 4, s));
+        D3_CUDA(cudaMemsetAsync(p.bin_cnt, 0, sizeof(int) * p.nbins_total, s));
+        D3_CUDA(cudaMemsetAsync(p.bin_fill, 0, sizeof(int) * p.nbins_total, s));
+        k_bin<<<gb, T, 0, s>>>(p);
+        k_scan<int, int><<<1, 1024, 0, s>>>(p.bin_cnt, p.bin_start, p.nbins_total);
+        k_scatter<<<gb, T, 0, s>>>(p);
+        k_binsort<<<(p.nbins_total + T - 1) / T, T, 0, s>>>(p);
+        k_gather<<<gb, T, 0, s>>>(p);
+        D3_CUDA(cudaEventRecord(ev[1], s));
+        if (p.precision)
+            k_cn32<<<gw, T, 0, s>>>(p);
+        else
+            k_cn<<<gw, T, 0, s>>>(p);
+        k_weights<NR><<<gb, T, 0, s>>>(p);
+        D3_CUDA(cudaEventRecord(ev[2], s));
+        if (p.shard_world > 1) {
+            // only this shard's central atoms are written
+            D3_CUDA(cudaMemsetAsync(p.e2, 0, sizeof(double) * n, s));
+            D3_CUDA(cudaMemsetAsync(p.g2, 0, sizeof(double) * n, s));
+            D3_CUDA(cudaMemsetAsync(p.f2, 0, sizeof(double) * 3 * n, s));
+            D3_CUDA(cudaMemsetAsync(p.v2, 0, sizeof(double) * 6 * n, s));
         }
-        if (surr) k_desc_bwd<NR><<<gw, T, 0, s>>>(p, sd);
+        if (p.precision)
+            k_twobody32<NR><<<gw, T, 0, s>>>(p);
+        else
+            k_twobody<NR><<<gw, T, 0, s>>>(p);
+        D3_CUDA(cudaEventRecord(ev[3], s));
+        D3_CUDA(cudaMemsetAsync(p.ea, 0, sizeof(double) * n, s));
+        D3_CUDA(cudaMemsetAsync(p.ga, 0, sizeof(double) * n, s));
+        D3_CUDA(cudaMemsetAsync(p.fa, 0, sizeof(double) * 3 * n, s));
+        D3_CUDA(cudaMemsetAsync(p.va, 0, sizeof(double) * 6 * n, s));
+        D3_CUDA(cudaMemsetAsync(p.eb, 0, sizeof(double) * n, s));
+        D3_CUDA(cudaMemsetAsync(p.gb, 0, sizeof(double) * n, s));
+        D3_CUDA(cudaMemsetAsync(p.fb, 0, sizeof(double) * 3 * n, s));
+        // learned surrogate: descriptors -> ensemble -> fallback flags; the exact ATM pass
+        // below then runs in centre mode over the flagged atoms only
+        const bool surr = e->use_atm && e->opt.atm_surrogate && e->surr.loaded;
+        KP pc = p;
+        SurrDesc sd{};
+        if (surr) {
+            SurrState &S = e->surr;
+            sd = surr_desc(S.chan.p, S.L.nch, S.G.p, S.dX.p, S.center.p);
+            k_desc_fwd<NR><<<gw, T, 0, s>>>(p, sd);
+            d3mlp::infer(surr_net(S), S.G.p, S.center.p, n, S.E.p, S.dX.p, e->dev_sms, s);
+            D3_CUDA(cudaMemsetAsync(S.napex.p, 0, sizeof(int), s));
+            SurrComb c{};
+            c.E = S.E.p;
+            c.dX = S.dX.p;
+            c.center = S.center.p;
+            c.e_shift = S.e_shift.p;
+            c.e_scale = S.e_scale;
+            c.members = S.members;
+            c.nfeat = S.L.nch * SURR_NRBF;
+            c.thr = S.thr_ev;
+            c.flag = S.flag.p;
+            c.apex = S.apex.p;
+            c.napex = S.napex.p;
+            k_surr_combine<<<gw, T, 0, s>>>(p, c);
+            pc.atm_center = 1;
+            pc.atm_apex = S.apex.p;
+            pc.atm_napex = S.napex.p;
+            pc.surr_flag = S.flag.p;
+        }
+        if (e->use_atm) {
+            k_atm_list<false><<<gw, T, 0, s>>>(pc);
+            k_scan<long long, int><<<1, 1024, 0, s>>>(p.atm_cnt, p.atm_off, n);
+            k_atm_list<true><<<gw, T, 0, s>>>(pc);
+        }
+        D3_CUDA(cudaEventRecord(ev[4], s));
+        if (e->use_atm) {
+            D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
+            if (p.precision) {
+                const size_t fixed = (size_t)p.ne * NR * sizeof(double) + ((p.ne * p.ne + 3) & ~3) * sizeof(float) +
+                                     ATM_PERM_CAP * sizeof(unsigned short) + 11 * ATM_THREADS * sizeof(double);
+                const size_t per = 2 * sizeof(float4) + sizeof(int2) + (size_t)p.ne * 2 * sizeof(float4);
+                const int tmax = (int)std::max<size_t>(32, std::min<size_t>(256, (100 * 1024 - fixed) / per)) & ~31;
+                const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(32, e->opt.atm_tile & ~31)) : std::min(tmax, 128);
+                const size_t sm = (size_t)tile * per + fixed;
+                const int nwb = blockpair_warps(e);
+                if (nwb > 0 && !surr) {
+                    // lists up to ATMB_MCAP entries: block-pair schedule; longer ones below
+                    const size_t smb = atmb_smem_fixed(p.ne, NR) + (size_t)nwb * atmb_smem_warp(p.ne);
+                    atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR>);
+                    k_atm32b<NR><<<e->dev_sms, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
+                    D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
+                    pc.atm_min_m = ATMB_MCAP;
+                }
+                const void *fn = surr ? (const void *)k_atm32<NR, true> : (const void *)k_atm32<NR, false>;
+                const int blocks_per_sm = atm_occupancy(e, surr ? 3 : 1, sm, fn);
+                const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
+                const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, per_sm)));
+                if (surr)
+                    k_atm32<NR, true><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
+                else
+                    k_atm32<NR, false><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
+            } else {
+                // partner tile: as many entries as fit in ~160 KB next to the apex tables
+                const size_t fixed = (size_t)p.ne * NR * sizeof(double) + (size_t)p.ne * p.ne * sizeof(double) +
+                                     ATM_PERM_CAP * sizeof(unsigned short);
+                const size_t per = sizeof(Partner) + (size_t)p.ne * NR * sizeof(double);
+                const int tmax = (int)std::max<size_t>(8, std::min<size_t>(256, (160 * 1024 - fixed) / per));
+                const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(8, e->opt.atm_tile)) : std::min(tmax, 128);
+                const size_t sm = (size_t)tile * per + fixed;
+                const void *fn = surr ? (const void *)k_atm<NR, true> : (const void *)k_atm<NR, false>;
+                const int blocks_per_sm = atm_occupancy(e, surr ? 2 : 0, sm, fn);
+                const int per_sm = e->opt.atm_ctas_per_sm > 0 ? std::min(e->opt.atm_ctas_per_sm, blocks_per_sm) : blocks_per_sm;
+                const int grid = std::max(1, std::min(n, e->dev_sms * std::max(1, per_sm)));
+                if (surr)
+                    k_atm<NR, true><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
+                else
+                    k_atm<NR, false><<<grid, ATM_THREADS, sm, s>>>(pc, tile);
+            }
+            if (surr) k_desc_bwd<NR><<<gw, T, 0, s>>>(p, sd);
+        }
+        D3_CUDA(cudaEventRecord(ev[5], s));
+        k_sum_g<<<gb, T, 0, s>>>(p, Gsum);
+        if (stage == 1) {
+            D3_CUDA(cudaGetLastError());
+            return;
+        }
+    } // stage != 2
+    if (p.shard_world > 1) {
+        D3_CUDA(cudaMemsetAsync(p.fc, 0, sizeof(double) * 3 * n, s));
+        D3_CUDA(cudaMemsetAsync(p.vc, 0, sizeof(double) * 6 * n, s));
     }
-    D3_CUDA(cudaEventRecord(ev[5], s));
-    k_sum_g<<<gb, T, 0, s>>>(p, e->G.p);
     if (p.precision)
-        k_chain32<<<gw, T, 0, s>>>(p, e->G.p);
+        k_chain32<<<gw, T, 0, s>>>(p, Gsum);
     else
-        k_chain<<<gw, T, 0, s>>>(p, e->G.p);
+        k_chain<<<gw, T, 0, s>>>(p, Gsum);
     D3_CUDA(cudaEventRecord(ev[6], s));
     k_forces_out<<<gb, T, 0, s>>>(p);
     k_reduce<<<p.nstruct, 256, 0, s>>>(p);
@@ -1903,23 +1934,26 @@ int engine_selftest_math(double max_rel[6]) {
     return 0;
 }
 
+// initial ATM list capacity from each structure's density over the half sphere
+static void ensure_atm_capacity(Engine *e) {
+    if (!e->use_atm || e->atm_cap != 0) return;
+    double cap = 0.0;
+    for (int k = 0; k < e->nstruct; ++k) {
+        const double nk = (double)e->sg[k].natoms;
+        const double rho = nk / std::fabs(e->geoms[k].volume);
+        const double k_half = 0.5 * rho * 4.18879020478639 * e->rc_atm * e->rc_atm * e->rc_atm;
+        cap += nk * (k_half * 1.25 + 64.0);
+    }
+    e->atm_cap = (long long)cap + 1024;
+    e->atm_ent.ensure((size_t)e->atm_cap);
+}
+
 uint16_t engine_compute(Engine *e, double *energy, double *forces, double *stress, cudaStream_t stream, bool sync) {
     if (!e->atoms_set || !e->cell_set) return ST_NOT_READY;
     cudaStream_t s = stream ? stream : e->stream;
     try {
         const uint64_t n = e->n;
-        if (e->use_atm && e->atm_cap == 0) {
-            // initial list capacity from each structure's density over the half sphere
-            double cap = 0.0;
-            for (int k = 0; k < e->nstruct; ++k) {
-                const double nk = (double)e->sg[k].natoms;
-                const double rho = nk / std::fabs(e->geoms[k].volume);
-                const double k_half = 0.5 * rho * 4.18879020478639 * e->rc_atm * e->rc_atm * e->rc_atm;
-                cap += nk * (k_half * 1.25 + 64.0);
-            }
-            e->atm_cap = (long long)cap + 1024;
-            e->atm_ent.ensure((size_t)e->atm_cap);
-        }
+        ensure_atm_capacity(e);
         for (int attempt = 0; attempt < 4; ++attempt) {
             D3_CUDA(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned int), s));
             KP p = make_kp(e);
@@ -2137,6 +2171,75 @@ int engine_surrogate_descriptors(Engine *e, const int *channel_z, int nch, float
     } catch (const std::exception &ex) {
         err = ex.what();
         return -1;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// sharded evaluation of one structure over several processes
+// ------------------------------------------------------------------------------------
+uint16_t engine_shard_begin(Engine *e, int rank, int world, double *G_out, cudaStream_t stream, std::string &err) {
+    if (!e->atoms_set || !e->cell_set) return ST_NOT_READY;
+    if (world < 1 || rank < 0 || rank >= world || !G_out) {
+        err = "shard: rank must be in [0, world) and the dE/dCN buffer given";
+        return ST_BAD_INPUT;
+    }
+    if (e->opt.atm_surrogate && e->surr.loaded) {
+        err = "shard: the learned surrogate is not available in a sharded evaluation";
+        return ST_BAD_INPUT;
+    }
+    cudaStream_t s = stream ? stream : e->stream;
+    try {
+        ensure_atm_capacity(e);
+        for (int attempt = 0; attempt < 4; ++attempt) {
+            D3_CUDA(cudaMemsetAsync(e->status.p, 0, sizeof(unsigned int), s));
+            KP p = make_kp(e);
+            p.shard_rank = rank;
+            p.shard_world = world;
+            if (e->nref == 5)
+                launch_all<5>(e, p, s, 1, G_out);
+            else
+                launch_all<7>(e, p, s, 1, G_out);
+            unsigned int st = 0;
+            D3_CUDA(cudaMemcpyAsync(&st, e->status.p, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+            D3_CUDA(cudaStreamSynchronize(s));
+            if ((st & ST_LIST_OVERFLOW) && e->use_atm) {
+                long long need = 0;
+                D3_CUDA(cudaMemcpy(&need, e->atm_off.p + e->n, sizeof(long long), cudaMemcpyDeviceToHost));
+                e->atm_cap = (long long)(need * 1.1) + 1024;
+                e->atm_ent.ensure((size_t)e->atm_cap);
+                continue;
+            }
+            e->shard_rank = rank;
+            e->shard_world = world;
+            return (uint16_t)st;
+        }
+        return ST_LIST_OVERFLOW;
+    } catch (const std::exception &ex) {
+        err = ex.what();
+        return ST_CUDA_ERROR;
+    }
+}
+
+uint16_t engine_shard_end(Engine *e, const double *G_in, double *out_dev, cudaStream_t stream, std::string &err) {
+    if (e->shard_world < 1 || !G_in || !out_dev) {
+        err = "shard: d3_shard_begin first, and give the dE/dCN and result buffers";
+        return ST_NOT_READY;
+    }
+    cudaStream_t s = stream ? stream : e->stream;
+    try {
+        KP p = make_kp(e);
+        p.shard_rank = e->shard_rank;
+        p.shard_world = e->shard_world;
+        if (e->nref == 5)
+            launch_all<5>(e, p, s, 2, const_cast<double *>(G_in));
+        else
+            launch_all<7>(e, p, s, 2, const_cast<double *>(G_in));
+        const size_t nout = 10 * (size_t)e->nstruct + 3 * (size_t)e->n;
+        D3_CUDA(cudaMemcpyAsync(out_dev, e->out.p, sizeof(double) * nout, cudaMemcpyDeviceToDevice, s));
+        return ST_OK;
+    } catch (const std::exception &ex) {
+        err = ex.what();
+        return ST_CUDA_ERROR;
     }
 }
 

@@ -119,6 +119,15 @@ int engine_surrogate_flagged(Engine *e);
 // triplet), each output skipped when null
 int engine_surrogate_descriptors(Engine *e, const int *channel_z, int nch, float *G_dev, int *center_dev,
                                  double *e_atm_dev, cudaStream_t stream, std::string &err);
+// Sharded evaluation of one structure by `world` processes: stage 1 (CN and weights of
+// every atom; two-body and ATM of this rank's share) writes this rank's partial dE/dCN
+// [n] (binned order) to G_out; the caller sums G over the ranks (all-reduce) and stage 2
+// (chain rule of this rank's share, forces, reductions) writes this rank's partial
+// results [S energies, 3n forces, 9S stresses] (eV units, caller order) to out_dev; the
+// caller sums them over the ranks. Stage 1 synchronises its stream (list capacity).
+uint16_t engine_shard_begin(Engine *e, int rank, int world, double *G_out, cudaStream_t stream, std::string &err);
+uint16_t engine_shard_end(Engine *e, const double *G_in, double *out_dev, cudaStream_t stream, std::string &err);
+
 // diagnostics for tests: coordination numbers, dE/dCN, per-atom energies (hartree),
 // in the caller's atom order; ATM list (caller indices and reference lattice shifts)
 int engine_debug_atom_arrays(Engine *e, double *cn, double *dedcn, double *energy_atoms);

@@ -121,6 +121,12 @@ def load_library(path=None):
     lib.d3_mlp_forward.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, ci, vp, vp, vp]
     lib.d3_mlp_train_batch.restype = ci
     lib.d3_mlp_train_batch.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, ci, vp, vp, vp, vp, vp]
+    lib.d3_shard_length.restype = u64
+    lib.d3_shard_length.argtypes = [vp]
+    lib.d3_shard_begin.restype = ctypes.c_uint16
+    lib.d3_shard_begin.argtypes = [vp, ci, ci, vp, vp]
+    lib.d3_shard_end.restype = ctypes.c_uint16
+    lib.d3_shard_end.argtypes = [vp, vp, vp, vp]
     lib.d3_mlp_adam.restype = ci
     lib.d3_mlp_adam.argtypes = [ci, ci, vp, vp, vp, vp, vp, ci, f32, f32, f32, f32, f32, ci, vp]
     if path is None:
@@ -189,7 +195,26 @@ class _Surrogate:
             raise RuntimeError(self.lib.d3_last_error().decode())
 
 
-class D3(_Surrogate):
+class _Shard:
+    """Sharded-evaluation stages shared by D3 and D3Batch (driver: d3_shard.py)."""
+
+    def shard_length(self):
+        return int(self.lib.d3_shard_length(self.h))
+
+    def shard_begin(self, rank, world, dedcn_ptr, stream_ptr=None):
+        st = int(self.lib.d3_shard_begin(self.h, int(rank), int(world), ctypes.c_void_p(dedcn_ptr),
+                                         ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+        if st:
+            raise RuntimeError("d3_shard_begin status %d: %s" % (st, self.lib.d3_last_error().decode()))
+
+    def shard_end(self, dedcn_ptr, results_ptr, stream_ptr=None):
+        st = int(self.lib.d3_shard_end(self.h, ctypes.c_void_p(dedcn_ptr), ctypes.c_void_p(results_ptr),
+                                       ctypes.c_void_p(stream_ptr) if stream_ptr else None))
+        if st:
+            raise RuntimeError("d3_shard_end status %d: %s" % (st, self.lib.d3_last_error().decode()))
+
+
+class D3(_Surrogate, _Shard):
     """One engine handle (FP64 path)."""
 
     def __init__(self, elements, max_atoms, rc=95.0, rc_cn=40.0, rc_atm=None, damping=BJ_DAMPING, functional=0,
@@ -295,7 +320,7 @@ class D3(_Surrogate):
             pass
 
 
-class D3Batch(_Surrogate):
+class D3Batch(_Surrogate, _Shard):
     """Many independent periodic structures in one handle (batching form)."""
 
     def __init__(self, elements, max_structures, max_total_atoms, rc=95.0, rc_cn=40.0, rc_atm=None,
