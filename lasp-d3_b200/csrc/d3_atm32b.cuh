@@ -108,7 +108,7 @@ struct AtmbSide {
 // corrections where the virial and force weights differ.
 // Branch-free: an out-of-range pair (act false) runs on safe stand-in values with zero
 // weights, so the two visits of an iteration can be interleaved by the compiler.
-template <int NR>
+template <int NR, bool SIMPLE>
 __device__ __forceinline__ void atmb_visit(const AtmbX &X, int k, const float4 ya, float d3in, bool act,
                                            const float4 *yB, const int4 *yJ, const float4 *yW0, const float4 *yW1,
                                            const float4 *yD0, const float4 *yD1, const float2 *xrow, int lane,
@@ -132,12 +132,18 @@ __device__ __forceinline__ void atmb_visit(const AtmbX &X, int k, const float4 y
     const float s3 = c6 * is3;
     const float lam_xy = act ? dcx * is3 * is3 : 0.0f, lam_yx = act ? dcy * is3 * is3 : 0.0f;
     const float u = r0sq[X.tx * ne + ty] * id3;
-    const float g3 = u * u * u * exp2f(__log2f(u) * (-1.0f / 3.0f));
-    // reference scale factors (src/d3_kernel.cu:1282-1290) as pair weights
-    const bool same = (X.jx == yj.x);
-    const bool apex_img = X.qa | (yj.x == a);
-    const float w = act ? (same ? (X.qa ? third : 1.0f) : (apex_img ? 0.5f : 1.0f)) : 0.0f;
-    const float wf = act ? (force_scaled ? w : (same ? 2.0f : 1.0f)) : 0.0f;
+    const float g3 = exp2f(__log2f(u) * (8.0f / 3.0f)); // u^(8/3)
+    // reference scale factors (src/d3_kernel.cu:1282-1290) as pair weights; SIMPLE: no
+    // atom appears twice in the list (cell heights > 2 rc_ATM), every weight is 1
+    float w, wf;
+    if (SIMPLE) {
+        w = wf = act ? 1.0f : 0.0f;
+    } else {
+        const bool same = (X.jx == yj.x);
+        const bool apex_img = X.qa | (yj.x == a);
+        w = act ? (same ? (X.qa ? third : 1.0f) : (apex_img ? 0.5f : 1.0f)) : 0.0f;
+        wf = act ? (force_scaled ? w : (same ? 2.0f : 1.0f)) : 0.0f;
+    }
     const float d1 = X.d1, d2 = act ? ya.w : X.d1;
     const float irsq = X.id1 * yb.y * id3;
     const float ir9 = irsq * X.ir1 * yb.x * ir3;
@@ -168,9 +174,11 @@ __device__ __forceinline__ void atmb_visit(const AtmbX &X, int k, const float4 y
     xt.Wy = fmaf(wf3, ya.y, xt.Wy);
     xt.Wz = fmaf(wf3, ya.z, xt.Wz);
     xt.SA = fmaf(wf, f1, xt.SA);
-    xt.Ux = fmaf(w3, ya.x, xt.Ux);
-    xt.Uy = fmaf(w3, ya.y, xt.Uy);
-    xt.Uz = fmaf(w3, ya.z, xt.Uz);
+    if (!SIMPLE) { // SIMPLE: U = W
+        xt.Ux = fmaf(w3, ya.x, xt.Ux);
+        xt.Uy = fmaf(w3, ya.y, xt.Uy);
+        xt.Uz = fmaf(w3, ya.z, xt.Uz);
+    }
     ys.SE += wE;
     ys.SD = fmaf(wE, lam_yx, ys.SD);
     ys.SF = fmaf(wf, f2 + f3, ys.SF);
@@ -181,7 +189,7 @@ __device__ __forceinline__ void atmb_visit(const AtmbX &X, int k, const float4 y
     aFx = fmaf(wf2, ya.x, aFx);
     aFy = fmaf(wf2, ya.y, aFy);
     aFz = fmaf(wf2, ya.z, aFz);
-    if (w != wf) {
+    if (!SIMPLE && w != wf) {
         // virial weights w where the force weights differ (repeated indices)
         const double c1 = (double)(w - wf) * (double)(f1 + f3), c2 = (double)(w - wf) * (double)(f2 + f3);
         apx[3] += c1 * X.vx * X.vx + c2 * ya.x * ya.x;
@@ -241,6 +249,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         const double4 xa = p.xs[a];
         const int ta = (int)xa.w;
         const SG &g = p.sg[p.sid[a]];
+        const bool simple = g.atm_simple != 0;
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
         for (int k = tid; k < 512; k += blockDim.x) cellpos[k] = 0;
         for (int q = 0; q < 6; ++q)
@@ -427,10 +436,17 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
                     const bool act1 = xvalid && (!diag || s + 1 < 16 || lane < 16) && d31 <= ratm2f && d31 >= 1e-12f;
                     if (__any_sync(0xffffffffu, act0 || act1)) {
                         visits += (act0 ? 2 : 0) + (act1 ? 2 : 0);
-                        atmb_visit<NR>(X, k0, ya0, d30, act0, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq, ne, a, x16c,
-                                       third, force_scaled, xt, y0, aFx, aFy, aFz, apx);
-                        atmb_visit<NR>(X, k1, ya1, d31, act1, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq, ne, a, x16c,
-                                       third, force_scaled, xt, y1, aFx, aFy, aFz, apx);
+                        if (simple) {
+                            atmb_visit<NR, true>(X, k0, ya0, d30, act0, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq,
+                                                 ne, a, x16c, third, force_scaled, xt, y0, aFx, aFy, aFz, apx);
+                            atmb_visit<NR, true>(X, k1, ya1, d31, act1, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq,
+                                                 ne, a, x16c, third, force_scaled, xt, y1, aFx, aFy, aFz, apx);
+                        } else {
+                            atmb_visit<NR, false>(X, k0, ya0, d30, act0, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq,
+                                                  ne, a, x16c, third, force_scaled, xt, y0, aFx, aFy, aFz, apx);
+                            atmb_visit<NR, false>(X, k1, ya1, d31, act1, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq,
+                                                  ne, a, x16c, third, force_scaled, xt, y1, aFx, aFy, aFz, apx);
+                        }
                     }
                     const int src = (lane + 2) & 31;
                     y0.shift(src);
@@ -440,8 +456,8 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
                 // B[(lane + s1 + 1) mod 32]
                 y0.flush(acc, B * 32 + ((lane + s1) & 31), m);
                 y1.flush(acc, B * 32 + ((lane + s1 + 1) & 31), m);
-                const float tSE = xt.SE, tSD = xt.SD, tSF = xt.SF, tWx = xt.Wx, tWy = xt.Wy, tWz = xt.Wz, tSA = xt.SA,
-                            tUx = xt.Ux, tUy = xt.Uy, tUz = xt.Uz;
+                const float tSE = xt.SE, tSD = xt.SD, tSF = xt.SF, tWx = xt.Wx, tWy = xt.Wy, tWz = xt.Wz, tSA = xt.SA;
+                const float tUx = simple ? xt.Wx : xt.Ux, tUy = simple ? xt.Wy : xt.Uy, tUz = simple ? xt.Wz : xt.Uz;
                 xs[0] += tSE;
                 xs[1] += tSD;
                 xs[2] += tSF;

@@ -58,6 +58,7 @@ struct SG {
     int half[3];              // image box half-widths
     int atom_base, natoms;    // atom range in caller order
     int st2_off, st2_n, stc_off, stc_n, sta_off, sta_n; // stencil rows (two-body, CN, ATM)
+    int atm_simple;           // every cell height > 2 rc_ATM: no atom twice in an ATM list
 };
 
 struct KP {
@@ -1408,6 +1409,9 @@ static void build_structures(Engine *e, int nstruct, const uint64_t *counts, con
             r.inv[i] = g.inv[i];
         }
         r.vol = g.volume;
+        // a nonzero lattice vector is at least as long as the smallest height, so with every
+        // height above 2 rc_ATM two images of one atom never lie within rc_ATM of an apex
+        r.atm_simple = std::min(g.height[0], std::min(g.height[1], g.height[2])) > 2.0 * e->rc_atm * (1.0 + 1e-9);
         int64_t mcb[3];
         r.box_mode = reference_box(cells_f + 9 * k, e->rc_f, e->rc_cn_f, mcb) ? 1 : 0;
         for (int i = 0; i < 3; ++i) r.half[i] = (int)(mcb[i] / 2);
