@@ -181,6 +181,41 @@ __device__ __forceinline__ void traverse(const KP &p, const SG &g, int bin_globa
     }
 }
 
+// FP32 variant for the precision-form pair kernels: instead of the image shift it hands f
+// the origin o = x_i - shift (float, rounded once per contiguous range of candidates), so
+// that dx = o.x - x_j.x needs no per-candidate conversion.
+template <class F, class R = NoRowEnd>
+__device__ __forceinline__ void traverse32(const KP &p, const SG &g, int bin_global, const int4 *rows, int nrows,
+                                           const float4 xi, F &&f, R &&row_end = R()) {
+    const int lane = threadIdx.x & 31;
+    const int nb0 = g.nb[0], nb1 = g.nb[1], nb2 = g.nb[2];
+    const int bin = bin_global - g.bin_base;
+    const int *bstart = p.bin_start + g.bin_base;
+    const int bx = bin % nb0, by = (bin / nb0) % nb1, bz = bin / (nb0 * nb1);
+    for (int r = 0; r < nrows; ++r) {
+        const int4 row = rows[r];
+        const int yy = by + row.x, zz = bz + row.y;
+        const int Ty = floordiv(yy, nb1), Tz = floordiv(zz, nb2);
+        const int byy = yy - Ty * nb1, bzz = zz - Tz * nb2;
+        const int xlo = bx + row.z, xhi = bx + row.w;
+        const int plo = floordiv(xlo, nb0), phi = floordiv(xhi, nb0);
+        const int rowbase = nb0 * (byy + nb1 * bzz);
+        for (int px = plo; px <= phi; ++px) {
+            const int a = max(xlo, px * nb0) - px * nb0;
+            const int b = min(xhi, px * nb0 + nb0 - 1) - px * nb0;
+            const int jlo = bstart[rowbase + a], jhi = bstart[rowbase + b + 1];
+            const float3 o = make_float3(xi.x - (float)(px * g.h[0] + Ty * g.h[3] + Tz * g.h[6]),
+                                         xi.y - (float)(px * g.h[1] + Ty * g.h[4] + Tz * g.h[7]),
+                                         xi.z - (float)(px * g.h[2] + Ty * g.h[5] + Tz * g.h[8]));
+            for (int base = jlo; base < jhi; base += 32) {
+                const int j = base + lane;
+                f(j, px, Ty, Tz, o, j < jhi);
+            }
+        }
+        row_end();
+    }
+}
+
 __device__ __forceinline__ bool in_box(const SG &g, int4 si, int4 sj, int Tx, int Ty, int Tz) {
     if (!g.box_mode) return true;
     // reference lattice shift of this image in unwrapped coordinates
@@ -603,14 +638,14 @@ __global__ void k_cn32(KP p) {
     double acc = 0.0;
     float part = 0.0f;
     unsigned int npair = 0;
-    traverse(
-        p, g, p.bin_s[i], p.stencils + g.stc_off, g.stc_n,
-        [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+    traverse32(
+        p, g, p.bin_s[i], p.stencils + g.stc_off, g.stc_n, xi,
+        [&](int j, int Tx, int Ty, int Tz, const float3 &o, bool act) {
             if (!act) return;
             if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
             const float4 xj = p.xs32[j];
-            const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
-                        dz = (xi.z - (float)sh.z) - xj.z;
+            const float dx = o.x - xj.x, dy = o.y - xj.y,
+                        dz = o.z - xj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (d2 <= rcn2 && d2 > 0.0f) {
                 float dd;
@@ -632,6 +667,14 @@ __global__ void k_cn32(KP p) {
 
 template <int NR>
 __global__ void k_twobody32(KP p) {
+    // per type pair, FP32: BJ A^6, A^8 (zero damping: R0) and 3 sqrt(Q_i Q_j)^2 ratio
+    extern __shared__ float4 pair_tab[]; // [ne][ne]
+    for (int k = threadIdx.x; k < p.ne * p.ne; k += blockDim.x) {
+        const double *pa = p.pairA + (size_t)k * 4;
+        pair_tab[k] = make_float4((float)pa[0], (float)pa[1],
+                                  3.0f * (float)p.r2r4[k / p.ne] * (float)p.r2r4[k % p.ne], 0.0f);
+    }
+    __syncthreads();
     const int i = shard_atom(p, (blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (i >= p.n) return;
     const SG &g = p.sg[p.sid[i]];
@@ -644,19 +687,18 @@ __global__ void k_twobody32(KP p) {
         wi[a] = p.w32[(size_t)i * NR + a];
         dwi[a] = p.dw32[(size_t)i * NR + a];
     }
-    const float rri = (float)p.r2r4[ti];
     const float rc2 = (float)p.rc2, s6 = (float)p.s6, s8 = (float)p.s8, p1 = (float)p.p1, p2 = (float)p.p2;
     double E = 0, G = 0, FX = 0, FY = 0, FZ = 0, VXX = 0, VYY = 0, VZZ = 0, VXY = 0, VXZ = 0, VYZ = 0;
     float e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
     unsigned int npair = 0;
-    traverse(
-        p, g, p.bin_s[i], p.stencils + g.st2_off, g.st2_n,
-        [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+    traverse32(
+        p, g, p.bin_s[i], p.stencils + g.st2_off, g.st2_n, xi,
+        [&](int j, int Tx, int Ty, int Tz, const float3 &o, bool act) {
             if (!act) return;
             if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
             const float4 xj = p.xs32[j];
-            const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
-                        dz = (xi.z - (float)sh.z) - xj.z;
+            const float dx = o.x - xj.x, dy = o.y - xj.y,
+                        dz = o.z - xj.z;
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (!(r2 < rc2 && r2 > 0.0f)) return;
             ++npair;
@@ -669,13 +711,13 @@ __global__ void k_twobody32(KP p) {
                 c6 = fmaf(y, wi[b], c6);
                 dc6 = fmaf(y, dwi[b], dc6);
             }
-            const float rr = 3.0f * rri * (float)p.r2r4[tj];
+            const float4 tp = pair_tab[ti * p.ne + tj];
+            const float rr = tp.z;
             const float c8 = c6 * rr, dc8 = dc6 * rr;
-            const double *pa = p.pairA + ((size_t)ti * p.ne + tj) * 4;
             float E6, E8, Gt, fs;
             if (p.damping == 1) {
                 const float r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
-                const float i6 = __fdividef(1.0f, r6 + (float)pa[0]), i8 = __fdividef(1.0f, r8 + (float)pa[1]);
+                const float i6 = __fdividef(1.0f, r6 + tp.x), i8 = __fdividef(1.0f, r8 + tp.y);
                 E6 = s6 * c6 * i6;
                 E8 = s8 * c8 * i8;
                 Gt = s6 * dc6 * i6 + s8 * dc8 * i8;
@@ -683,7 +725,7 @@ __global__ void k_twobody32(KP p) {
             } else {
                 const float ir = rsqrtf(r2), ir2 = ir * ir;
                 const float ir6 = ir2 * ir2 * ir2, ir8 = ir6 * ir2;
-                const float R0 = (float)pa[0];
+                const float R0 = tp.x;
                 const float x6 = p1 * R0 * ir, x8 = p2 * R0 * ir;
                 const float x6_2 = x6 * x6, x6_4 = x6_2 * x6_2, x6_8 = x6_4 * x6_4, x6_14 = x6_8 * x6_4 * x6_2;
                 const float x8_2 = x8 * x8, x8_4 = x8_2 * x8_2, x8_8 = x8_4 * x8_4, x8_16 = x8_8 * x8_8;
@@ -761,14 +803,14 @@ __global__ void k_chain32(KP p, const double *Gd) {
     const float rcn2 = (float)p.rcn2;
     double FX = 0, FY = 0, FZ = 0, VXX = 0, VYY = 0, VZZ = 0, VXY = 0, VXZ = 0, VYZ = 0;
     float fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
-    traverse(
-        p, g, p.bin_s[i], p.stencils + g.stc_off, g.stc_n,
-        [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
+    traverse32(
+        p, g, p.bin_s[i], p.stencils + g.stc_off, g.stc_n, xi,
+        [&](int j, int Tx, int Ty, int Tz, const float3 &o, bool act) {
             if (!act) return;
             if (!in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
             const float4 xj = p.xs32[j];
-            const float dx = (xi.x - (float)sh.x) - xj.x, dy = (xi.y - (float)sh.y) - xj.y,
-                        dz = (xi.z - (float)sh.z) - xj.z;
+            const float dx = o.x - xj.x, dy = o.y - xj.y,
+                        dz = o.z - xj.z;
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (!(d2 <= rcn2 && d2 > 0.0f)) return;
             float dcn;
@@ -1726,7 +1768,7 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
             D3_CUDA(cudaMemsetAsync(p.v2, 0, sizeof(double) * 6 * n, s));
         }
         if (p.precision)
-            k_twobody32<NR><<<gw, T, 0, s>>>(p);
+            k_twobody32<NR><<<gw, T, (size_t)p.ne * p.ne * sizeof(float4), s>>>(p);
         else
             k_twobody<NR><<<gw, T, 0, s>>>(p);
         D3_CUDA(cudaEventRecord(ev[3], s));

@@ -13,7 +13,8 @@
 //     dE/dCN_i:               sum_j (b_ij + b_ji) dC6_ij/dCN_i
 //     virial:                 -(x_i - x_j) (x) (x_i - x_j) (a_ij + a_ji) / (2 V r) per ordered pair
 // Forward: one warp per atom, one lane per radial function; backward: one lane per
-// neighbour. Neighbours come from the rc_ATM stencil.
+// neighbour. Neighbours come from the rc_ATM stencil. The cutoff function is evaluated in
+// FP32 (sincospif) in both passes.
 
 constexpr int SURR_NRBF = 32;
 constexpr int SURR_MAXCH = 8;
@@ -28,17 +29,24 @@ struct SurrDesc {
     int *center;       // [n] channel of each atom (binned order), -1: not a channel
 };
 
+// smooth cutoff fc(r) = (1 + cos(pi r / rc)) / 2 and its derivative, FP32 (the same
+// values in the forward and the backward pass)
+__device__ __forceinline__ void surr_cutoff(float r, float inv_rc, float &fc, float &dfc) {
+    float sn, cs;
+    sincospif(r * inv_rc, &sn, &cs);
+    fc = 0.5f * (1.0f + cs);
+    dfc = -0.5f * 3.14159265358979f * inv_rc * sn;
+}
+
+// Forward: lane k of the atom's warp owns radial function k of every channel, in
+// registers. Each stencil chunk's in-range neighbours are broadcast channel by channel
+// (one ballot per channel), so each channel's sum is a register of a compile-time index.
 template <int NR>
 __global__ void k_desc_fwd(KP p, SurrDesc sd) {
-    __shared__ float Gs[8][SURR_MAXCH][SURR_NRBF];
-    const int warp_in_block = threadIdx.x >> 5;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= p.n) return;
     const SG &g = p.sg[p.sid[i]];
-    float(*Gw)[SURR_NRBF] = Gs[warp_in_block];
-    for (int c = 0; c < SURR_MAXCH; ++c) Gw[c][lane] = 0.0f;
-    __syncwarp();
     const double4 xi = p.xs[i];
     const int4 si = p.shift[i];
     const int ti = (int)xi.w;
@@ -47,43 +55,50 @@ __global__ void k_desc_fwd(KP p, SurrDesc sd) {
 #pragma unroll
     for (int a = 0; a < NR; ++a) wi[a] = p.w[(size_t)i * NR + a];
     const float mu_k = sd.mu0 + sd.dmu * lane;
-    const double rc = sqrt(p.ratm2);
-    const double pirc = 3.14159265358979323846 / rc;
+    const float inv_rc = (float)(1.0 / sqrt(p.ratm2));
+    const int nch = sd.nch;
+    float acc[SURR_MAXCH];
+#pragma unroll
+    for (int c = 0; c < SURR_MAXCH; ++c) acc[c] = 0.0f;
     traverse(p, g, p.bin_s[i], p.stencils + g.sta_off, g.sta_n,
              [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
-                 float r = 0.f, c6fc = 0.f;
+                 float r = 0.f, wgt = 0.f;
                  int ch = -1;
-                 bool keep = false;
                  if (act && in_box(g, si, p.shift[j], Tx, Ty, Tz)) {
                      const double4 xj = p.xs[j];
                      const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
                      const double d2 = dx * dx + dy * dy + dz * dz;
-                     ch = sd.chan[(int)xj.w];
-                     if (d2 <= p.ratm2 && d2 > 0.0 && ch >= 0) {
-                         const double rr = sqrt(d2);
+                     const int cj = sd.chan[(int)xj.w];
+                     if (d2 <= p.ratm2 && d2 > 0.0 && cj >= 0) {
                          const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
                          double c6 = 0.0;
 #pragma unroll
                          for (int b = 0; b < NR; ++b) c6 += yj[b] * wi[b];
-                         r = (float)rr;
-                         c6fc = (float)(c6 * 0.5 * (1.0 + cos(pirc * rr)));
-                         keep = true;
+                         r = (float)sqrt(d2);
+                         float fc, dfc;
+                         surr_cutoff(r, inv_rc, fc, dfc);
+                         wgt = (float)c6 * fc;
+                         ch = cj;
                      }
                  }
-                 unsigned m = __ballot_sync(0xffffffffu, keep);
-                 while (m) {
-                     const int b = __ffs(m) - 1;
-                     m &= m - 1u;
-                     const float rb = __shfl_sync(0xffffffffu, r, b);
-                     const float cb = __shfl_sync(0xffffffffu, c6fc, b);
-                     const int chb = __shfl_sync(0xffffffffu, ch, b);
-                     const float d = rb - mu_k;
-                     Gw[chb][lane] += cb * __expf(-d * d * sd.inv2s2);
+#pragma unroll
+                 for (int c = 0; c < SURR_MAXCH; ++c) {
+                     if (c >= nch) break;
+                     unsigned m = __ballot_sync(0xffffffffu, ch == c);
+                     while (m) {
+                         const int b = __ffs(m) - 1;
+                         m &= m - 1u;
+                         const float rb = __shfl_sync(0xffffffffu, r, b);
+                         const float wb = __shfl_sync(0xffffffffu, wgt, b);
+                         const float d = rb - mu_k;
+                         acc[c] = fmaf(wb, __expf(-d * d * sd.inv2s2), acc[c]);
+                     }
                  }
              });
-    __syncwarp();
-    float *out = sd.G + (size_t)i * sd.nch * SURR_NRBF;
-    for (int c = 0; c < sd.nch; ++c) out[c * SURR_NRBF + lane] = Gw[c][lane];
+    float *out = sd.G + (size_t)i * nch * SURR_NRBF;
+#pragma unroll
+    for (int c = 0; c < SURR_MAXCH; ++c)
+        if (c < nch) out[c * SURR_NRBF + lane] = acc[c];
 }
 
 // Backward, one warp per atom and one neighbour per lane. With phi_k = exp(-(r - mu_k)^2
@@ -93,16 +108,25 @@ __global__ void k_desc_fwd(KP p, SurrDesc sd) {
 // so each neighbour costs 32 exponentials and two FMAs per radial function; the atom's own
 // dE/dG rows sit in shared memory (rows padded to 33 floats: lanes reading different
 // channels at the same k hit different banks), the neighbour's row is read as 8 float4.
+// In-range neighbours are first compacted into a per-warp queue, so that the radial loop
+// always runs with 32 busy lanes.
+struct SurrNb {
+    int j, ch;
+    float r, c6, dc6, dx, dy, dz;
+};
+
 template <int NR>
 __global__ void __launch_bounds__(256, 2) k_desc_bwd(KP p, SurrDesc sd) {
     constexpr int PITCH = SURR_NRBF + 1;
     __shared__ float Ds[8][SURR_MAXCH * PITCH];
+    __shared__ SurrNb Q[8][64];
     const int warp_in_block = threadIdx.x >> 5;
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (i >= p.n) return;
     const SG &g = p.sg[p.sid[i]];
     float *Dw = Ds[warp_in_block];
+    SurrNb *q = Q[warp_in_block];
     const float *din = sd.dEdG + (size_t)i * sd.nch * SURR_NRBF;
     for (int c = 0; c < sd.nch; ++c) Dw[c * PITCH + lane] = din[c * SURR_NRBF + lane];
     __syncwarp();
@@ -116,57 +140,81 @@ __global__ void __launch_bounds__(256, 2) k_desc_bwd(KP p, SurrDesc sd) {
         wi[a] = p.w[(size_t)i * NR + a];
         dwi[a] = p.dw[(size_t)i * NR + a];
     }
-    const double rc = sqrt(p.ratm2);
-    const double pirc = 3.14159265358979323846 / rc;
+    const float inv_rc = (float)(1.0 / sqrt(p.ratm2));
     const float a2 = sd.inv2s2;
     double fx = 0, fy = 0, fz = 0, gcn = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+    // one queued neighbour per lane: the radial sums and their contributions
+    auto process = [&](bool valid) {
+        if (!valid) return;
+        const SurrNb nb = q[lane];
+        float fc, dfc;
+        surr_cutoff(nb.r, inv_rc, fc, dfc);
+        const float4 *gj = reinterpret_cast<const float4 *>(sd.dEdG + ((size_t)nb.j * sd.nch + chi) * SURR_NRBF);
+        const float *gi = Dw + nb.ch * PITCH;
+        float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+        for (int qd = 0; qd < SURR_NRBF / 4; ++qd) {
+            const float4 v = __ldg(gj + qd);
+            const float gv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const int k = 4 * qd + t;
+                const float u = nb.r - (sd.mu0 + sd.dmu * k);
+                const float w = (gv[t] + gi[k]) * __expf(-u * u * a2);
+                s0 += w;
+                s1 = fmaf(w, u, s1);
+            }
+        }
+        // dE/dr / r and dE/dC6_ij
+        const double fs = (double)nb.c6 * ((double)dfc * s0 - 2.0 * (double)a2 * (double)fc * s1) / (double)nb.r;
+        const double dx = nb.dx, dy = nb.dy, dz = nb.dz;
+        fx += fs * dx;
+        fy += fs * dy;
+        fz += fs * dz;
+        vxx += fs * dx * dx;
+        vyy += fs * dy * dy;
+        vzz += fs * dz * dz;
+        vxy += fs * dx * dy;
+        vxz += fs * dx * dz;
+        vyz += fs * dy * dz;
+        gcn += (double)(fc * s0) * (double)nb.dc6; // dE/dC6_ij dC6_ij/dCN_i
+    };
+    int count = 0; // queued neighbours (warp-uniform)
     traverse(p, g, p.bin_s[i], p.stencils + g.sta_off, g.sta_n,
              [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
-                 if (!act || chi < 0 || !in_box(g, si, p.shift[j], Tx, Ty, Tz)) return;
-                 const double4 xj = p.xs[j];
-                 const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
-                 const double d2 = dx * dx + dy * dy + dz * dz;
-                 const int ch = sd.chan[(int)xj.w];
-                 if (!(d2 <= p.ratm2 && d2 > 0.0) || ch < 0) return;
-                 const double rr = sqrt(d2);
-                 const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
-                 double c6 = 0.0, dc6 = 0.0;
+                 bool keep = false;
+                 SurrNb nb;
+                 if (act && chi >= 0 && in_box(g, si, p.shift[j], Tx, Ty, Tz)) {
+                     const double4 xj = p.xs[j];
+                     const double dx = xi.x - (xj.x + sh.x), dy = xi.y - (xj.y + sh.y), dz = xi.z - (xj.z + sh.z);
+                     const double d2 = dx * dx + dy * dy + dz * dz;
+                     const int ch = sd.chan[(int)xj.w];
+                     if (d2 <= p.ratm2 && d2 > 0.0 && ch >= 0) {
+                         const double *yj = p.Y + ((size_t)j * p.ne + ti) * NR;
+                         double c6 = 0.0, dc6 = 0.0;
 #pragma unroll
-                 for (int b = 0; b < NR; ++b) {
-                     c6 += yj[b] * wi[b];
-                     dc6 += yj[b] * dwi[b]; // dC6_ij/dCN_i
-                 }
-                 const double fc = 0.5 * (1.0 + cos(pirc * rr));
-                 const double dfc = -0.5 * pirc * sin(pirc * rr);
-                 const float r = (float)rr;
-                 const float4 *gj = reinterpret_cast<const float4 *>(sd.dEdG + ((size_t)j * sd.nch + chi) * SURR_NRBF);
-                 const float *gi = Dw + ch * PITCH;
-                 float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-                 for (int q = 0; q < SURR_NRBF / 4; ++q) {
-                     const float4 v = __ldg(gj + q);
-                     const float gv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                     for (int t = 0; t < 4; ++t) {
-                         const int k = 4 * q + t;
-                         const float u = r - (sd.mu0 + sd.dmu * k);
-                         const float w = (gv[t] + gi[k]) * __expf(-u * u * a2);
-                         s0 += w;
-                         s1 = fmaf(w, u, s1);
+                         for (int b = 0; b < NR; ++b) {
+                             c6 += yj[b] * wi[b];
+                             dc6 += yj[b] * dwi[b]; // dC6_ij/dCN_i
+                         }
+                         nb = SurrNb{j, ch, (float)sqrt(d2), (float)c6, (float)dc6, (float)dx, (float)dy, (float)dz};
+                         keep = true;
                      }
                  }
-                 const double fs = c6 * (dfc * (double)s0 - 2.0 * (double)a2 * fc * (double)s1) / rr; // dE/dr / r
-                 fx += fs * dx;
-                 fy += fs * dy;
-                 fz += fs * dz;
-                 vxx += fs * dx * dx;
-                 vyy += fs * dy * dy;
-                 vzz += fs * dz * dz;
-                 vxy += fs * dx * dy;
-                 vxz += fs * dx * dz;
-                 vyz += fs * dy * dz;
-                 gcn += fc * (double)s0 * dc6; // dE/dC6_ij dC6_ij/dCN_i
+                 const unsigned m = __ballot_sync(0xffffffffu, keep);
+                 if (keep) q[count + __popc(m & ((1u << lane) - 1u))] = nb;
+                 count += __popc(m);
+                 if (count >= 32) {
+                     __syncwarp();
+                     process(true);
+                     __syncwarp();
+                     if (lane < count - 32) q[lane] = q[32 + lane];
+                     count -= 32;
+                     __syncwarp();
+                 }
              });
+    __syncwarp();
+    process(lane < count);
     fx = warp_sum(fx);
     fy = warp_sum(fy);
     fz = warp_sum(fz);
