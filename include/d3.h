@@ -154,6 +154,11 @@ int d3_set_positions_device(d3_handle_t *handle, const double *coords_dev, void 
    d3_compute_f64 or compute_dispersion_energy_from_handle_status first). */
 uint16_t d3_compute_async(d3_handle_t *handle, void *cuda_stream);
 const double *d3_device_results(d3_handle_t *handle);
+/* Stream-ordered device-to-device copy of the results of the last enqueued evaluation
+   (energies [S], forces [n][3], stresses [S][9], double) to a caller buffer; it can be
+   captured in a CUDA graph together with d3_compute_async (MD loops). */
+int d3_copy_results_device(d3_handle_t *handle, double *results_dev, void *cuda_stream);
+
 /* Copy the device results of the last evaluation to host arrays (energies [S], forces
    [n][3], stresses [S][9]; any may be NULL). Synchronise the evaluation's stream first. */
 int d3_fetch_results(d3_handle_t *handle, double *energies, double *forces, double *stresses);

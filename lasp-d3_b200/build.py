@@ -39,6 +39,9 @@ def _stale():
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in CU_SOURCES + CXX_SOURCES + HEADERS]
     deps.append(os.path.join(HERE, "..", "include", "d3.h"))
+    deps.append(os.path.join(HERE, "cli", "d3_cli.cpp"))
+    if not os.path.exists(os.path.join(OUT_DIR, "d3_cli")):
+        return True
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
@@ -68,6 +71,11 @@ def build(verbose=False, ptxas=False, force=False):
     tmp = LIB + ".tmp"
     _run([NVCC, "-shared"] + ARCH + objs + ["-o", tmp, "-lcudart"], verbose)
     os.replace(tmp, LIB)
+    # command-line front end on the library (drop-in for the reference's d3_cpp)
+    cli = os.path.join(OUT_DIR, "d3_cli")
+    _run(["g++", "-std=c++17", "-O2", "-I", os.path.join(HERE, "..", "include"), os.path.join(HERE, "cli", "d3_cli.cpp"),
+          "-L", OUT_DIR, "-ld3", "-Wl,-rpath,$ORIGIN", "-o", cli + ".tmp"], verbose)
+    os.replace(cli + ".tmp", cli)
     if ptxas:
         print(log)
     return LIB

@@ -606,4 +606,20 @@ uint16_t d3_shard_end(d3_handle_t *handle, const double *dedcn_dev, double *resu
     return st;
 }
 
+int d3_copy_results_device(d3_handle_t *handle, double *results_dev, void *cuda_stream) {
+    if (!handle || !results_dev) {
+        set_error("NULL argument in d3_copy_results_device");
+        return 1;
+    }
+    const double *src = d3::engine_device_results(H(handle)->engine);
+    const size_t S = (size_t)d3::engine_num_structures(H(handle)->engine), n = d3::engine_num_atoms(H(handle)->engine);
+    const cudaError_t e = cudaMemcpyAsync(results_dev, src, sizeof(double) * (10 * S + 3 * n), cudaMemcpyDeviceToDevice,
+                                          (cudaStream_t)cuda_stream);
+    if (e != cudaSuccess) {
+        set_error(std::string("d3_copy_results_device: ") + cudaGetErrorString(e));
+        return 1;
+    }
+    return 0;
+}
+
 } // extern "C"

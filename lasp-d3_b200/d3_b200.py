@@ -121,6 +121,8 @@ def load_library(path=None):
     lib.d3_mlp_forward.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, ci, vp, vp, vp]
     lib.d3_mlp_train_batch.restype = ci
     lib.d3_mlp_train_batch.argtypes = [ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, ci, vp, vp, vp, vp, vp]
+    lib.d3_copy_results_device.restype = ci
+    lib.d3_copy_results_device.argtypes = [vp, vp, vp]
     lib.d3_shard_length.restype = u64
     lib.d3_shard_length.argtypes = [vp]
     lib.d3_shard_begin.restype = ctypes.c_uint16
@@ -289,6 +291,12 @@ class D3(_Surrogate, _Shard):
 
     def device_results_ptr(self):
         return self.lib.d3_device_results(self.h)
+
+    def copy_results_device(self, dst_ptr, stream_ptr=None):
+        """Stream-ordered copy of the device results [1 + 3n + 9] (double) to dst_ptr."""
+        if self.lib.d3_copy_results_device(self.h, ctypes.c_void_p(dst_ptr),
+                                           ctypes.c_void_p(stream_ptr) if stream_ptr else None):
+            raise RuntimeError(self.lib.d3_last_error().decode())
 
     def atom_arrays(self):
         cn, g, e = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
