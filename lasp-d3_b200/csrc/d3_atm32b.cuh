@@ -33,22 +33,37 @@
 constexpr int ATMB_MCAP = 4096;   // longest list this kernel takes (longer lists: k_atm32)
 constexpr int ATMB_GRID = 8;      // spatial grid per dimension for the entry sort
 constexpr int ATMB_MAXW = 8;      // warps per CTA at most
+constexpr int ATMB_VPI = 4;       // visits per lane per iteration (independent, for ILP)
+
+// global scratch per CTA (float4 units): per-entry records sA, sB, sJ and the per-entry
+// accumulators [6][MCAP] floats
+constexpr size_t ATMB_SCRATCH_PER_CTA = 3 * ATMB_MCAP + (6 * ATMB_MCAP + 3) / 4;
 
 // shared memory: fixed part + per-warp staging
 __host__ __device__ inline size_t atmb_smem_fixed(int ne, int NR) {
-    size_t b = 6 * ATMB_MCAP * sizeof(float);                 // per-entry accumulators
+    size_t b = ATMB_MCAP * sizeof(int);                       // atom of each sorted entry
     b += 2 * (ATMB_MCAP / 32) * sizeof(float4);               // block bounding boxes
     b += 512 * sizeof(int);                                   // sort cells
     b += (size_t)((ne * ne + 3) & ~3) * sizeof(float);        // r0^2
     b += (size_t)((ne * NR + 1) & ~1) * sizeof(double);       // apex C6 rows
     return (b + 15) & ~(size_t)15;
 }
-// per warp: the x entries' C6 rows and derivative rows, float2 [type][8][lane] (lanes read
-// consecutive 8-byte words whatever the partner type, so the reads are free of bank
-// conflicts), and the staged y block as seven float4 arrays [lane]
-__host__ __device__ inline size_t atmb_smem_warp(int ne) {
-    return 32 * ((size_t)ne * 8 * sizeof(float2) + 7 * sizeof(float4));
+// per warp: two buffers (the block pair being visited and the next one, filled by
+// cp.async meanwhile), each the staged y block: the rows of its entries for every partner
+// type as float4 [type][row quad][lane] (lanes read consecutive 16-byte words whatever the
+// x type, so the reads are free of bank conflicts) and positions / per-entry constants
+__host__ __device__ inline size_t atmb_buf_quads(int ne, int NR) { return 32 * ((size_t)ne * (atmb_row_floats(NR) / 4) + 2); }
+__host__ __device__ inline size_t atmb_smem_warp(int ne, int NR) { return 2 * atmb_buf_quads(ne, NR) * sizeof(float4); }
+
+// 16-byte global -> shared copy that bypasses registers (cached in L2 only)
+__device__ __forceinline__ void atmb_cp16(void *dst, const void *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
+__device__ __forceinline__ void atmb_cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's groups are still in flight
+template <int N>
+__device__ __forceinline__ void atmb_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ int atmb_morton(int x, int y, int z) {
     int k = 0;
@@ -57,45 +72,108 @@ __device__ __forceinline__ int atmb_morton(int x, int y, int z) {
     return k;
 }
 
-// sum_b r[b] v[b] over the NR references: r as four float2 (8 floats), v as two float4
+// one row of the table (atmb_row_floats(NR) floats as float4 quads): C6 row Y, r0^2 of the
+// type pair, derivative row D, atom index bits
 template <int NR>
-__device__ __forceinline__ float atmb_dot(const float2 r0, const float2 r1, const float2 r2, const float2 r3,
-                                          const float4 v0, const float4 v1) {
-    float s = r0.x * v0.x;
-    s = fmaf(r0.y, v0.y, s);
-    s = fmaf(r1.x, v0.z, s);
-    s = fmaf(r1.y, v0.w, s);
-    s = fmaf(r2.x, v1.x, s);
-    if (NR > 5) {
-        s = fmaf(r2.y, v1.y, s);
-        s = fmaf(r3.x, v1.z, s);
+struct AtmbRow {
+    float Y[NR], D[NR], r0sq;
+    int j;
+    __device__ __forceinline__ void load(const float4 *r, int k) {
+        const float4 q0 = r[k], q1 = r[32 + k], q2 = r[64 + k];
+        Y[0] = q0.x;
+        Y[1] = q0.y;
+        Y[2] = q0.z;
+        Y[3] = q0.w;
+        Y[4] = q1.x;
+        if constexpr (NR == 5) {
+            r0sq = q1.y;
+            D[0] = q1.z;
+            D[1] = q1.w;
+            D[2] = q2.x;
+            D[3] = q2.y;
+            D[4] = q2.z;
+            j = __float_as_int(q2.w);
+        } else {
+            const float4 q3 = r[96 + k];
+            Y[5] = q1.y;
+            Y[6] = q1.z;
+            r0sq = q1.w;
+            D[0] = q2.x;
+            D[1] = q2.y;
+            D[2] = q2.z;
+            D[3] = q2.w;
+            D[4] = q3.x;
+            D[5] = q3.y;
+            D[6] = q3.z;
+            j = __float_as_int(q3.w);
+        }
     }
+};
+
+// padding partner rows: unit C6 row and r0^2, zero derivative row, atom bits -1
+template <int NR>
+struct AtmbRowFill {
+    __device__ __forceinline__ static void padding(float4 *r) {
+        if constexpr (NR == 5) {
+            r[0] = make_float4(1.f, 1.f, 1.f, 1.f);
+            r[32] = make_float4(1.f, 1.f, 0.f, 0.f);
+            r[64] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        } else {
+            r[0] = make_float4(1.f, 1.f, 1.f, 1.f);
+            r[32] = make_float4(1.f, 1.f, 1.f, 1.f);
+            r[64] = make_float4(0.f, 0.f, 0.f, 0.f);
+            r[96] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+        }
+    }
+};
+
+template <int NR>
+__device__ __forceinline__ float atmb_dot(const float *r, const float *v) {
+    float s = r[0] * v[0];
+#pragma unroll
+    for (int b = 1; b < NR; ++b) s = fmaf(r[b], v[b], s);
     return s;
 }
 
+// per-row constants of the x entry; gq carries the factor (4/3)^16, c1 = -0.75 d1,
+// d1x3 = 3 d1; w, dw its own C6 weights and their CN derivatives
+template <int NR>
 struct AtmbX {
-    float vx, vy, vz, d1, ir1, id1, sq, gq;
-    int jx, tx;
-    bool qa, valid;
+    float vx, vy, vz, d1, ir1, id1, sq, gq, c1, d1x3;
+    float w[NR], dw[NR];
+    int jx;
+    bool qa;
 };
 
-// per-side sums of one block pair: SE = sum w E, SD = sum w E lam, SF = sum wf (f_e + f3),
-// W = sum wf f3 v_other; the x side also SA = sum wf f1 and U = sum w f3 v_y
+// per-side sums of one block pair: SE = sum w E, SD = sum w E lam, SA = sum wf f_apex-side,
+// S3 = sum wf f3, W = sum wf f3 v_other; the x side also U = sum w f3 v_y
+// (force scalar of the entry SF = SA + S3)
 struct AtmbSide {
-    float SE, SD, SF, Wx, Wy, Wz, SA, Ux, Uy, Uz;
+    float SE, SD, SA, S3, Wx, Wy, Wz, Ux, Uy, Uz;
     __device__ __forceinline__ void shift(int src) {
         SE = __shfl_sync(0xffffffffu, SE, src);
         SD = __shfl_sync(0xffffffffu, SD, src);
-        SF = __shfl_sync(0xffffffffu, SF, src);
+        SA = __shfl_sync(0xffffffffu, SA, src);
+        S3 = __shfl_sync(0xffffffffu, S3, src);
         Wx = __shfl_sync(0xffffffffu, Wx, src);
         Wy = __shfl_sync(0xffffffffu, Wy, src);
         Wz = __shfl_sync(0xffffffffu, Wz, src);
     }
+    // add the y sums that lane src holds
+    __device__ __forceinline__ void add_from(const AtmbSide &o, int src) {
+        SE += __shfl_sync(0xffffffffu, o.SE, src);
+        SD += __shfl_sync(0xffffffffu, o.SD, src);
+        SA += __shfl_sync(0xffffffffu, o.SA, src);
+        S3 += __shfl_sync(0xffffffffu, o.S3, src);
+        Wx += __shfl_sync(0xffffffffu, o.Wx, src);
+        Wy += __shfl_sync(0xffffffffu, o.Wy, src);
+        Wz += __shfl_sync(0xffffffffu, o.Wz, src);
+    }
     __device__ __forceinline__ void flush(float *acc, int e, int m) {
-        if (e < m && (SE != 0.f || SF != 0.f || SD != 0.f)) {
+        if (e < m && (SE != 0.f || SA != 0.f || S3 != 0.f || SD != 0.f)) {
             atomicAdd(&acc[0 * ATMB_MCAP + e], SE);
             atomicAdd(&acc[1 * ATMB_MCAP + e], SD);
-            atomicAdd(&acc[2 * ATMB_MCAP + e], SF);
+            atomicAdd(&acc[2 * ATMB_MCAP + e], SA + S3);
             atomicAdd(&acc[3 * ATMB_MCAP + e], Wx);
             atomicAdd(&acc[4 * ATMB_MCAP + e], Wy);
             atomicAdd(&acc[5 * ATMB_MCAP + e], Wz);
@@ -103,35 +181,34 @@ struct AtmbSide {
     }
 };
 
-// One (possible) visit of entry x with staged partner k: range test, triplet term,
-// x-side sums into xt, y-side sums into ys, apex force of the a-y side, virial
-// corrections where the virial and force weights differ.
-// Branch-free: an out-of-range pair (act false) runs on safe stand-in values with zero
-// weights, so the two visits of an iteration can be interleaved by the compiler.
+// One (possible) visit of entry x with staged partner k: triplet term, x-side sums into
+// xt, y-side sums into ys, virial corrections where the virial and force weights differ.
+// Branch-free: an out-of-range pair (act false) runs on finite stand-in values (lanes
+// without entry and padding partners sit at far, distinct points with positive C6 rows)
+// with zero weights, so the visits of an iteration can be interleaved by the compiler.
+// With P = t1 t2 t3 (t1 = d1 + d2 - d3 ...), the angular term is
+// A = (1 + 3/8 P / (d1 d2 d3)) / (r1 r2 r3)^3 and its side derivatives
+// dA/dr_k / r_k = q52 G_k, G_k = 15/8 P + 3 d1 d2 d3 - 3/4 d_k (T - 2 t_ij),
+// T = t12 + t13 + t23 (t_ij the product of the two t's without t_k).
 template <int NR, bool SIMPLE>
-__device__ __forceinline__ void atmb_visit(const AtmbX &X, int k, const float4 ya, float d3in, bool act,
-                                           const float4 *yB, const int4 *yJ, const float4 *yW0, const float4 *yW1,
-                                           const float4 *yD0, const float4 *yD1, const float2 *xrow, int lane,
-                                           const float *r0sq, int ne, int a, float x16c, float third, bool force_scaled,
-                                           AtmbSide &xt, AtmbSide &ys, float &aFx, float &aFy, float &aFz,
-                                           double *apx) {
+__device__ __forceinline__ void atmb_visit(const AtmbX<NR> &X, int k, const float4 ya, float d3in, bool act,
+                                           const float4 *yB, const float4 *yrow, int a, float third,
+                                           bool force_scaled, AtmbSide &xt, AtmbSide &ys, double *apx) {
     const float d3 = act ? d3in : X.d1;
     const float4 yb = yB[k];
-    const int4 yj = yJ[k];
-    const int ty = yj.y;
+    AtmbRow<NR> R; // the y entry's rows at the x entry's type
+    R.load(yrow, k);
     const float ir3 = rsqrtf(d3);
     const float id3 = ir3 * ir3;
-    const float2 *xr = xrow + ty * 8 * 32 + lane;
-    const float2 Ya = xr[0], Yb = xr[32], Yc = xr[64], Yd = xr[96];
-    const float2 Da = xr[128], Db = xr[160], Dc = xr[192], Dd = xr[224];
-    const float4 W0 = yW0[k], W1 = yW1[k], V0 = yD0[k], V1 = yD1[k];
-    const float c6 = act ? atmb_dot<NR>(Ya, Yb, Yc, Yd, W0, W1) : 1.0f;
-    const float dcx = atmb_dot<NR>(Da, Db, Dc, Dd, W0, W1); // dC6_xy/dCN_x
-    const float dcy = atmb_dot<NR>(Ya, Yb, Yc, Yd, V0, V1); // dC6_xy/dCN_y
+    // C6_xy = Y_y[t_x] . w_x, its derivatives dw_x and through D_y[t_x] = dw_y C
+    const float c6 = atmb_dot<NR>(R.Y, X.w);
+    const float dcx = atmb_dot<NR>(R.Y, X.dw); // dC6_xy/dCN_x
+    const float dcy = atmb_dot<NR>(R.D, X.w);  // dC6_xy/dCN_y
     const float is3 = rsqrtf(c6);
     const float s3 = c6 * is3;
-    const float lam_xy = act ? dcx * is3 * is3 : 0.0f, lam_yx = act ? dcy * is3 * is3 : 0.0f;
-    const float u = r0sq[X.tx * ne + ty] * id3;
+    const float is3q = is3 * is3;
+    const float lam_xy = dcx * is3q, lam_yx = dcy * is3q;
+    const float u = R.r0sq * id3; // r0_xy^2 / d3
     const float g3 = exp2f(__log2f(u) * (8.0f / 3.0f)); // u^(8/3)
     // reference scale factors (src/d3_kernel.cu:1282-1290) as pair weights; SIMPLE: no
     // atom appears twice in the list (cell heights > 2 rc_ATM), every weight is 1
@@ -139,56 +216,57 @@ __device__ __forceinline__ void atmb_visit(const AtmbX &X, int k, const float4 y
     if (SIMPLE) {
         w = wf = act ? 1.0f : 0.0f;
     } else {
-        const bool same = (X.jx == yj.x);
-        const bool apex_img = X.qa | (yj.x == a);
+        const int jy = R.j;
+        const bool same = (X.jx == jy);
+        const bool apex_img = X.qa | (jy == a);
         w = act ? (same ? (X.qa ? third : 1.0f) : (apex_img ? 0.5f : 1.0f)) : 0.0f;
         wf = act ? (force_scaled ? w : (same ? 2.0f : 1.0f)) : 0.0f;
     }
-    const float d1 = X.d1, d2 = act ? ya.w : X.d1;
+    const float d1 = X.d1, d2 = ya.w;
     const float irsq = X.id1 * yb.y * id3;
     const float ir9 = irsq * X.ir1 * yb.x * ir3;
     const float t1 = d1 + d2 - d3, t2 = d1 - d2 + d3, t3 = -d1 + d2 + d3;
     const float t12 = t1 * t2, t13 = t1 * t3, t23 = t2 * t3;
     const float P = t12 * t3;
+    const float T = t12 + t13 + t23;
     const float Aang = fmaf(0.375f * P, irsq, 1.0f) * ir9;
     const float q52 = ir9 * irsq;
-    const float base = fmaf(1.875f, P, 3.0f * d1 * d2 * d3);
-    const float dang1 = q52 * fmaf(-0.75f * d1, t23 + t13 - t12, base);
-    const float dang2 = q52 * fmaf(-0.75f * d2, t23 - t13 + t12, base);
-    const float dang3 = q52 * fmaf(-0.75f * d3, t13 + t12 - t23, base);
-    const float x16 = act ? x16c * X.gq * yb.w * g3 : 0.0f;
+    const float base = fmaf(1.875f, P, X.d1x3 * d2 * d3);
+    const float G1 = fmaf(X.c1, fmaf(-2.0f, t12, T), base);
+    const float G2 = fmaf(-0.75f * d2, fmaf(-2.0f, t13, T), base);
+    const float G3 = fmaf(-0.75f * d3, fmaf(-2.0f, t23, T), base);
+    const float x16 = X.gq * yb.w * g3;
     const float fd = __fdividef(1.0f, fmaf(6.0f, x16, 1.0f));
     const float dfd = 32.0f * x16 * fd * fd;
-    const float C9 = -X.sq * yb.z * s3;
-    const float Et = C9 * Aang * fd;
-    const float Adfd = Aang * dfd;
-    const float f1 = -C9 * fmaf(dang1, fd, -Adfd) * X.id1;
-    const float f2 = -C9 * fmaf(dang2, fd, -Adfd) * yb.y;
-    const float f3 = -C9 * fmaf(dang3, fd, -Adfd) * id3;
+    const float nC9 = X.sq * yb.z * s3; // -C9
+    const float nC9fd = nC9 * fd;
+    const float Et = -nC9fd * Aang;
+    const float Ap = nC9fd * q52, Bp = nC9 * Aang * dfd;
+    const float f1 = fmaf(Ap, G1, -Bp) * X.id1;
+    const float f2 = fmaf(Ap, G2, -Bp) * yb.y;
+    const float f3 = fmaf(Ap, G3, -Bp) * id3;
     const float wE = w * Et;
-    const float wf3 = wf * f3, w3 = w * f3;
+    const float wf3 = wf * f3;
     xt.SE += wE;
     xt.SD = fmaf(wE, lam_xy, xt.SD);
-    xt.SF = fmaf(wf, f1 + f3, xt.SF);
+    xt.SA = fmaf(wf, f1, xt.SA);
+    xt.S3 += wf3;
     xt.Wx = fmaf(wf3, ya.x, xt.Wx);
     xt.Wy = fmaf(wf3, ya.y, xt.Wy);
     xt.Wz = fmaf(wf3, ya.z, xt.Wz);
-    xt.SA = fmaf(wf, f1, xt.SA);
     if (!SIMPLE) { // SIMPLE: U = W
+        const float w3 = w * f3;
         xt.Ux = fmaf(w3, ya.x, xt.Ux);
         xt.Uy = fmaf(w3, ya.y, xt.Uy);
         xt.Uz = fmaf(w3, ya.z, xt.Uz);
     }
     ys.SE += wE;
     ys.SD = fmaf(wE, lam_yx, ys.SD);
-    ys.SF = fmaf(wf, f2 + f3, ys.SF);
+    ys.SA = fmaf(wf, f2, ys.SA);
+    ys.S3 += wf3;
     ys.Wx = fmaf(wf3, X.vx, ys.Wx);
     ys.Wy = fmaf(wf3, X.vy, ys.Wy);
     ys.Wz = fmaf(wf3, X.vz, ys.Wz);
-    const float wf2 = wf * f2;
-    aFx = fmaf(wf2, ya.x, aFx);
-    aFy = fmaf(wf2, ya.y, aFy);
-    aFz = fmaf(wf2, ya.z, aFz);
     if (!SIMPLE && w != wf) {
         // virial weights w where the force weights differ (repeated indices)
         const double c1 = (double)(w - wf) * (double)(f1 + f3), c2 = (double)(w - wf) * (double)(f2 + f3);
@@ -207,28 +285,26 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
     const int ne = p.ne;
     const int nw = blockDim.x >> 5;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float *acc = reinterpret_cast<float *>(smb);                         // [6][MCAP]
-    float4 *bblo = reinterpret_cast<float4 *>(acc + 6 * ATMB_MCAP);      // [MCAP/32]
+    int *sjy = reinterpret_cast<int *>(smb);                             // [MCAP] atom of each sorted entry
+    float4 *bblo = reinterpret_cast<float4 *>(sjy + ATMB_MCAP);          // [MCAP/32]
     float4 *bbhi = bblo + ATMB_MCAP / 32;
     int *cellpos = reinterpret_cast<int *>(bbhi + ATMB_MCAP / 32);       // [512]
     float *r0sq = reinterpret_cast<float *>(cellpos + 512);              // [ne][ne]
     double *yapex = reinterpret_cast<double *>(r0sq + ((ne * ne + 3) & ~3)); // [ne][NR]
-    unsigned char *wbase = smb + atmb_smem_fixed(ne, NR) + (size_t)warp * atmb_smem_warp(ne);
-    float2 *xrow = reinterpret_cast<float2 *>(wbase);                    // [ne][8][32]: Y (4 pairs) D (4 pairs)
-    float4 *yA = reinterpret_cast<float4 *>(xrow + ne * 8 * 32);         // [32] vx vy vz d2
-    float4 *yB = yA + 32;                                                // [32] ir id2 s g
-    int4 *yJ = reinterpret_cast<int4 *>(yB + 32);                        // [32] j t
-    float4 *yW0 = reinterpret_cast<float4 *>(yJ + 32);                   // [32] w[0..3]
-    float4 *yW1 = yW0 + 32;                                              // [32] w[4..7] (zero padded)
-    float4 *yD0 = yW1 + 32;                                              // [32] dw[0..3]
-    float4 *yD1 = yD0 + 32;                                              // [32] dw[4..7]
+    unsigned char *wbase = smb + atmb_smem_fixed(ne, NR) + (size_t)warp * atmb_smem_warp(ne, NR);
+    constexpr int RQ = atmb_row_floats(NR) / 4;                          // float4 quads per row
+    // buffer layout: [ne][RQ][32] rows of the y block, [32] vx vy vz d2, [32] ir id2 s g
+    float4 *ybuf0 = reinterpret_cast<float4 *>(wbase);
+    const size_t bufq = atmb_buf_quads(ne, NR);
     __shared__ int s_item;
     __shared__ double red[ATMB_MAXW][12];
-    float4 *sA = scratch + (size_t)blockIdx.x * 3 * ATMB_MCAP;           // vx vy vz d2
+    float4 *sA = scratch + (size_t)blockIdx.x * ATMB_SCRATCH_PER_CTA;    // vx vy vz d2
     float4 *sB = sA + ATMB_MCAP;                                         // ir id2 s g
     float4 *sJ = sB + ATMB_MCAP;                                         // j t lam_ea lam_ae
+    float *acc = reinterpret_cast<float *>(sJ + ATMB_MCAP);              // [6][MCAP] (global, L2-resident)
     if (p.atm_off[p.n] > p.atm_cap) return; // list overflowed: the host grows it and re-runs
     for (int k = tid; k < ne * ne; k += blockDim.x) r0sq[k] = (float)(p.r0ab[k] * p.r0ab[k]);
+    static_assert(NR == 5 || NR == 7, "reference counts of the parameter tables");
     const float x16c = (float)(4294967296.0 / 43046721.0); // (4/3)^16
     const float third = 1.0f / 3.0f;
     const float ratm2f = (float)p.ratm2;
@@ -253,7 +329,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
         for (int k = tid; k < 512; k += blockDim.x) cellpos[k] = 0;
         for (int q = 0; q < 6; ++q)
-            for (int e = tid; e < m; e += blockDim.x) acc[q * ATMB_MCAP + e] = 0.f;
+            for (int e = tid; e < m; e += blockDim.x) __stcg(&acc[q * ATMB_MCAP + e], 0.f);
         double dwa[NR];
 #pragma unroll
         for (int b = 0; b < NR; ++b) dwa[b] = p.dw[(size_t)a * NR + b];
@@ -318,6 +394,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
             sB[pos] = make_float4((float)(1.0 / sqrt(d2)), (float)(1.0 / d2), (float)sqrt(c6),
                                   (float)pow((double)r0sq[ta * ne + tp] / d2, 8.0 / 3.0));
             sJ[pos] = make_float4(__int_as_float(jp), __int_as_float(tp), (float)(dcq / c6), (float)(dca / c6));
+            sjy[pos] = jp;
         }
         __syncthreads();
         // ---- block bounding boxes
@@ -348,8 +425,16 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
             if (A >= nb) break;
             const int xe = A * 32 + lane;
             const bool xvalid = xe < m;
-            float vx = 1e30f, vy = 1e30f, vz = 1e30f, d1 = 1.f, ir1 = 1.f, id1 = 1.f, sq = 0.f, gq = 0.f;
+            // a lane without entry sits at a far point (distinct from the padding partners)
+            // with weights (1, 0, ...), so its visits stay finite
+            float vx = 3e4f, vy = 3e4f, vz = 3e4f, d1 = 1.f, ir1 = 1.f, id1 = 1.f, sq = 0.f, gq = 0.f;
             int jx = -1, tx = 0;
+            float wx[NR], dwx[NR];
+#pragma unroll
+            for (int b = 0; b < NR; ++b) {
+                wx[b] = b == 0 ? 1.f : 0.f;
+                dwx[b] = 0.f;
+            }
             if (xvalid) {
                 const float4 qa4 = sA[xe], qb4 = sB[xe], qj4 = sJ[xe];
                 vx = qa4.x;
@@ -359,104 +444,138 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
                 ir1 = qb4.x;
                 id1 = qb4.y;
                 sq = qb4.z;
-                gq = qb4.w;
+                gq = qb4.w * x16c;
                 jx = __float_as_int(qj4.x);
                 tx = __float_as_int(qj4.y);
-                // the entry's C6 rows and their CN derivatives for every type
-                for (int t = 0; t < ne; ++t) {
-                    const float *ys = p.Y32 + ((size_t)jx * ne + t) * NR;
-                    const float *ds = p.D32 + ((size_t)jx * ne + t) * NR;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        xrow[(t * 8 + q) * 32 + lane] =
-                            make_float2(2 * q < NR ? ys[2 * q] : 0.f, 2 * q + 1 < NR ? ys[2 * q + 1] : 0.f);
-                        xrow[(t * 8 + 4 + q) * 32 + lane] =
-                            make_float2(2 * q < NR ? ds[2 * q] : 0.f, 2 * q + 1 < NR ? ds[2 * q + 1] : 0.f);
-                    }
+                for (int b = 0; b < NR; ++b) {
+                    wx[b] = p.w32[(size_t)jx * NR + b];
+                    dwx[b] = p.dw32[(size_t)jx * NR + b];
                 }
-            } else {
-                // rows of a lane without entry stay finite (its visits run with zero weights)
-                for (int t = 0; t < ne * 8; ++t) xrow[t * 32 + lane] = make_float2(0.f, 0.f);
             }
             const bool qa = (jx == a);
             double xs[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0}; // SE SD SF Wx Wy Wz SA Ux Uy Uz (row carries)
-            for (int B = A; B < nb; ++B) {
-                {
-                    const float4 la = bblo[A], ha = bbhi[A], lb = bblo[B], hb = bbhi[B];
-                    const float dx = fmaxf(0.f, fmaxf(la.x - hb.x, lb.x - ha.x));
-                    const float dy = fmaxf(0.f, fmaxf(la.y - hb.y, lb.y - ha.y));
-                    const float dz = fmaxf(0.f, fmaxf(la.z - hb.z, lb.z - ha.z));
-                    if (fmaf(dx, dx, fmaf(dy, dy, dz * dz)) > ratm2f * 1.0001f) continue;
-                }
-                __syncwarp();
-                {
-                    const int ye = B * 32 + lane;
-                    if (ye < m) {
-                        yA[lane] = sA[ye];
-                        yB[lane] = sB[ye];
-                        const float4 qj4 = sJ[ye];
-                        const int jy = __float_as_int(qj4.x);
-                        yJ[lane] = make_int4(jy, __float_as_int(qj4.y), 0, 0);
-                        float wv[8], dv[8];
+            // block pairs (A, B) whose boxes are within rc_ATM, visited in order of B; the
+            // y block of the next one is copied (cp.async) while the current one is visited
+            auto near = [&](int B) {
+                const float4 la = bblo[A], ha = bbhi[A], lb = bblo[B], hb = bbhi[B];
+                const float dx = fmaxf(0.f, fmaxf(la.x - hb.x, lb.x - ha.x));
+                const float dy = fmaxf(0.f, fmaxf(la.y - hb.y, lb.y - ha.y));
+                const float dz = fmaxf(0.f, fmaxf(la.z - hb.z, lb.z - ha.z));
+                return fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= ratm2f * 1.0001f;
+            };
+            auto next_near = [&](int B) {
+                while (B < nb && !near(B)) ++B;
+                return B;
+            };
+            auto stage = [&](int B, float4 *buf) {
+                float4 *rows = buf, *ya = buf + ne * RQ * 32, *yb = ya + 32;
+                const int ye = B * 32 + lane;
+                if (ye < m) {
+                    atmb_cp16(ya + lane, sA + ye);
+                    atmb_cp16(yb + lane, sB + ye);
+                    const float4 *src = reinterpret_cast<const float4 *>(p.YD32) + (size_t)sjy[ye] * ne * RQ;
+                    for (int t = 0; t < ne; ++t)
 #pragma unroll
-                        for (int b = 0; b < 8; ++b) {
-                            wv[b] = b < NR ? p.w32[(size_t)jy * NR + b] : 0.f;
-                            dv[b] = b < NR ? p.dw32[(size_t)jy * NR + b] : 0.f;
-                        }
-                        yW0[lane] = make_float4(wv[0], wv[1], wv[2], wv[3]);
-                        yW1[lane] = make_float4(wv[4], wv[5], wv[6], wv[7]);
-                        yD0[lane] = make_float4(dv[0], dv[1], dv[2], dv[3]);
-                        yD1[lane] = make_float4(dv[4], dv[5], dv[6], dv[7]);
-                    } else {
-                        // far-away dummy: fails every distance test
-                        yA[lane] = make_float4(1e30f, 1e30f, 1e30f, 1.f);
-                        yB[lane] = make_float4(1.f, 1.f, 0.f, 0.f);
-                        yJ[lane] = make_int4(-1, 0, 0, 0);
-                        yW0[lane] = yW1[lane] = yD0[lane] = yD1[lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-                    }
+                        for (int q = 0; q < RQ; ++q) atmb_cp16(rows + (t * RQ + q) * 32 + lane, src + t * RQ + q);
+                } else {
+                    // padding partner: a far point with zero C6 share that fails every
+                    // distance test; unit rows keep C6_xy positive
+                    ya[lane] = make_float4(-3e4f, -3e4f, -3e4f, 1.f);
+                    yb[lane] = make_float4(1.f, 1.f, 0.f, 0.f);
+                    for (int t = 0; t < ne; ++t) AtmbRowFill<NR>::padding(rows + t * RQ * 32 + lane);
                 }
-                __syncwarp();
-                AtmbSide xt{};     // x side of this block pair
-                AtmbSide y0{}, y1{}; // y sides, travelling with their y (two steps per iteration)
-                float aFx = 0.f, aFy = 0.f, aFz = 0.f; // apex force, a-y sides
+            };
+            int B = next_near(A);
+            int cur = 0;
+            __syncwarp(); // the previous row's visits are done with both buffers
+            if (B < nb) stage(B, ybuf0);
+            atmb_cp_commit();
+            while (B < nb) {
+                const int Bn = next_near(B + 1);
+                __syncwarp(); // every lane is done with the other buffer
+                if (Bn < nb) stage(Bn, ybuf0 + (cur ^ 1) * bufq);
+                atmb_cp_commit();
+                atmb_cp_wait<1>(); // this lane's copies of block B have landed
+                __syncwarp();      // ... and every lane's
+                const float4 *yrow = ybuf0 + cur * bufq;
+                const float4 *yA = yrow + ne * RQ * 32;
+                const float4 *yB = yA + 32;
+                AtmbSide xt{}; // x side of this block pair
+                AtmbSide ys[ATMB_VPI]; // y sides, travelling with their y (ATMB_VPI steps per iteration)
+#pragma unroll
+                for (int q = 0; q < ATMB_VPI; ++q) ys[q] = AtmbSide{};
                 const bool diag = (A == B);
                 const int s0 = diag ? 1 : 0, s1 = diag ? 17 : 32;
-                const AtmbX X{vx, vy, vz, d1, ir1, id1, sq, gq, jx, tx, qa, xvalid};
-                for (int s = s0; s < s1; s += 2) {
-                    // two independent visits per iteration (steps s and s + 1) for ILP
-                    const int k0 = (lane + s) & 31, k1 = (lane + s + 1) & 31;
-                    const float4 ya0 = yA[k0], ya1 = yA[k1];
-                    float rx = vx - ya0.x, ry = vy - ya0.y, rz = vz - ya0.z;
-                    const float d30 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-                    rx = vx - ya1.x;
-                    ry = vy - ya1.y;
-                    rz = vz - ya1.z;
-                    const float d31 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-                    const bool act0 = xvalid && (!diag || s < 16 || lane < 16) && d30 <= ratm2f && d30 >= 1e-12f;
-                    const bool act1 = xvalid && (!diag || s + 1 < 16 || lane < 16) && d31 <= ratm2f && d31 >= 1e-12f;
-                    if (__any_sync(0xffffffffu, act0 || act1)) {
-                        visits += (act0 ? 2 : 0) + (act1 ? 2 : 0);
+                AtmbX<NR> X;
+                X.vx = vx;
+                X.vy = vy;
+                X.vz = vz;
+                X.d1 = d1;
+                X.ir1 = ir1;
+                X.id1 = id1;
+                X.sq = sq;
+                X.gq = gq;
+                X.c1 = -0.75f * d1;
+                X.d1x3 = 3.0f * d1;
+#pragma unroll
+                for (int b = 0; b < NR; ++b) {
+                    X.w[b] = wx[b];
+                    X.dw[b] = dwx[b];
+                }
+                X.jx = jx;
+                X.qa = qa;
+                const float4 *yrow_x = yrow + tx * RQ * 32; // rows at the x entry's type
+                int nv = 0;
+                for (int s = s0; s < s1; s += ATMB_VPI) {
+                    // ATMB_VPI independent visits per iteration (steps s .. s + ATMB_VPI - 1) for ILP
+                    int kq[ATMB_VPI];
+                    float4 yq[ATMB_VPI];
+                    float d3q[ATMB_VPI];
+                    bool aq[ATMB_VPI];
+                    bool any = false;
+#pragma unroll
+                    for (int q = 0; q < ATMB_VPI; ++q) {
+                        kq[q] = (lane + s + q) & 31;
+                        yq[q] = yA[kq[q]];
+                        const float rx = vx - yq[q].x, ry = vy - yq[q].y, rz = vz - yq[q].z;
+                        d3q[q] = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+                        aq[q] = xvalid && (!diag || s + q < 16 || lane < 16) && d3q[q] <= ratm2f && d3q[q] >= 1e-12f;
+                        any |= aq[q];
+                        nv += aq[q] ? 2 : 0;
+                    }
+                    if (__any_sync(0xffffffffu, any)) {
                         if (simple) {
-                            atmb_visit<NR, true>(X, k0, ya0, d30, act0, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq,
-                                                 ne, a, x16c, third, force_scaled, xt, y0, aFx, aFy, aFz, apx);
-                            atmb_visit<NR, true>(X, k1, ya1, d31, act1, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq,
-                                                 ne, a, x16c, third, force_scaled, xt, y1, aFx, aFy, aFz, apx);
+#pragma unroll
+                            for (int q = 0; q < ATMB_VPI; ++q)
+                                atmb_visit<NR, true>(X, kq[q], yq[q], d3q[q], aq[q], yB, yrow_x, a, third,
+                                                     force_scaled, xt, ys[q], apx);
                         } else {
-                            atmb_visit<NR, false>(X, k0, ya0, d30, act0, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq,
-                                                  ne, a, x16c, third, force_scaled, xt, y0, aFx, aFy, aFz, apx);
-                            atmb_visit<NR, false>(X, k1, ya1, d31, act1, yB, yJ, yW0, yW1, yD0, yD1, xrow, lane, r0sq,
-                                                  ne, a, x16c, third, force_scaled, xt, y1, aFx, aFy, aFz, apx);
+#pragma unroll
+                            for (int q = 0; q < ATMB_VPI; ++q)
+                                atmb_visit<NR, false>(X, kq[q], yq[q], d3q[q], aq[q], yB, yrow_x, a, third,
+                                                      force_scaled, xt, ys[q], apx);
                         }
                     }
-                    const int src = (lane + 2) & 31;
-                    y0.shift(src);
-                    y1.shift(src);
+                    const int src = (lane + ATMB_VPI) & 31;
+#pragma unroll
+                    for (int q = 0; q < ATMB_VPI; ++q) ys[q].shift(src);
                 }
-                // lanes now hold the complete sums of y entries B[(lane + s1) mod 32] and
-                // B[(lane + s1 + 1) mod 32]
-                y0.flush(acc, B * 32 + ((lane + s1) & 31), m);
-                y1.flush(acc, B * 32 + ((lane + s1 + 1) & 31), m);
-                const float tSE = xt.SE, tSD = xt.SD, tSF = xt.SF, tWx = xt.Wx, tWy = xt.Wy, tWz = xt.Wz, tSA = xt.SA;
+                visits += (unsigned long long)nv;
+                // lane L now holds in ys[q] the complete sums of y entry B[(L + s1 + q) mod 32]
+                // from the visits of step parity q: gather the entry B[(L + s1) mod 32] in ys[0]
+#pragma unroll
+                for (int q = 1; q < ATMB_VPI; ++q) ys[0].add_from(ys[q], (lane - q) & 31);
+                {
+                    const int ey = (lane + s1) & 31;
+                    ys[0].flush(acc, B * 32 + ey, m);
+                    // apex force of the a-y sides (padding partners carry zero sums)
+                    const float4 vyv = yA[ey];
+                    apx[0] -= (double)(ys[0].SA * vyv.x);
+                    apx[1] -= (double)(ys[0].SA * vyv.y);
+                    apx[2] -= (double)(ys[0].SA * vyv.z);
+                }
+                const float tSE = xt.SE, tSD = xt.SD, tSF = xt.SA + xt.S3, tWx = xt.Wx, tWy = xt.Wy, tWz = xt.Wz, tSA = xt.SA;
                 const float tUx = simple ? xt.Wx : xt.Ux, tUy = simple ? xt.Wy : xt.Uy, tUz = simple ? xt.Wz : xt.Uz;
                 xs[0] += tSE;
                 xs[1] += tSD;
@@ -468,10 +587,10 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
                 xs[7] += tUx;
                 xs[8] += tUy;
                 xs[9] += tUz;
-                apx[0] -= aFx;
-                apx[1] -= aFy;
-                apx[2] -= aFz;
+                B = Bn;
+                cur ^= 1;
             }
+            atmb_cp_wait<0>();
             if (xvalid) {
                 atomicAdd(&acc[0 * ATMB_MCAP + xe], (float)xs[0]);
                 atomicAdd(&acc[1 * ATMB_MCAP + xe], (float)xs[1]);
@@ -496,8 +615,10 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         // ---- 4. per entry: atom shares (FP64 atomics) and the apex's sums
         double ea = 0, ga = 0;
         for (int e = tid; e < m; e += blockDim.x) {
-            const double SE = acc[e], SD = acc[ATMB_MCAP + e], SF = acc[2 * ATMB_MCAP + e];
-            const double Wx = acc[3 * ATMB_MCAP + e], Wy = acc[4 * ATMB_MCAP + e], Wz = acc[5 * ATMB_MCAP + e];
+            // accumulated at L2 by atomics: read past L1
+            const double SE = __ldcg(&acc[e]), SD = __ldcg(&acc[ATMB_MCAP + e]), SF = __ldcg(&acc[2 * ATMB_MCAP + e]);
+            const double Wx = __ldcg(&acc[3 * ATMB_MCAP + e]), Wy = __ldcg(&acc[4 * ATMB_MCAP + e]);
+            const double Wz = __ldcg(&acc[5 * ATMB_MCAP + e]);
             const float4 qa4 = sA[e], qj4 = sJ[e];
             const int j = __float_as_int(qj4.x);
             const double lam_ea = qj4.z, lam_ae = qj4.w;

@@ -45,6 +45,9 @@ namespace d3 {
 
 constexpr double K1 = 16.0;
 constexpr double K3 = 4.0;
+// floats per (atom, partner type) row of the block-pair ATM table (NR 5 or 7: 12 or 16,
+// whole float4s)
+__host__ __device__ constexpr int atmb_row_floats(int nr) { return 2 * nr + 2; }
 
 // ------------------------------------------------------------------------------------
 // kernel parameter block (passed by value)
@@ -117,7 +120,8 @@ struct KP {
     int precision;
     float4 *xs32;
     float *w32, *dw32, *Y32;
-    float *D32;     // [n][ne][NR]: d/dCN of the own weights through the C6 rows (block-pair ATM)
+    float *YD32;    // [n][ne][2 NR + 2] (block-pair ATM): per partner type the C6 row, r0^2 of
+                    // the type pair, the row of the weight derivatives, the atom index bits
     int atm_min_m;  // k_atm32 takes only apexes with longer lists (the rest: k_atm32b)
     // sharded evaluation: this process computes the two-body and chain-rule terms of central
     // atoms i = shard_rank + k shard_world (binned order) and the ATM apexes of work items
@@ -444,12 +448,20 @@ __global__ void k_weights(KP p) {
             for (int a = 0; a < NR; ++a) acc += w[a] * C[a * NR + b];
             Yo[b] = acc;
             if (p.precision) p.Y32[((size_t)i * p.ne + tt) * NR + b] = (float)acc;
-            if (p.D32) {
+            if (p.YD32) {
                 double dacc = 0.0;
 #pragma unroll
                 for (int a = 0; a < NR; ++a) dacc += dw[a] * C[a * NR + b];
-                p.D32[((size_t)i * p.ne + tt) * NR + b] = (float)dacc;
+                float *r = p.YD32 + ((size_t)i * p.ne + tt) * atmb_row_floats(NR);
+                r[b] = (float)acc;
+                r[NR + 1 + b] = (float)dacc;
             }
+        }
+        if (p.YD32) {
+            float *r = p.YD32 + ((size_t)i * p.ne + tt) * atmb_row_floats(NR);
+            const double r0 = p.r0ab[tt * p.ne + t]; // partner type tt first, as the triplet kernel reads it
+            r[NR] = (float)(r0 * r0);
+            r[2 * NR + 1] = __int_as_float(i);
         }
     }
 }
@@ -1125,7 +1137,7 @@ struct Engine {
     DBuf<int> atm_cnt, work, sid_in, sid;
     DBuf<SG> sg_dev;
     DBuf<float4> xs32;
-    DBuf<float> w32, dw32, Y32, D32;
+    DBuf<float> w32, dw32, Y32, YD32;
     DBuf<float4> atmb_scratch;
     DBuf<long long> atm_off;
     DBuf<int2> atm_ent;
@@ -1161,7 +1173,7 @@ struct Engine {
         w32.release();
         dw32.release();
         Y32.release();
-        D32.release();
+        YD32.release();
         atmb_scratch.release();
         xw_in.release();
         xs.release();
@@ -1594,7 +1606,7 @@ static int blockpair_warps(const Engine *e) {
     if (!e->use_atm || !e->opt.precision || e->opt.atm_schedule != 0) return 0;
     if (e->opt.atm_surrogate && e->surr.loaded) return 0;
     const size_t limit = 227 * 1024 - 1024; // opt-in maximum minus the static arrays
-    const size_t fixed = atmb_smem_fixed(e->ne, e->nref), per = atmb_smem_warp(e->ne);
+    const size_t fixed = atmb_smem_fixed(e->ne, e->nref), per = atmb_smem_warp(e->ne, e->nref);
     if (fixed + 2 * per > limit) return 0;
     return (int)std::min<size_t>(ATMB_MAXW, (limit - fixed) / per);
 }
@@ -1642,12 +1654,12 @@ static KP make_kp(Engine *e) {
     p.w32 = e->w32.p;
     p.dw32 = e->dw32.p;
     p.Y32 = e->Y32.p;
-    p.D32 = nullptr;
+    p.YD32 = nullptr;
     p.atm_min_m = 0;
     if (blockpair_warps(e) > 0) {
-        e->D32.ensure((size_t)e->max_atoms * e->ne * e->nref);
-        e->atmb_scratch.ensure((size_t)e->dev_sms * 3 * ATMB_MCAP);
-        p.D32 = e->D32.p;
+        e->YD32.ensure((size_t)e->max_atoms * e->ne * atmb_row_floats(e->nref));
+        e->atmb_scratch.ensure((size_t)e->dev_sms * ATMB_SCRATCH_PER_CTA);
+        p.YD32 = e->YD32.p;
     }
     p.atm_force_scaled = e->opt.atm_force_scaled ? 1 : 0;
     p.pos_in = e->pos_in.p;
@@ -1826,7 +1838,7 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
                 const int nwb = blockpair_warps(e);
                 if (nwb > 0 && !surr) {
                     // lists up to ATMB_MCAP entries: block-pair schedule; longer ones below
-                    const size_t smb = atmb_smem_fixed(p.ne, NR) + (size_t)nwb * atmb_smem_warp(p.ne);
+                    const size_t smb = atmb_smem_fixed(p.ne, NR) + (size_t)nwb * atmb_smem_warp(p.ne, NR);
                     atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR>);
                     k_atm32b<NR><<<e->dev_sms, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
                     D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
