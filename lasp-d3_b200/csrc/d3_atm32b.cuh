@@ -33,6 +33,7 @@
 constexpr int ATMB_MCAP = 4096;   // longest list this kernel takes (longer lists: k_atm32)
 constexpr int ATMB_GRID = 8;      // spatial grid per dimension for the entry sort
 constexpr int ATMB_MAXW = 8;      // warps per CTA at most
+constexpr int ATMB_CTAS_PER_SM = 2; // preferred CTAs per SM (of four warps each)
 constexpr int ATMB_VPI = 4;       // visits per lane per iteration (independent, for ILP)
 
 // global scratch per CTA (float4 units): per-entry records sA, sB, sJ and the per-entry
@@ -53,7 +54,20 @@ __host__ __device__ inline size_t atmb_smem_fixed(int ne, int NR) {
 // type as float4 [type][row quad][lane] (lanes read consecutive 16-byte words whatever the
 // x type, so the reads are free of bank conflicts) and positions / per-entry constants
 __host__ __device__ inline size_t atmb_buf_quads(int ne, int NR) { return 32 * ((size_t)ne * (atmb_row_floats(NR) / 4) + 2); }
-__host__ __device__ inline size_t atmb_smem_warp(int ne, int NR) { return 2 * atmb_buf_quads(ne, NR) * sizeof(float4); }
+// plus the lanes' FP64 carries (apex force and virial, row sums of the x entry), [19][lane]
+// and the current block's positions / per-entry constants with entries k, k + 1 side by
+// side ([4][32] float4)
+constexpr int ATMB_NCARRY = 19;
+__host__ __device__ inline size_t atmb_smem_warp(int ne, int NR) {
+    return 2 * atmb_buf_quads(ne, NR) * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double) + 4 * 32 * sizeof(float4);
+}
+
+// a lane's view of FP64 carries kept in shared memory ([q][32] doubles): they change once
+// per block pair, so they need not hold registers through the visits
+struct AtmbCarry {
+    double *p;
+    __device__ __forceinline__ double &operator[](int q) const { return p[q * 32]; }
+};
 
 // 16-byte global -> shared copy that bypasses registers (cached in L2 only)
 __device__ __forceinline__ void atmb_cp16(void *dst, const void *src) {
@@ -127,20 +141,30 @@ struct AtmbRowFill {
     }
 };
 
+// packed pairs of references: NR = 5 as (0,1) (2,3) + 4, NR = 7 as (0,1) (2,3) (4,5) + 6
 template <int NR>
-__device__ __forceinline__ float atmb_dot(const float *r, const float *v) {
-    float s = r[0] * v[0];
-#pragma unroll
-    for (int b = 1; b < NR; ++b) s = fmaf(r[b], v[b], s);
-    return s;
+struct AtmbVec {
+    float2 p[(NR - 1) / 2];
+    float l;
+};
+
+// sum_b r[b] v[b]: pairs of references in packed multiply-adds, the last one and the
+// halves of the pair sum as scalars
+template <int NR>
+__device__ __forceinline__ float atmb_dot2(const float *r, const AtmbVec<NR> &v) {
+    float2 acc = __fmul2_rn(make_float2(r[0], r[1]), v.p[0]);
+    acc = __ffma2_rn(make_float2(r[2], r[3]), v.p[1], acc);
+    if constexpr (NR == 7) acc = __ffma2_rn(make_float2(r[4], r[5]), v.p[2], acc);
+    return fmaf(r[NR - 1], v.l, acc.x) + acc.y;
 }
 
-// per-row constants of the x entry; gq carries the factor (4/3)^16, c1 = -0.75 d1,
-// d1x3 = 3 d1; w, dw its own C6 weights and their CN derivatives
+// per-row constants of the x entry as (v, v) pairs for the packed arithmetic of two visits;
+// gq carries the factor (4/3)^16, c1 = -0.75 d1, d1x3 = 3 d1; w, dw its own C6 weights and
+// their CN derivatives
 template <int NR>
-struct AtmbX {
-    float vx, vy, vz, d1, ir1, id1, sq, gq, c1, d1x3;
-    float w[NR], dw[NR];
+struct AtmbX2 {
+    float2 vx, vy, vz, d1, ir1, id1, sq, gq, c1, d1x3;
+    AtmbVec<NR> w, dw;
     int jx;
     bool qa;
 };
@@ -181,101 +205,151 @@ struct AtmbSide {
     }
 };
 
-// One (possible) visit of entry x with staged partner k: triplet term, x-side sums into
-// xt, y-side sums into ys, virial corrections where the virial and force weights differ.
+// packed sums of one block pair: component x for one visit of a pair, y for the other
+struct AtmbSide2 {
+    float2 SE, SD, SA, S3, Wx, Wy, Wz, Ux, Uy, Uz;
+    // the y sums move with their y: take those of lane src
+    __device__ __forceinline__ void shift(int src) {
+        float2 *v[7] = {&SE, &SD, &SA, &S3, &Wx, &Wy, &Wz};
+#pragma unroll
+        for (int q = 0; q < 7; ++q) {
+            v[q]->x = __shfl_sync(0xffffffffu, v[q]->x, src);
+            v[q]->y = __shfl_sync(0xffffffffu, v[q]->y, src);
+        }
+    }
+    // one component as a scalar side (y sums only)
+    __device__ __forceinline__ AtmbSide part(int c) const {
+        AtmbSide o{};
+        o.SE = c ? SE.y : SE.x;
+        o.SD = c ? SD.y : SD.x;
+        o.SA = c ? SA.y : SA.x;
+        o.S3 = c ? S3.y : S3.x;
+        o.Wx = c ? Wx.y : Wx.x;
+        o.Wy = c ? Wy.y : Wy.x;
+        o.Wz = c ? Wz.y : Wz.x;
+        return o;
+    }
+};
+
+// Two (possible) visits of entry x, with the staged partners k0 and k1 = k0 + 1 (mod 32)
+// of two consecutive steps, in packed f32x2 arithmetic (component x: k0, y: k1): triplet
+// terms, x-side sums into xt, y-side sums into ys, virial corrections where the virial and
+// force weights differ. P0 = (x, x', y, y'), P1 = (z, z', d2, d2') of the two partners.
 // Branch-free: an out-of-range pair (act false) runs on finite stand-in values (lanes
 // without entry and padding partners sit at far, distinct points with positive C6 rows)
-// with zero weights, so the visits of an iteration can be interleaved by the compiler.
-// With P = t1 t2 t3 (t1 = d1 + d2 - d3 ...), the angular term is
+// with zero weights. With P = t1 t2 t3 (t1 = d1 + d2 - d3 ...), the angular term is
 // A = (1 + 3/8 P / (d1 d2 d3)) / (r1 r2 r3)^3 and its side derivatives
 // dA/dr_k / r_k = q52 G_k, G_k = 15/8 P + 3 d1 d2 d3 - 3/4 d_k (T - 2 t_ij),
-// T = t12 + t13 + t23 (t_ij the product of the two t's without t_k).
+// T = t12 + t13 + t23 (t_ij the product of the two t's without t_k). Signs are carried in
+// the constants (f32x2 has add, mul and fma only): nw = -w, Em = -E, ndfd = -dfd.
 template <int NR, bool SIMPLE>
-__device__ __forceinline__ void atmb_visit(const AtmbX<NR> &X, int k, const float4 ya, float d3in, bool act,
-                                           const float4 *yB, const float4 *yrow, int a, float third,
-                                           bool force_scaled, AtmbSide &xt, AtmbSide &ys, double *apx) {
-    const float d3 = act ? d3in : X.d1;
-    const float4 yb = yB[k];
-    AtmbRow<NR> R; // the y entry's rows at the x entry's type
-    R.load(yrow, k);
-    const float ir3 = rsqrtf(d3);
-    const float id3 = ir3 * ir3;
+__device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 d3in, bool act0, bool act1,
+                                            const float4 P0, const float4 P1, const float4 *yQ0, const float4 *yQ1,
+                                            const float4 *yrow, int a, float third, bool force_scaled,
+                                            AtmbSide2 &xt, AtmbSide2 &ys, const AtmbCarry &apx) {
+    const int k1 = (k0 + 1) & 31;
+    const float2 ONE = make_float2(1.0f, 1.0f), M1 = make_float2(-1.0f, -1.0f), M2 = make_float2(-2.0f, -2.0f);
+    const float2 d3 = make_float2(act0 ? d3in.x : X.d1.x, act1 ? d3in.y : X.d1.x);
+    const float4 Q0 = yQ0[k0], Q1 = yQ1[k0]; // (ir, ir', id2, id2'), (s, s', g, g')
+    AtmbRow<NR> R0, R1; // the partners' rows at the x entry's type
+    R0.load(yrow, k0);
+    R1.load(yrow, k1);
+    const float2 ir3 = make_float2(rsqrtf(d3.x), rsqrtf(d3.y));
+    const float2 id3 = __fmul2_rn(ir3, ir3);
     // C6_xy = Y_y[t_x] . w_x, its derivatives dw_x and through D_y[t_x] = dw_y C
-    const float c6 = atmb_dot<NR>(R.Y, X.w);
-    const float dcx = atmb_dot<NR>(R.Y, X.dw); // dC6_xy/dCN_x
-    const float dcy = atmb_dot<NR>(R.D, X.w);  // dC6_xy/dCN_y
-    const float is3 = rsqrtf(c6);
-    const float s3 = c6 * is3;
-    const float is3q = is3 * is3;
-    const float lam_xy = dcx * is3q, lam_yx = dcy * is3q;
-    const float u = R.r0sq * id3; // r0_xy^2 / d3
-    const float g3 = exp2f(__log2f(u) * (8.0f / 3.0f)); // u^(8/3)
+    const float2 c6 = make_float2(atmb_dot2<NR>(R0.Y, X.w), atmb_dot2<NR>(R1.Y, X.w));
+    const float2 dcx = make_float2(atmb_dot2<NR>(R0.Y, X.dw), atmb_dot2<NR>(R1.Y, X.dw)); // dC6_xy/dCN_x
+    const float2 dcy = make_float2(atmb_dot2<NR>(R0.D, X.w), atmb_dot2<NR>(R1.D, X.w));   // dC6_xy/dCN_y
+    const float2 is3 = make_float2(rsqrtf(c6.x), rsqrtf(c6.y));
+    const float2 s3 = __fmul2_rn(c6, is3);
+    const float2 is3q = __fmul2_rn(is3, is3);
+    const float2 lam_xy = __fmul2_rn(dcx, is3q), lam_yx = __fmul2_rn(dcy, is3q);
+    // (r0_xy^2 / d3)^(8/3)
+    const float2 lgu = __fmul2_rn(make_float2(__log2f(R0.r0sq * id3.x), __log2f(R1.r0sq * id3.y)),
+                                  make_float2(8.0f / 3.0f, 8.0f / 3.0f));
+    const float2 g3 = make_float2(exp2f(lgu.x), exp2f(lgu.y));
     // reference scale factors (src/d3_kernel.cu:1282-1290) as pair weights; SIMPLE: no
     // atom appears twice in the list (cell heights > 2 rc_ATM), every weight is 1
-    float w, wf;
+    float2 nw, wf;
     if (SIMPLE) {
-        w = wf = act ? 1.0f : 0.0f;
+        wf = make_float2(act0 ? 1.0f : 0.0f, act1 ? 1.0f : 0.0f);
+        nw = make_float2(act0 ? -1.0f : 0.0f, act1 ? -1.0f : 0.0f);
     } else {
-        const int jy = R.j;
-        const bool same = (X.jx == jy);
-        const bool apex_img = X.qa | (jy == a);
-        w = act ? (same ? (X.qa ? third : 1.0f) : (apex_img ? 0.5f : 1.0f)) : 0.0f;
-        wf = act ? (force_scaled ? w : (same ? 2.0f : 1.0f)) : 0.0f;
+        const bool same0 = (X.jx == R0.j), same1 = (X.jx == R1.j);
+        const bool img0 = X.qa | (R0.j == a), img1 = X.qa | (R1.j == a);
+        const float w0 = act0 ? (same0 ? (X.qa ? third : 1.0f) : (img0 ? 0.5f : 1.0f)) : 0.0f;
+        const float w1 = act1 ? (same1 ? (X.qa ? third : 1.0f) : (img1 ? 0.5f : 1.0f)) : 0.0f;
+        nw = make_float2(-w0, -w1);
+        wf = make_float2(act0 ? (force_scaled ? w0 : (same0 ? 2.0f : 1.0f)) : 0.0f,
+                         act1 ? (force_scaled ? w1 : (same1 ? 2.0f : 1.0f)) : 0.0f);
     }
-    const float d1 = X.d1, d2 = ya.w;
-    const float irsq = X.id1 * yb.y * id3;
-    const float ir9 = irsq * X.ir1 * yb.x * ir3;
-    const float t1 = d1 + d2 - d3, t2 = d1 - d2 + d3, t3 = -d1 + d2 + d3;
-    const float t12 = t1 * t2, t13 = t1 * t3, t23 = t2 * t3;
-    const float P = t12 * t3;
-    const float T = t12 + t13 + t23;
-    const float Aang = fmaf(0.375f * P, irsq, 1.0f) * ir9;
-    const float q52 = ir9 * irsq;
-    const float base = fmaf(1.875f, P, X.d1x3 * d2 * d3);
-    const float G1 = fmaf(X.c1, fmaf(-2.0f, t12, T), base);
-    const float G2 = fmaf(-0.75f * d2, fmaf(-2.0f, t13, T), base);
-    const float G3 = fmaf(-0.75f * d3, fmaf(-2.0f, t23, T), base);
-    const float x16 = X.gq * yb.w * g3;
-    const float fd = __fdividef(1.0f, fmaf(6.0f, x16, 1.0f));
-    const float dfd = 32.0f * x16 * fd * fd;
-    const float nC9 = X.sq * yb.z * s3; // -C9
-    const float nC9fd = nC9 * fd;
-    const float Et = -nC9fd * Aang;
-    const float Ap = nC9fd * q52, Bp = nC9 * Aang * dfd;
-    const float f1 = fmaf(Ap, G1, -Bp) * X.id1;
-    const float f2 = fmaf(Ap, G2, -Bp) * yb.y;
-    const float f3 = fmaf(Ap, G3, -Bp) * id3;
-    const float wE = w * Et;
-    const float wf3 = wf * f3;
-    xt.SE += wE;
-    xt.SD = fmaf(wE, lam_xy, xt.SD);
-    xt.SA = fmaf(wf, f1, xt.SA);
-    xt.S3 += wf3;
-    xt.Wx = fmaf(wf3, ya.x, xt.Wx);
-    xt.Wy = fmaf(wf3, ya.y, xt.Wy);
-    xt.Wz = fmaf(wf3, ya.z, xt.Wz);
-    if (!SIMPLE) { // SIMPLE: U = W
-        const float w3 = w * f3;
-        xt.Ux = fmaf(w3, ya.x, xt.Ux);
-        xt.Uy = fmaf(w3, ya.y, xt.Uy);
-        xt.Uz = fmaf(w3, ya.z, xt.Uz);
+    const float2 d1 = X.d1, d2 = make_float2(P1.z, P1.w);
+    const float2 irsq = __fmul2_rn(__fmul2_rn(X.id1, make_float2(Q0.z, Q0.w)), id3);
+    const float2 ir9 = __fmul2_rn(__fmul2_rn(__fmul2_rn(irsq, X.ir1), make_float2(Q0.x, Q0.y)), ir3);
+    const float2 t1 = __ffma2_rn(d3, M1, __fadd2_rn(d1, d2)); // d1 + d2 - d3
+    const float2 t2 = __fadd2_rn(__ffma2_rn(d2, M1, d1), d3); // d1 - d2 + d3
+    const float2 t3 = __fadd2_rn(__ffma2_rn(d1, M1, d2), d3); // -d1 + d2 + d3
+    const float2 t12 = __fmul2_rn(t1, t2), t13 = __fmul2_rn(t1, t3), t23 = __fmul2_rn(t2, t3);
+    const float2 P = __fmul2_rn(t12, t3);
+    const float2 T = __fadd2_rn(__fadd2_rn(t12, t13), t23);
+    const float2 Aang = __fmul2_rn(__ffma2_rn(__fmul2_rn(make_float2(0.375f, 0.375f), P), irsq, ONE), ir9);
+    const float2 q52 = __fmul2_rn(ir9, irsq);
+    const float2 base = __ffma2_rn(make_float2(1.875f, 1.875f), P, __fmul2_rn(__fmul2_rn(X.d1x3, d2), d3));
+    const float2 G1 = __ffma2_rn(X.c1, __ffma2_rn(M2, t12, T), base);
+    const float2 G2 = __ffma2_rn(__fmul2_rn(make_float2(-0.75f, -0.75f), d2), __ffma2_rn(M2, t13, T), base);
+    const float2 G3 = __ffma2_rn(__fmul2_rn(make_float2(-0.75f, -0.75f), d3), __ffma2_rn(M2, t23, T), base);
+    const float2 x16 = __fmul2_rn(__fmul2_rn(X.gq, make_float2(Q1.z, Q1.w)), g3);
+    const float2 den = __ffma2_rn(make_float2(6.0f, 6.0f), x16, ONE);
+    const float2 fd = make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y));
+    const float2 ndfd = __fmul2_rn(__fmul2_rn(__fmul2_rn(make_float2(-32.0f, -32.0f), x16), fd), fd);
+    const float2 nC9 = __fmul2_rn(__fmul2_rn(X.sq, make_float2(Q1.x, Q1.y)), s3); // -C9
+    const float2 nC9fd = __fmul2_rn(nC9, fd);
+    const float2 Em = __fmul2_rn(nC9fd, Aang); // -E
+    const float2 Ap = __fmul2_rn(nC9fd, q52), nBp = __fmul2_rn(__fmul2_rn(nC9, Aang), ndfd);
+    const float2 f1 = __fmul2_rn(__ffma2_rn(Ap, G1, nBp), X.id1);
+    const float2 f2 = __fmul2_rn(__ffma2_rn(Ap, G2, nBp), make_float2(Q0.z, Q0.w));
+    const float2 f3 = __fmul2_rn(__ffma2_rn(Ap, G3, nBp), id3);
+    const float2 wE = __fmul2_rn(nw, Em);
+    const float2 wf3 = __fmul2_rn(wf, f3);
+    const float2 yx = make_float2(P0.x, P0.y), yy = make_float2(P0.z, P0.w), yz = make_float2(P1.x, P1.y);
+    xt.SE = __fadd2_rn(xt.SE, wE);
+    xt.SD = __ffma2_rn(wE, lam_xy, xt.SD);
+    xt.SA = __ffma2_rn(wf, f1, xt.SA);
+    xt.S3 = __fadd2_rn(xt.S3, wf3);
+    xt.Wx = __ffma2_rn(wf3, yx, xt.Wx);
+    xt.Wy = __ffma2_rn(wf3, yy, xt.Wy);
+    xt.Wz = __ffma2_rn(wf3, yz, xt.Wz);
+    if (!SIMPLE) { // SIMPLE: U = W; here U accumulates -w f3 v_y
+        const float2 nw3 = __fmul2_rn(nw, f3);
+        xt.Ux = __ffma2_rn(nw3, yx, xt.Ux);
+        xt.Uy = __ffma2_rn(nw3, yy, xt.Uy);
+        xt.Uz = __ffma2_rn(nw3, yz, xt.Uz);
     }
-    ys.SE += wE;
-    ys.SD = fmaf(wE, lam_yx, ys.SD);
-    ys.SA = fmaf(wf, f2, ys.SA);
-    ys.S3 += wf3;
-    ys.Wx = fmaf(wf3, X.vx, ys.Wx);
-    ys.Wy = fmaf(wf3, X.vy, ys.Wy);
-    ys.Wz = fmaf(wf3, X.vz, ys.Wz);
-    if (!SIMPLE && w != wf) {
+    ys.SE = __fadd2_rn(ys.SE, wE);
+    ys.SD = __ffma2_rn(wE, lam_yx, ys.SD);
+    ys.SA = __ffma2_rn(wf, f2, ys.SA);
+    ys.S3 = __fadd2_rn(ys.S3, wf3);
+    ys.Wx = __ffma2_rn(wf3, X.vx, ys.Wx);
+    ys.Wy = __ffma2_rn(wf3, X.vy, ys.Wy);
+    ys.Wz = __ffma2_rn(wf3, X.vz, ys.Wz);
+    if (!SIMPLE) {
         // virial weights w where the force weights differ (repeated indices)
-        const double c1 = (double)(w - wf) * (double)(f1 + f3), c2 = (double)(w - wf) * (double)(f2 + f3);
-        apx[3] += c1 * X.vx * X.vx + c2 * ya.x * ya.x;
-        apx[4] += c1 * X.vy * X.vy + c2 * ya.y * ya.y;
-        apx[5] += c1 * X.vz * X.vz + c2 * ya.z * ya.z;
-        apx[6] += c1 * X.vx * X.vy + c2 * ya.x * ya.y;
-        apx[7] += c1 * X.vx * X.vz + c2 * ya.x * ya.z;
-        apx[8] += c1 * X.vy * X.vz + c2 * ya.y * ya.z;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const float w = c ? -nw.y : -nw.x, f = c ? wf.y : wf.x;
+            if (w != f) {
+                const float F1 = c ? f1.y : f1.x, F2 = c ? f2.y : f2.x, F3 = c ? f3.y : f3.x;
+                const float py = c ? P0.y : P0.x, pyy = c ? P0.w : P0.z, pz = c ? P1.y : P1.x;
+                const float vx = X.vx.x, vy = X.vy.x, vz = X.vz.x;
+                const double c1 = (double)(w - f) * (double)(F1 + F3), c2 = (double)(w - f) * (double)(F2 + F3);
+                apx[3] += c1 * vx * vx + c2 * py * py;
+                apx[4] += c1 * vy * vy + c2 * pyy * pyy;
+                apx[5] += c1 * vz * vz + c2 * pz * pz;
+                apx[6] += c1 * vx * vy + c2 * py * pyy;
+                apx[7] += c1 * vx * vz + c2 * py * pz;
+                apx[8] += c1 * vy * vz + c2 * pyy * pz;
+            }
+        }
     }
 }
 
@@ -419,7 +493,15 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         }
         __syncthreads();
         // ---- 2./3. block pairs
-        double apx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}; // apex force (3) and virial (6) of this lane
+        // apex force (3) and virial (6) of this lane, and the row sums of its x entry
+        const AtmbCarry apx{reinterpret_cast<double *>(wbase + 2 * bufq * sizeof(float4)) + lane};
+        const AtmbCarry xs{apx.p + 9 * 32}; // SE SD SF Wx Wy Wz SA Ux Uy Uz
+        // positions (x, x', y, y'), (z, z', d2, d2') and constants (ir, ir', id2, id2'),
+        // (s, s', g, g') of the current y block, entries k and k + 1 at slot k
+        float4 *yP0 = reinterpret_cast<float4 *>(wbase + 2 * bufq * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double));
+        float4 *yP1 = yP0 + 32, *yQ0 = yP1 + 32, *yQ1 = yQ0 + 32;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) apx[q] = 0.0;
         for (int r = 0;; ++r) {
             const int A = nw * r + ((r & 1) ? (nw - 1 - warp) : warp);
             if (A >= nb) break;
@@ -454,7 +536,28 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
                 }
             }
             const bool qa = (jx == a);
-            double xs[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0}; // SE SD SF Wx Wy Wz SA Ux Uy Uz (row carries)
+            AtmbX2<NR> X;
+            X.vx = make_float2(vx, vx);
+            X.vy = make_float2(vy, vy);
+            X.vz = make_float2(vz, vz);
+            X.d1 = make_float2(d1, d1);
+            X.ir1 = make_float2(ir1, ir1);
+            X.id1 = make_float2(id1, id1);
+            X.sq = make_float2(sq, sq);
+            X.gq = make_float2(gq, gq);
+            X.c1 = make_float2(-0.75f * d1, -0.75f * d1);
+            X.d1x3 = make_float2(3.0f * d1, 3.0f * d1);
+#pragma unroll
+            for (int i = 0; i < (NR - 1) / 2; ++i) {
+                X.w.p[i] = make_float2(wx[2 * i], wx[2 * i + 1]);
+                X.dw.p[i] = make_float2(dwx[2 * i], dwx[2 * i + 1]);
+            }
+            X.w.l = wx[NR - 1];
+            X.dw.l = dwx[NR - 1];
+            X.jx = jx;
+            X.qa = qa;
+#pragma unroll
+            for (int q = 0; q < 10; ++q) xs[q] = 0.0;
             // block pairs (A, B) whose boxes are within rc_ATM, visited in order of B; the
             // y block of the next one is copied (cp.async) while the current one is visited
             auto near = [&](int B) {
@@ -501,92 +604,101 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
                 const float4 *yrow = ybuf0 + cur * bufq;
                 const float4 *yA = yrow + ne * RQ * 32;
                 const float4 *yB = yA + 32;
-                AtmbSide xt{}; // x side of this block pair
-                AtmbSide ys[ATMB_VPI]; // y sides, travelling with their y (ATMB_VPI steps per iteration)
-#pragma unroll
-                for (int q = 0; q < ATMB_VPI; ++q) ys[q] = AtmbSide{};
+                {
+                    // entries k and k + 1 side by side at slot k, for the packed visits
+                    const float4 a0 = yA[lane], b0 = yB[lane];
+                    const int nx = (lane + 1) & 31;
+                    const float a1x = __shfl_sync(0xffffffffu, a0.x, nx), a1y = __shfl_sync(0xffffffffu, a0.y, nx);
+                    const float a1z = __shfl_sync(0xffffffffu, a0.z, nx), a1w = __shfl_sync(0xffffffffu, a0.w, nx);
+                    const float b1x = __shfl_sync(0xffffffffu, b0.x, nx), b1y = __shfl_sync(0xffffffffu, b0.y, nx);
+                    const float b1z = __shfl_sync(0xffffffffu, b0.z, nx), b1w = __shfl_sync(0xffffffffu, b0.w, nx);
+                    yP0[lane] = make_float4(a0.x, a1x, a0.y, a1y);
+                    yP1[lane] = make_float4(a0.z, a1z, a0.w, a1w);
+                    yQ0[lane] = make_float4(b0.x, b1x, b0.y, b1y);
+                    yQ1[lane] = make_float4(b0.z, b1z, b0.w, b1w);
+                }
+                __syncwarp();
+                AtmbSide2 xt{};    // x side of this block pair (two partial sums)
+                AtmbSide2 ys[2]{}; // y sides of steps s + 2p (x) and s + 2p + 1 (y), travelling with their y
                 const bool diag = (A == B);
                 const int s0 = diag ? 1 : 0, s1 = diag ? 17 : 32;
-                AtmbX<NR> X;
-                X.vx = vx;
-                X.vy = vy;
-                X.vz = vz;
-                X.d1 = d1;
-                X.ir1 = ir1;
-                X.id1 = id1;
-                X.sq = sq;
-                X.gq = gq;
-                X.c1 = -0.75f * d1;
-                X.d1x3 = 3.0f * d1;
-#pragma unroll
-                for (int b = 0; b < NR; ++b) {
-                    X.w[b] = wx[b];
-                    X.dw[b] = dwx[b];
-                }
-                X.jx = jx;
-                X.qa = qa;
                 const float4 *yrow_x = yrow + tx * RQ * 32; // rows at the x entry's type
+                const float2 M1 = make_float2(-1.0f, -1.0f);
                 int nv = 0;
-                for (int s = s0; s < s1; s += ATMB_VPI) {
-                    // ATMB_VPI independent visits per iteration (steps s .. s + ATMB_VPI - 1) for ILP
-                    int kq[ATMB_VPI];
-                    float4 yq[ATMB_VPI];
-                    float d3q[ATMB_VPI];
-                    bool aq[ATMB_VPI];
+                for (int s = s0; s < s1; s += 4) {
+                    // four independent visits per iteration (steps s .. s + 3) as two packed pairs
+                    int kp[2];
+                    float4 P0q[2], P1q[2];
+                    float2 d3p[2];
+                    bool a0q[2], a1q[2];
                     bool any = false;
 #pragma unroll
-                    for (int q = 0; q < ATMB_VPI; ++q) {
-                        kq[q] = (lane + s + q) & 31;
-                        yq[q] = yA[kq[q]];
-                        const float rx = vx - yq[q].x, ry = vy - yq[q].y, rz = vz - yq[q].z;
-                        d3q[q] = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-                        aq[q] = xvalid && (!diag || s + q < 16 || lane < 16) && d3q[q] <= ratm2f && d3q[q] >= 1e-12f;
-                        any |= aq[q];
-                        nv += aq[q] ? 2 : 0;
+                    for (int pq = 0; pq < 2; ++pq) {
+                        kp[pq] = (lane + s + 2 * pq) & 31;
+                        P0q[pq] = yP0[kp[pq]];
+                        P1q[pq] = yP1[kp[pq]];
+                        const float2 rx = __ffma2_rn(make_float2(P0q[pq].x, P0q[pq].y), M1, X.vx);
+                        const float2 ry = __ffma2_rn(make_float2(P0q[pq].z, P0q[pq].w), M1, X.vy);
+                        const float2 rz = __ffma2_rn(make_float2(P1q[pq].x, P1q[pq].y), M1, X.vz);
+                        d3p[pq] = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+                        const int st = s + 2 * pq;
+                        a0q[pq] = xvalid && (!diag || st < 16 || lane < 16) && d3p[pq].x <= ratm2f && d3p[pq].x >= 1e-12f;
+                        a1q[pq] = xvalid && (!diag || st + 1 < 16 || lane < 16) && d3p[pq].y <= ratm2f && d3p[pq].y >= 1e-12f;
+                        any |= a0q[pq] | a1q[pq];
+                        nv += (a0q[pq] ? 2 : 0) + (a1q[pq] ? 2 : 0);
                     }
                     if (__any_sync(0xffffffffu, any)) {
                         if (simple) {
 #pragma unroll
-                            for (int q = 0; q < ATMB_VPI; ++q)
-                                atmb_visit<NR, true>(X, kq[q], yq[q], d3q[q], aq[q], yB, yrow_x, a, third,
-                                                     force_scaled, xt, ys[q], apx);
+                            for (int pq = 0; pq < 2; ++pq)
+                                atmb_visit2<NR, true>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0, yQ1,
+                                                      yrow_x, a, third, force_scaled, xt, ys[pq], apx);
                         } else {
 #pragma unroll
-                            for (int q = 0; q < ATMB_VPI; ++q)
-                                atmb_visit<NR, false>(X, kq[q], yq[q], d3q[q], aq[q], yB, yrow_x, a, third,
-                                                      force_scaled, xt, ys[q], apx);
+                            for (int pq = 0; pq < 2; ++pq)
+                                atmb_visit2<NR, false>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0, yQ1,
+                                                       yrow_x, a, third, force_scaled, xt, ys[pq], apx);
                         }
                     }
-                    const int src = (lane + ATMB_VPI) & 31;
-#pragma unroll
-                    for (int q = 0; q < ATMB_VPI; ++q) ys[q].shift(src);
+                    const int src = (lane + 4) & 31;
+                    ys[0].shift(src);
+                    ys[1].shift(src);
                 }
                 visits += (unsigned long long)nv;
-                // lane L now holds in ys[q] the complete sums of y entry B[(L + s1 + q) mod 32]
-                // from the visits of step parity q: gather the entry B[(L + s1) mod 32] in ys[0]
-#pragma unroll
-                for (int q = 1; q < ATMB_VPI; ++q) ys[0].add_from(ys[q], (lane - q) & 31);
+                // lane L now holds the complete sums of y entry B[(L + s1 + q) mod 32] from the
+                // visits of steps = q (mod 4) (q = 0, 1 in ys[0].x, .y; 2, 3 in ys[1].x, .y):
+                // gather the entry B[(L + s1) mod 32]
+                AtmbSide yg = ys[0].part(0);
+                yg.add_from(ys[0].part(1), (lane - 1) & 31);
+                yg.add_from(ys[1].part(0), (lane - 2) & 31);
+                yg.add_from(ys[1].part(1), (lane - 3) & 31);
                 {
                     const int ey = (lane + s1) & 31;
-                    ys[0].flush(acc, B * 32 + ey, m);
+                    yg.flush(acc, B * 32 + ey, m);
                     // apex force of the a-y sides (padding partners carry zero sums)
                     const float4 vyv = yA[ey];
-                    apx[0] -= (double)(ys[0].SA * vyv.x);
-                    apx[1] -= (double)(ys[0].SA * vyv.y);
-                    apx[2] -= (double)(ys[0].SA * vyv.z);
+                    apx[0] -= (double)(yg.SA * vyv.x);
+                    apx[1] -= (double)(yg.SA * vyv.y);
+                    apx[2] -= (double)(yg.SA * vyv.z);
                 }
-                const float tSE = xt.SE, tSD = xt.SD, tSF = xt.SA + xt.S3, tWx = xt.Wx, tWy = xt.Wy, tWz = xt.Wz, tSA = xt.SA;
-                const float tUx = simple ? xt.Wx : xt.Ux, tUy = simple ? xt.Wy : xt.Uy, tUz = simple ? xt.Wz : xt.Uz;
-                xs[0] += tSE;
-                xs[1] += tSD;
-                xs[2] += tSF;
+                const float tSA = xt.SA.x + xt.SA.y, tS3 = xt.S3.x + xt.S3.y;
+                const float tWx = xt.Wx.x + xt.Wx.y, tWy = xt.Wy.x + xt.Wy.y, tWz = xt.Wz.x + xt.Wz.y;
+                xs[0] += xt.SE.x + xt.SE.y;
+                xs[1] += xt.SD.x + xt.SD.y;
+                xs[2] += tSA + tS3;
                 xs[3] += tWx;
                 xs[4] += tWy;
                 xs[5] += tWz;
                 xs[6] += tSA;
-                xs[7] += tUx;
-                xs[8] += tUy;
-                xs[9] += tUz;
+                if (simple) { // U = W
+                    xs[7] += tWx;
+                    xs[8] += tWy;
+                    xs[9] += tWz;
+                } else { // xt.U holds -U
+                    xs[7] -= xt.Ux.x + xt.Ux.y;
+                    xs[8] -= xt.Uy.x + xt.Uy.y;
+                    xs[9] -= xt.Uz.x + xt.Uz.y;
+                }
                 B = Bn;
                 cur ^= 1;
             }

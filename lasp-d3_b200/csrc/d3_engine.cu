@@ -1602,14 +1602,22 @@ void engine_fetch_results(Engine *e, double *energies, double *forces, double *s
 // warps per CTA of the block-pair ATM kernel for this handle, 0 when it is not used
 // (plain form, surrogate, mirror schedule chosen, or the type count leaves too little
 // shared memory)
-static int blockpair_warps(const Engine *e) {
-    if (!e->use_atm || !e->opt.precision || e->opt.atm_schedule != 0) return 0;
-    if (e->opt.atm_surrogate && e->surr.loaded) return 0;
-    const size_t limit = 227 * 1024 - 1024; // opt-in maximum minus the static arrays
+struct AtmbShape {
+    int warps, ctas; // warps per CTA (0: kernel not used), CTAs per SM
+};
+static AtmbShape blockpair_shape(const Engine *e) {
+    if (!e->use_atm || !e->opt.precision || e->opt.atm_schedule != 0) return {0, 0};
+    if (e->opt.atm_surrogate && e->surr.loaded) return {0, 0};
     const size_t fixed = atmb_smem_fixed(e->ne, e->nref), per = atmb_smem_warp(e->ne, e->nref);
-    if (fixed + 2 * per > limit) return 0;
-    return (int)std::min<size_t>(ATMB_MAXW, (limit - fixed) / per);
+    // two CTAs of four warps per SM, so that one CTA's per-apex sort and set-up overlap the
+    // other's block pairs, when both fit the SM's 228 KB (each with 2 KB for the static
+    // arrays and the system's share); else one CTA of up to ATMB_MAXW warps
+    if (ATMB_CTAS_PER_SM == 2 && 2 * (fixed + 4 * per + 2048) <= 228 * 1024) return {4, 2};
+    const size_t limit = 227 * 1024 - 1024; // opt-in maximum minus the static arrays
+    if (fixed + 2 * per > limit) return {0, 0};
+    return {(int)std::min<size_t>(ATMB_MAXW, (limit - fixed) / per), 1};
 }
+static int blockpair_warps(const Engine *e) { return blockpair_shape(e).warps; }
 
 static KP make_kp(Engine *e) {
     KP p;
@@ -1658,7 +1666,7 @@ static KP make_kp(Engine *e) {
     p.atm_min_m = 0;
     if (blockpair_warps(e) > 0) {
         e->YD32.ensure((size_t)e->max_atoms * e->ne * atmb_row_floats(e->nref));
-        e->atmb_scratch.ensure((size_t)e->dev_sms * ATMB_SCRATCH_PER_CTA);
+        e->atmb_scratch.ensure((size_t)e->dev_sms * blockpair_shape(e).ctas * ATMB_SCRATCH_PER_CTA);
         p.YD32 = e->YD32.p;
     }
     p.atm_force_scaled = e->opt.atm_force_scaled ? 1 : 0;
@@ -1835,12 +1843,13 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
                 const int tmax = (int)std::max<size_t>(32, std::min<size_t>(256, (100 * 1024 - fixed) / per)) & ~31;
                 const int tile = e->opt.atm_tile > 0 ? std::min(tmax, std::max(32, e->opt.atm_tile & ~31)) : std::min(tmax, 128);
                 const size_t sm = (size_t)tile * per + fixed;
-                const int nwb = blockpair_warps(e);
+                const AtmbShape shb = blockpair_shape(e);
+                const int nwb = shb.warps;
                 if (nwb > 0 && !surr) {
                     // lists up to ATMB_MCAP entries: block-pair schedule; longer ones below
                     const size_t smb = atmb_smem_fixed(p.ne, NR) + (size_t)nwb * atmb_smem_warp(p.ne, NR);
                     atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR>);
-                    k_atm32b<NR><<<e->dev_sms, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
+                    k_atm32b<NR><<<e->dev_sms * shb.ctas, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
                     D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
                     pc.atm_min_m = ATMB_MCAP;
                 }
