@@ -11,24 +11,33 @@
 //     at step s it pairs with y = B[(L + s) mod 32], so no two lanes of the warp touch the
 //     same y in a step. Diagonal blocks take steps 1..16 (step 16 on lanes 0..15 only), so
 //     every unordered pair of entries is visited exactly once.
-//  3. x-side sums stay in the lane's registers for the whole row; y-side sums travel with
-//     their y: a lane takes two steps per iteration (two independent visits, for ILP) and
-//     then passes both sets of y sums two lanes down (six shuffles per step), so after the
-//     last step lane L holds the complete sums of two y's and adds them to those entries'
-//     accumulators in shared memory (one atomic per quantity per block pair).
+//  3. The y block (positions, per-entry constants, and for every partner type the entry's
+//     C6 row, derivative row and r0^2, from the YD32 table) is copied to shared memory by
+//     cp.async while the previous block pair is visited (two buffers per warp). A lane takes
+//     four steps per iteration as two packed f32x2 pairs (steps s, s+1 and s+2, s+3: their
+//     partners sit side by side in one 16-byte slot), so every FP32 add / mul / fma of the
+//     triplet term serves two visits. x-side sums stay in the lane's registers for the whole
+//     row; y-side sums travel with their y (shifted four lanes down per iteration), so after
+//     the last step the four sets in lane L belong to four consecutive y's and are gathered
+//     by three shuffles into one entry's sums, added to that entry's accumulators (L2
+//     atomics on this CTA's global slot, one per quantity per block pair).
 //  4. Per entry e at the end: energy share SE/3, dE/dCN 0.5 (lam_ea SE + SD), force
 //     SF v_e - W (FP64 atomics to the entry atom, as k_atm32); the apex gets SE/6,
-//     0.5 lam_ae SE, the force -sum (wf f_e) v_e and the virial sum SF v_e (x) v_e minus the
+//     0.5 lam_ae SE, the force -sum SA_e v_e and the virial sum SF v_e (x) v_e minus the
 //     cross terms (accumulated by the x lanes) plus the w != wf corrections.
 // With f1, f2, f3 the force scalars of sides a-x, a-y, x-y of a triplet (mirror symmetry of
 // k_atm: f2 of visit (x, y) is f1 of the mirrored visit), the quantities per entry are
-//   SE = sum w E, SD = sum w E lam_{e,other}, SF = sum wf (f_e + f3), W = sum wf f3 v_other.
-// C6_xy = Y_x[t_y] . w_y, dC6_xy/dCN_x = D_x[t_y] . w_y, dC6_xy/dCN_y = Y_x[t_y] . dw_y with
-// the x entry's rows Y, D (all types) staged in shared memory once per row.
-// Profile of the one-visit-per-step version on the 2,000-atom box (ncu): issue active 54 %,
-// 21 of 32 lanes active per instruction, stalls dominated by fixed-latency dependencies and
-// shared-memory/MUFU scoreboards with one 8-warp CTA per SM, and 3.5e9 shared bank conflicts
-// from type-dependent row offsets; hence two visits per iteration and the transposed rows.
+//   SE = sum w E, SD = sum w E lam_{e,other}, SA = sum wf f_apex-side, S3 = sum wf f3,
+//   SF = SA + S3, W = sum wf f3 v_other.
+// C6_xy = Y_y[t_x] . w_x, dC6_xy/dCN_x = Y_y[t_x] . dw_x, dC6_xy/dCN_y = D_y[t_x] . w_x
+// with the x entry's own weights in registers and the y entry's rows at the x type read
+// from the staged block (the reverse factorisation halves the shared-memory bytes per
+// visit against staging the x rows for every partner type).
+// Profiles on the 10,000-atom box (ncu, one launch): shared-memory data pipe 85 % of peak
+// with the x rows staged per type -> 49 % with the y rows; long-scoreboard stalls of the
+// synchronous y gather removed by the cp.async double buffer; warp instructions -22 % with
+// the packed pairs, which leaves the kernel bound by the latency of the packed chains
+// (2 warps of 243 registers per scheduler, four independent chains).
 
 constexpr int ATMB_MCAP = 4096;   // longest list this kernel takes (longer lists: k_atm32)
 constexpr int ATMB_GRID = 8;      // spatial grid per dimension for the entry sort
