@@ -39,20 +39,22 @@
 // the packed pairs, which leaves the kernel bound by the latency of the packed chains
 // (2 warps of 243 registers per scheduler, four independent chains).
 
-constexpr int ATMB_MCAP = 4096;   // longest list this kernel takes (longer lists: k_atm32)
+// longest list this kernel takes (longer lists: k_atm32): chosen per launch, a multiple of
+// 512 in [ATMB_MCAP_MIN, ATMB_MCAP_MAX], as large as the shared memory left by the warps allows
+constexpr int ATMB_MCAP_MIN = 4096, ATMB_MCAP_MAX = 8192;
 constexpr int ATMB_GRID = 8;      // spatial grid per dimension for the entry sort
 constexpr int ATMB_MAXW = 8;      // warps per CTA at most
 constexpr int ATMB_CTAS_PER_SM = 2; // preferred CTAs per SM (of four warps each)
 constexpr int ATMB_VPI = 4;       // visits per lane per iteration (independent, for ILP)
 
 // global scratch per CTA (float4 units): per-entry records sA, sB, sJ and the per-entry
-// accumulators [6][MCAP] floats
-constexpr size_t ATMB_SCRATCH_PER_CTA = 3 * ATMB_MCAP + (6 * ATMB_MCAP + 3) / 4;
+// accumulators [6][mcap] floats
+__host__ __device__ inline size_t atmb_scratch_per_cta(int mcap) { return 3 * (size_t)mcap + (6 * (size_t)mcap + 3) / 4; }
 
 // shared memory: fixed part + per-warp staging
-__host__ __device__ inline size_t atmb_smem_fixed(int ne, int NR) {
-    size_t b = ATMB_MCAP * sizeof(int);                       // atom of each sorted entry
-    b += 2 * (ATMB_MCAP / 32) * sizeof(float4);               // block bounding boxes
+__host__ __device__ inline size_t atmb_smem_fixed(int ne, int NR, int mcap) {
+    size_t b = (size_t)mcap * sizeof(int);                    // atom of each sorted entry
+    b += 2 * (size_t)(mcap / 32) * sizeof(float4);            // block bounding boxes
     b += 512 * sizeof(int);                                   // sort cells
     b += (size_t)((ne * ne + 3) & ~3) * sizeof(float);        // r0^2
     b += (size_t)((ne * NR + 1) & ~1) * sizeof(double);       // apex C6 rows
@@ -202,14 +204,14 @@ struct AtmbSide {
         Wy += __shfl_sync(0xffffffffu, o.Wy, src);
         Wz += __shfl_sync(0xffffffffu, o.Wz, src);
     }
-    __device__ __forceinline__ void flush(float *acc, int e, int m) {
+    __device__ __forceinline__ void flush(float *acc, int mcap, int e, int m) {
         if (e < m && (SE != 0.f || SA != 0.f || S3 != 0.f || SD != 0.f)) {
-            atomicAdd(&acc[0 * ATMB_MCAP + e], SE);
-            atomicAdd(&acc[1 * ATMB_MCAP + e], SD);
-            atomicAdd(&acc[2 * ATMB_MCAP + e], SA + S3);
-            atomicAdd(&acc[3 * ATMB_MCAP + e], Wx);
-            atomicAdd(&acc[4 * ATMB_MCAP + e], Wy);
-            atomicAdd(&acc[5 * ATMB_MCAP + e], Wz);
+            atomicAdd(&acc[0 * mcap + e], SE);
+            atomicAdd(&acc[1 * mcap + e], SD);
+            atomicAdd(&acc[2 * mcap + e], SA + S3);
+            atomicAdd(&acc[3 * mcap + e], Wx);
+            atomicAdd(&acc[4 * mcap + e], Wy);
+            atomicAdd(&acc[5 * mcap + e], Wz);
         }
     }
 };
@@ -368,23 +370,24 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
     const int ne = p.ne;
     const int nw = blockDim.x >> 5;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int *sjy = reinterpret_cast<int *>(smb);                             // [MCAP] atom of each sorted entry
-    float4 *bblo = reinterpret_cast<float4 *>(sjy + ATMB_MCAP);          // [MCAP/32]
-    float4 *bbhi = bblo + ATMB_MCAP / 32;
-    int *cellpos = reinterpret_cast<int *>(bbhi + ATMB_MCAP / 32);       // [512]
+    const int mcap = p.atmb_mcap;
+    int *sjy = reinterpret_cast<int *>(smb);                             // [mcap] atom of each sorted entry
+    float4 *bblo = reinterpret_cast<float4 *>(sjy + mcap);               // [mcap/32]
+    float4 *bbhi = bblo + mcap / 32;
+    int *cellpos = reinterpret_cast<int *>(bbhi + mcap / 32);            // [512]
     float *r0sq = reinterpret_cast<float *>(cellpos + 512);              // [ne][ne]
     double *yapex = reinterpret_cast<double *>(r0sq + ((ne * ne + 3) & ~3)); // [ne][NR]
-    unsigned char *wbase = smb + atmb_smem_fixed(ne, NR) + (size_t)warp * atmb_smem_warp(ne, NR);
+    unsigned char *wbase = smb + atmb_smem_fixed(ne, NR, mcap) + (size_t)warp * atmb_smem_warp(ne, NR);
     constexpr int RQ = atmb_row_floats(NR) / 4;                          // float4 quads per row
     // buffer layout: [ne][RQ][32] rows of the y block, [32] vx vy vz d2, [32] ir id2 s g
     float4 *ybuf0 = reinterpret_cast<float4 *>(wbase);
     const size_t bufq = atmb_buf_quads(ne, NR);
     __shared__ int s_item;
     __shared__ double red[ATMB_MAXW][12];
-    float4 *sA = scratch + (size_t)blockIdx.x * ATMB_SCRATCH_PER_CTA;    // vx vy vz d2
-    float4 *sB = sA + ATMB_MCAP;                                         // ir id2 s g
-    float4 *sJ = sB + ATMB_MCAP;                                         // j t lam_ea lam_ae
-    float *acc = reinterpret_cast<float *>(sJ + ATMB_MCAP);              // [6][MCAP] (global, L2-resident)
+    float4 *sA = scratch + (size_t)blockIdx.x * atmb_scratch_per_cta(mcap); // vx vy vz d2
+    float4 *sB = sA + mcap;                                              // ir id2 s g
+    float4 *sJ = sB + mcap;                                              // j t lam_ea lam_ae
+    float *acc = reinterpret_cast<float *>(sJ + mcap);                   // [6][mcap] (global, L2-resident)
     if (p.atm_off[p.n] > p.atm_cap) return; // list overflowed: the host grows it and re-runs
     for (int k = tid; k < ne * ne; k += blockDim.x) r0sq[k] = (float)(p.r0ab[k] * p.r0ab[k]);
     static_assert(NR == 5 || NR == 7, "reference counts of the parameter tables");
@@ -404,7 +407,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         const int a = p.sorted_of[p.n - 1 - item];
         const long long e0 = p.atm_off[a];
         const int m = (int)(p.atm_off[a + 1] - e0);
-        if (m > ATMB_MCAP) continue; // long lists: k_atm32
+        if (m > mcap) continue; // long lists: k_atm32
         const double4 xa = p.xs[a];
         const int ta = (int)xa.w;
         const SG &g = p.sg[p.sid[a]];
@@ -412,7 +415,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
         for (int k = tid; k < 512; k += blockDim.x) cellpos[k] = 0;
         for (int q = 0; q < 6; ++q)
-            for (int e = tid; e < m; e += blockDim.x) __stcg(&acc[q * ATMB_MCAP + e], 0.f);
+            for (int e = tid; e < m; e += blockDim.x) __stcg(&acc[q * mcap + e], 0.f);
         double dwa[NR];
 #pragma unroll
         for (int b = 0; b < NR; ++b) dwa[b] = p.dw[(size_t)a * NR + b];
@@ -683,7 +686,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
                 yg.add_from(ys[1].part(1), (lane - 3) & 31);
                 {
                     const int ey = (lane + s1) & 31;
-                    yg.flush(acc, B * 32 + ey, m);
+                    yg.flush(acc, mcap, B * 32 + ey, m);
                     // apex force of the a-y sides (padding partners carry zero sums)
                     const float4 vyv = yA[ey];
                     apx[0] -= (double)(yg.SA * vyv.x);
@@ -713,12 +716,12 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
             }
             atmb_cp_wait<0>();
             if (xvalid) {
-                atomicAdd(&acc[0 * ATMB_MCAP + xe], (float)xs[0]);
-                atomicAdd(&acc[1 * ATMB_MCAP + xe], (float)xs[1]);
-                atomicAdd(&acc[2 * ATMB_MCAP + xe], (float)xs[2]);
-                atomicAdd(&acc[3 * ATMB_MCAP + xe], (float)xs[3]);
-                atomicAdd(&acc[4 * ATMB_MCAP + xe], (float)xs[4]);
-                atomicAdd(&acc[5 * ATMB_MCAP + xe], (float)xs[5]);
+                atomicAdd(&acc[0 * mcap + xe], (float)xs[0]);
+                atomicAdd(&acc[1 * mcap + xe], (float)xs[1]);
+                atomicAdd(&acc[2 * mcap + xe], (float)xs[2]);
+                atomicAdd(&acc[3 * mcap + xe], (float)xs[3]);
+                atomicAdd(&acc[4 * mcap + xe], (float)xs[4]);
+                atomicAdd(&acc[5 * mcap + xe], (float)xs[5]);
                 // apex force of the a-x sides and the x-y cross terms of the virial
                 apx[0] -= xs[6] * vx;
                 apx[1] -= xs[6] * vy;
@@ -737,9 +740,9 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         double ea = 0, ga = 0;
         for (int e = tid; e < m; e += blockDim.x) {
             // accumulated at L2 by atomics: read past L1
-            const double SE = __ldcg(&acc[e]), SD = __ldcg(&acc[ATMB_MCAP + e]), SF = __ldcg(&acc[2 * ATMB_MCAP + e]);
-            const double Wx = __ldcg(&acc[3 * ATMB_MCAP + e]), Wy = __ldcg(&acc[4 * ATMB_MCAP + e]);
-            const double Wz = __ldcg(&acc[5 * ATMB_MCAP + e]);
+            const double SE = __ldcg(&acc[e]), SD = __ldcg(&acc[mcap + e]), SF = __ldcg(&acc[2 * mcap + e]);
+            const double Wx = __ldcg(&acc[3 * mcap + e]), Wy = __ldcg(&acc[4 * mcap + e]);
+            const double Wz = __ldcg(&acc[5 * mcap + e]);
             const float4 qa4 = sA[e], qj4 = sJ[e];
             const int j = __float_as_int(qj4.x);
             const double lam_ea = qj4.z, lam_ae = qj4.w;

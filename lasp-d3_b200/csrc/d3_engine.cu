@@ -123,6 +123,7 @@ struct KP {
     float *YD32;    // [n][ne][2 NR + 2] (block-pair ATM): per partner type the C6 row, r0^2 of
                     // the type pair, the row of the weight derivatives, the atom index bits
     int atm_min_m;  // k_atm32 takes only apexes with longer lists (the rest: k_atm32b)
+    int atmb_mcap;  // longest list k_atm32b takes
     // sharded evaluation: this process computes the two-body and chain-rule terms of central
     // atoms i = shard_rank + k shard_world (binned order) and the ATM apexes of work items
     // shard_rank + k shard_world; CN and weights for every atom
@@ -1603,19 +1604,26 @@ void engine_fetch_results(Engine *e, double *energies, double *forces, double *s
 // (plain form, surrogate, mirror schedule chosen, or the type count leaves too little
 // shared memory)
 struct AtmbShape {
-    int warps, ctas; // warps per CTA (0: kernel not used), CTAs per SM
+    int warps, ctas, mcap; // warps per CTA (0: kernel not used), CTAs per SM, longest list
 };
 static AtmbShape blockpair_shape(const Engine *e) {
-    if (!e->use_atm || !e->opt.precision || e->opt.atm_schedule != 0) return {0, 0};
-    if (e->opt.atm_surrogate && e->surr.loaded) return {0, 0};
-    const size_t fixed = atmb_smem_fixed(e->ne, e->nref), per = atmb_smem_warp(e->ne, e->nref);
+    if (!e->use_atm || !e->opt.precision || e->opt.atm_schedule != 0) return {0, 0, 0};
+    if (e->opt.atm_surrogate && e->surr.loaded) return {0, 0, 0};
+    const size_t per = atmb_smem_warp(e->ne, e->nref);
     // two CTAs of four warps per SM, so that one CTA's per-apex sort and set-up overlap the
     // other's block pairs, when both fit the SM's 228 KB (each with 2 KB for the static
-    // arrays and the system's share); else one CTA of up to ATMB_MAXW warps
-    if (ATMB_CTAS_PER_SM == 2 && 2 * (fixed + 4 * per + 2048) <= 228 * 1024) return {4, 2};
+    // arrays and the system's share)
+    if (ATMB_CTAS_PER_SM == 2 && 2 * (atmb_smem_fixed(e->ne, e->nref, ATMB_MCAP_MIN) + 4 * per + 2048) <= 228 * 1024)
+        return {4, 2, ATMB_MCAP_MIN};
+    // else one CTA of up to ATMB_MAXW warps; the shared memory they leave sets the list
+    // capacity (longer lists go to the mirror kernel)
     const size_t limit = 227 * 1024 - 1024; // opt-in maximum minus the static arrays
-    if (fixed + 2 * per > limit) return {0, 0};
-    return {(int)std::min<size_t>(ATMB_MAXW, (limit - fixed) / per), 1};
+    for (int w = ATMB_MAXW; w >= 2; --w) {
+        int mcap = ATMB_MCAP_MAX;
+        while (mcap >= ATMB_MCAP_MIN && atmb_smem_fixed(e->ne, e->nref, mcap) + w * per > limit) mcap -= 512;
+        if (mcap >= ATMB_MCAP_MIN) return {w, 1, mcap};
+    }
+    return {0, 0, 0};
 }
 static int blockpair_warps(const Engine *e) { return blockpair_shape(e).warps; }
 
@@ -1666,7 +1674,9 @@ static KP make_kp(Engine *e) {
     p.atm_min_m = 0;
     if (blockpair_warps(e) > 0) {
         e->YD32.ensure((size_t)e->max_atoms * e->ne * atmb_row_floats(e->nref));
-        e->atmb_scratch.ensure((size_t)e->dev_sms * blockpair_shape(e).ctas * ATMB_SCRATCH_PER_CTA);
+        const AtmbShape sh = blockpair_shape(e);
+        e->atmb_scratch.ensure((size_t)e->dev_sms * sh.ctas * atmb_scratch_per_cta(sh.mcap));
+        p.atmb_mcap = sh.mcap;
         p.YD32 = e->YD32.p;
     }
     p.atm_force_scaled = e->opt.atm_force_scaled ? 1 : 0;
@@ -1846,12 +1856,12 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
                 const AtmbShape shb = blockpair_shape(e);
                 const int nwb = shb.warps;
                 if (nwb > 0 && !surr) {
-                    // lists up to ATMB_MCAP entries: block-pair schedule; longer ones below
-                    const size_t smb = atmb_smem_fixed(p.ne, NR) + (size_t)nwb * atmb_smem_warp(p.ne, NR);
+                    // lists up to shb.mcap entries: block-pair schedule; longer ones below
+                    const size_t smb = atmb_smem_fixed(p.ne, NR, shb.mcap) + (size_t)nwb * atmb_smem_warp(p.ne, NR);
                     atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR>);
                     k_atm32b<NR><<<e->dev_sms * shb.ctas, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
                     D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
-                    pc.atm_min_m = ATMB_MCAP;
+                    pc.atm_min_m = shb.mcap;
                 }
                 const void *fn = surr ? (const void *)k_atm32<NR, true> : (const void *)k_atm32<NR, false>;
                 const int blocks_per_sm = atm_occupancy(e, surr ? 3 : 1, sm, fn);
