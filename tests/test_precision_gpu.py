@@ -54,15 +54,37 @@ def test_precision_form_scaled_atm_forces():
     assert np.abs(f - r["forces"]).max() <= 1e-4
 
 
-@pytest.mark.parametrize("case", ["tric", "fe", "water"])
+def _half_list_lengths(sys_, rc_bohr, stride=25):
+    """Half-list lengths (entries j <= a within rc, all images) of every stride-th apex,
+    for cells whose heights exceed rc (images -1..1 suffice)."""
+    pos, cell = sys_["pos"], sys_["cell"]
+    rc = rc_bohr * 0.52917726
+    imgs = np.array([[i, j, k] for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)], float) @ cell
+    out = []
+    for a in range(0, len(pos), stride):
+        v = (pos[: a + 1][None] + imgs[:, None]) - pos[a]
+        d2 = (v * v).sum(-1)
+        out.append(int(((d2 <= rc * rc) & (d2 >= 1e-12)).sum()))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("case", ["tric", "split", "fe", "water"])
 def test_atm_schedules_agree(case):
-    """Block-pair schedule (each triplet once; lists longer than its cap go to the mirror
-    kernel) against the mirror-symmetric schedule (each triplet twice): the same in-range
-    triplets (visit counters equal) and the same energy, forces and stress to FP32 level."""
+    """Block-pair schedule (each triplet once; lists longer than its capacity go to the
+    mirror kernel) against the mirror-symmetric schedule (each triplet twice): the same
+    in-range triplets (visit counters equal) and the same energy, forces and stress to FP32
+    level. "split": rc_ATM 50 bohr in a 3,000-atom box, so that about a sixth of the half
+    lists are longer than the block-pair capacity for five element types (6,656 entries)
+    and one evaluation runs both kernels; its cells are lower than 2 rc_ATM, so atoms
+    repeat within a list (pair weights below 1)."""
     from d3_b200 import OPT_ATM_SCHEDULE
 
     if case == "tric":
         sys_, kw = S.triclinic_box(3000, seed=5), dict(rc=95.0, rc_cn=40.0, rc_atm=40.0)
+    elif case == "split":
+        sys_, kw = S.triclinic_box(3000, seed=5), dict(rc=95.0, rc_cn=40.0, rc_atm=50.0)
+        lens = _half_list_lengths(sys_, 50.0)
+        assert lens.max() > 6656 and lens.min() < 4096
     elif case == "fe":
         sys_ = S.gtest_bcc_fe(True)
         sys_["pos"] = sys_["pos"] + np.random.default_rng(1).uniform(-0.1, 0.1, sys_["pos"].shape)
