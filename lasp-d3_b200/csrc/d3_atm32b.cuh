@@ -45,7 +45,6 @@ constexpr int ATMB_MCAP_MIN = 4096, ATMB_MCAP_MAX = 8192;
 constexpr int ATMB_GRID = 8;      // spatial grid per dimension for the entry sort
 constexpr int ATMB_MAXW = 8;      // warps per CTA at most
 constexpr int ATMB_CTAS_PER_SM = 2; // preferred CTAs per SM (of four warps each)
-constexpr int ATMB_VPI = 4;       // visits per lane per iteration (independent, for ILP)
 
 // global scratch per CTA (float4 units): per-entry records sA, sB, sJ and the per-entry
 // accumulators [6][mcap] floats
@@ -180,20 +179,10 @@ struct AtmbX2 {
     bool qa;
 };
 
-// per-side sums of one block pair: SE = sum w E, SD = sum w E lam, SA = sum wf f_apex-side,
-// S3 = sum wf f3, W = sum wf f3 v_other; the x side also U = sum w f3 v_y
-// (force scalar of the entry SF = SA + S3)
+// y sums of one entry over a block pair: SE = sum w E, SD = sum w E lam, SA = sum wf
+// f_apex-side, S3 = sum wf f3, W = sum wf f3 v_other (force scalar of the entry SF = SA + S3)
 struct AtmbSide {
-    float SE, SD, SA, S3, Wx, Wy, Wz, Ux, Uy, Uz;
-    __device__ __forceinline__ void shift(int src) {
-        SE = __shfl_sync(0xffffffffu, SE, src);
-        SD = __shfl_sync(0xffffffffu, SD, src);
-        SA = __shfl_sync(0xffffffffu, SA, src);
-        S3 = __shfl_sync(0xffffffffu, S3, src);
-        Wx = __shfl_sync(0xffffffffu, Wx, src);
-        Wy = __shfl_sync(0xffffffffu, Wy, src);
-        Wz = __shfl_sync(0xffffffffu, Wz, src);
-    }
+    float SE, SD, SA, S3, Wx, Wy, Wz;
     // add the y sums that lane src holds
     __device__ __forceinline__ void add_from(const AtmbSide &o, int src) {
         SE += __shfl_sync(0xffffffffu, o.SE, src);
