@@ -315,7 +315,7 @@ def engine_arm(args, world, rank, local):
         if os.path.exists(tfile) and args.system == "triclinic" and n == N_ATOMS and table == TABLE_5REF:
             traffic = json.load(open(tfile)).get("atm_fp64_bytes_per_launch" if fp64 else "atm_fp32_bytes_per_launch")
         kernel = ("k_atm (ATM triplets, FP64)" if fp64 else
-                  "k_atm32b + k_atm32 (ATM triplets, FP32 arithmetic; block pairs, lists over 4,096 entries mirrored)")
+                  "k_atm32b + k_atm32 (ATM triplets, FP32 arithmetic; block pairs, packed f32x2 pairs of visits; lists beyond the per-launch block-pair capacity mirrored)")
         algorithmic = "%d in-range triplets x %d FLOP per launch" % (triplets, ATM_FLOP_PER_TRIPLET)
     else:
         achieved = pairs * TWOBODY_FLOP_PER_PAIR / (ch["twobody_ms"] * 1e-3) / 1e12
