@@ -7,7 +7,7 @@
 //     Per-entry set-up (FP64 C6 of the apex pair, its CN derivatives, damping ratio) is
 //     written once per apex, in sorted order, to this CTA's slot of a global scratch array.
 //  2. Block pairs (A, B), B >= A, whose bounding boxes are within rc_ATM of each other are
-//     walked by the warps (rows A in a zigzag over the warps). Lane L owns entry x = A[L];
+//     walked by the warps (rows A taken from a counter, in order). Lane L owns entry x = A[L];
 //     at step s it pairs with y = B[(L + s) mod 32], so no two lanes of the warp touch the
 //     same y in a step. Diagonal blocks take steps 1..16 (step 16 on lanes 0..15 only), so
 //     every unordered pair of entries is visited exactly once.
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
     // buffer layout: [ne][RQ][32] rows of the y block, [32] vx vy vz d2, [32] ir id2 s g
     float4 *ybuf0 = reinterpret_cast<float4 *>(wbase);
     const size_t bufq = atmb_buf_quads(ne, NR);
-    __shared__ int s_item;
+    __shared__ int s_item, s_row;
     __shared__ double red[ATMB_MAXW][12];
     float4 *sA = scratch + (size_t)blockIdx.x * atmb_scratch_per_cta(mcap); // vx vy vz d2
     float4 *sB = sA + mcap;                                              // ir id2 s g
@@ -403,6 +403,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         const bool simple = g.atm_simple != 0;
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
         for (int k = tid; k < 512; k += blockDim.x) cellpos[k] = 0;
+        if (tid == 0) s_row = 0;
         for (int q = 0; q < 6; ++q)
             for (int e = tid; e < m; e += blockDim.x) __stcg(&acc[q * mcap + e], 0.f);
         double dwa[NR];
@@ -503,8 +504,12 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         float4 *yP1 = yP0 + 32, *yQ0 = yP1 + 32, *yQ1 = yQ0 + 32;
 #pragma unroll
         for (int q = 0; q < 9; ++q) apx[q] = 0.0;
-        for (int r = 0;; ++r) {
-            const int A = nw * r + ((r & 1) ? (nw - 1 - warp) : warp);
+        // rows are handed out in order (row A holds nb - A block pairs, so the dearest go
+        // first and the cheapest close the apex, shortening the wait at its barrier)
+        for (;;) {
+            int A = 0;
+            if (lane == 0) A = atomicAdd(&s_row, 1);
+            A = __shfl_sync(0xffffffffu, A, 0);
             if (A >= nb) break;
             const int xe = A * 32 + lane;
             const bool xvalid = xe < m;
