@@ -1,6 +1,6 @@
 """Engine (FP64 path, through the C ABI) against the FP64 oracle.
 
-Tolerances (north-star bar for the plain method): energy 1e-9 relative, forces
+Tolerances (the accuracy bar of the FP64 plain form): energy 1e-9 relative, forces
 1e-7 eV/A, stress 1e-7 eV/A^3, on the same seeded inputs. Cases follow the reference's
 own test systems (test/d3_test.cpp:343-417), the 96-atom water box and small
 triclinic boxes of the benchmark generator, both damping types, both table layouts,

@@ -1,6 +1,6 @@
 """Precision form (FP32 pair/triplet arithmetic, FP64 weights, dE/dCN and reductions)
 against the FP64 oracle. Targets of the form: energy within 1e-6 relative, forces within
-1e-4 eV/A, stress within 1e-6 eV/A^3 (the north-star bar for the mixed-precision form)."""
+1e-4 eV/A, stress within 1e-6 eV/A^3 (the accuracy bar of the mixed-precision form)."""
 import numpy as np
 import pytest
 

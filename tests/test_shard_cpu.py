@@ -1,4 +1,4 @@
-"""Sharded evaluation, host side: the driver's two all-reduces over a gloo process group of
+"""Sharded evaluation, host side: ShardedEvaluator's two all-reduces over a gloo process group of
 two ranks on CPU. Each rank's handle is a stand-in whose two stages are known linear maps
 (stage 1 writes a rank-specific part of dE/dCN; stage 2 maps the summed dE/dCN to a
 rank-specific part of the results), so the expected sum is known exactly: the test checks

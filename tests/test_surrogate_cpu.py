@@ -1,6 +1,6 @@
 """Learned ATM surrogate, host side: parameter layout shared by the library, the model
 file and the CPU checker; model file round trip; the CPU checker's own derivatives
-against finite differences (so that it can judge the kernels' gradients)."""
+against finite differences (so that it can check the kernels' gradients)."""
 import os
 
 import numpy as np
