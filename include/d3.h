@@ -195,9 +195,16 @@ double d3_peak_probe(int fp64);
    larger sizes are rejected with an error (return 1, see d3_last_error). The only
    scratch is a fixed array in device memory shared by all calls on a device (held until
    the process exits): calls that overlap on the GPU race on it. The first call on each
-   device does a one-time set-up and should come before any stream capture. Returns 0
-   on success. Atoms whose element is outside the table get CN = NaN. */
+   device does a one-time set-up and should come before any stream capture; that set-up
+   does not survive cudaDeviceReset. Returns 0 on success. Atoms whose element is outside
+   the table get CN = NaN and contribute nothing to the others. Every image within the
+   cutoff of the positions wrapped into the cell is used (the handle API follows the
+   reference's image box over the positions as given; both agree for atoms given inside
+   the cell); the smooth-cutoff CN option has no counterpart here. The work is bounded
+   before launch: cells so thin that more than D3_NOALLOC_MAX_IMAGES images, or more than
+   2^36 pair-image tests, would be needed are rejected with an error. */
 #define D3_NOALLOC_MAX_ATOMS 8192
+#define D3_NOALLOC_MAX_IMAGES 4096
 int d3_coordination_numbers_noalloc(const double *coords, const uint16_t *elements, uint64_t num_atoms,
                                     const double cell[9], double cn_cutoff, int table, double *cn,
                                     void *cuda_stream);
@@ -270,6 +277,8 @@ int d3_mlp_adam(int n_channels, int members, float *params_dev, uint16_t *packed
    dE/dCN chain rule for this rank's share and writes this rank's part of the results
    (energies [S], forces [n][3], stresses [S][9], double, eV units, the layout of
    d3_device_results) to results_dev; the sum of results_dev over the ranks is the result.
+   results_dev must hold 10 S + 3 n doubles, S = d3_num_structures(handle) and
+   n = d3_shard_length(handle): d3_shard_end writes that many whatever the buffer's size.
    d3_shard_begin synchronises cuda_stream (it checks the neighbour-list capacity); the
    learned surrogate is not available here. Returns the status word. */
 uint64_t d3_shard_length(d3_handle_t *handle);

@@ -16,7 +16,13 @@
 //   * every call shares the one scratch array of the device, which keeps the previous
 //     call's contents; calls whose work overlaps on the GPU (different streams, or
 //     different host threads) race on it and must be serialised by the caller;
-//   * the device holds the scratch array (256 KiB) until the process exits.
+//   * the device holds the scratch array (256 KiB) until the process exits;
+//   * the set-up is cached per device and does not survive cudaDeviceReset: after a reset
+//     in the same process this entry point must not be called again;
+//   * images: every periodic image within the cutoff of the WRAPPED positions is used.
+//     The handle API instead reproduces the reference's image box over the positions as
+//     given (unwrapped); the two agree when the atoms are given inside the cell, and can
+//     differ for atoms given outside it. The smooth-cutoff CN option has no counterpart.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -76,6 +82,7 @@ __global__ void k_noalloc_cn(int n, NoallocGeom g, const double *scratch, double
     double acc = 0.0;
     for (int j = 0; j < n; ++j) {
         const double *xj = scratch + 4 * (size_t)j;
+        if (!(xj[3] > 0.0)) continue; // an atom outside the table contributes nothing
         const double rsum = xi[3] + xj[3];
         for (int tz = -g.half[2]; tz <= g.half[2]; ++tz)
             for (int ty = -g.half[1]; ty <= g.half[1]; ++ty)
@@ -144,12 +151,6 @@ extern "C" int d3_coordination_numbers_noalloc(const double *coords, const uint1
                     std::to_string(D3_NOALLOC_MAX_ATOMS) + "; use the handle API for larger systems");
     if (table != D3_TABLE_5REF && table != D3_TABLE_7REF) return fail("d3_coordination_numbers_noalloc: unknown table");
     if (!(cn_cutoff > 0.0) || !std::isfinite(cn_cutoff)) return fail("d3_coordination_numbers_noalloc: bad cutoff");
-    int dev = 0;
-    cudaError_t err = cudaGetDevice(&dev);
-    if (err != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
-        return fail(std::string("d3_coordination_numbers_noalloc: no usable device: ") + cudaGetErrorString(err));
-    double *scratch = nullptr;
-    if (setup_device(dev, &scratch)) return 1;
     double hb[9];
     for (int k = 0; k < 9; ++k) {
         if (!std::isfinite(cell[k])) return fail("d3_coordination_numbers_noalloc: non-finite cell");
@@ -163,13 +164,34 @@ extern "C" int d3_coordination_numbers_noalloc(const double *coords, const uint1
         g.inv[k] = geom.inv[k];
     }
     // wrapped atoms lie inside the cell, so images up to floor(rc / height) + 1 cells
-    // away cover every pair within the cutoff
+    // away cover every pair within the cutoff. The kernel visits every image of every
+    // pair, so the work is bounded before launch: at most D3_NOALLOC_MAX_IMAGES images
+    // and n^2 x images <= 2^36 pair-image tests (about a second on one GPU)
+    double images = 1.0;
     for (int k = 0; k < 3; ++k) {
         const double reach = std::floor(cn_cutoff / geom.height[k]) + 1.0;
-        if (reach > 64.0) return fail("d3_coordination_numbers_noalloc: cell too thin for the cutoff");
+        if (!(reach <= 64.0)) return fail("d3_coordination_numbers_noalloc: cell too thin for the cutoff");
         g.half[k] = (int)reach;
+        images *= 2.0 * reach + 1.0;
     }
+    if (images > (double)D3_NOALLOC_MAX_IMAGES || (double)num_atoms * (double)num_atoms * images > 68719476736.0)
+        return fail("d3_coordination_numbers_noalloc: " + std::to_string((long long)images) + " periodic images for " +
+                    std::to_string(num_atoms) + " atoms exceed the work bound of this entry point (at most " +
+                    std::to_string(D3_NOALLOC_MAX_IMAGES) +
+                    " images and 2^36 pair-image tests); use the handle API, whose cell list scales");
     g.rcn2 = cn_cutoff * cn_cutoff;
+    // arguments are valid: only now touch the device
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
+        return fail(std::string("d3_coordination_numbers_noalloc: no usable device: ") + cudaGetErrorString(err));
+    double *scratch = nullptr;
+    if (setup_device(dev, &scratch)) return 1;
+    // an error left by earlier work of this thread would otherwise be reported as ours
+    err = cudaGetLastError();
+    if (err != cudaSuccess)
+        return fail(std::string("d3_coordination_numbers_noalloc: CUDA error pending from earlier work: ") +
+                    cudaGetErrorString(err));
     cudaStream_t s = (cudaStream_t)cuda_stream;
     const int n = (int)num_atoms, T = 128, blocks = (n + T - 1) / T;
     k_noalloc_wrap<<<blocks, T, 0, s>>>(coords, elements, n, g, table, scratch);

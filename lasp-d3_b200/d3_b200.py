@@ -203,6 +203,10 @@ class _Shard:
     def shard_length(self):
         return int(self.lib.d3_shard_length(self.h))
 
+    def shard_structures(self):
+        """Structures of this handle: d3_shard_end writes 10 S + 3 n result values."""
+        return int(self.lib.d3_num_structures(self.h))
+
     def shard_begin(self, rank, world, dedcn_ptr, stream_ptr=None):
         st = int(self.lib.d3_shard_begin(self.h, int(rank), int(world), ctypes.c_void_p(dedcn_ptr),
                                          ctypes.c_void_p(stream_ptr) if stream_ptr else None))

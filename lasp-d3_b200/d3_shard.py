@@ -15,10 +15,15 @@ every rank instead of all-gathering it.
     energy, forces, stress = ShardedEvaluator(d3).compute()
 """
 class ShardedEvaluator:
-    """Drives the two stages of a handle (anything with shard_length, shard_begin and
-    shard_end) and the two all-reduces between and after them."""
+    """Drives the two stages of a handle (anything with shard_length, shard_structures,
+    shard_begin and shard_end) and the two all-reduces between and after them.
 
-    def __init__(self, handle, group=None, num_structures=1, device=None):
+    The results buffer holds 10 S + 3 n doubles, S the structures of the handle (one for a
+    D3 handle, the batch size for a D3Batch); S is taken from the handle, since
+    d3_shard_end writes that many values whatever buffer it is given. `num_structures`,
+    when given, must agree with it."""
+
+    def __init__(self, handle, group=None, num_structures=None, device=None):
         import torch
         import torch.distributed as dist
 
@@ -28,7 +33,9 @@ class ShardedEvaluator:
         self.rank = dist.get_rank(group)
         self.world = dist.get_world_size(group)
         self.n = int(handle.shard_length())
-        self.S = int(num_structures)
+        self.S = int(handle.shard_structures())
+        if num_structures is not None and int(num_structures) != self.S:
+            raise ValueError("num_structures=%d but the handle holds %d structures" % (num_structures, self.S))
         if device is None:
             device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else "cpu"
         self.G = torch.zeros(self.n, dtype=torch.float64, device=device)

@@ -65,3 +65,20 @@ def test_cffi_binding_declares_reference_api():
     for s in REFERENCE_ABI[:2] + ["init_d3_handle_with_atm", "set_atoms", "set_cell",
                                   "compute_dispersion_energy_from_handle_status"]:
         assert hasattr(d3_cffi.lib, s)
+
+
+def test_noalloc_entry_point_rejects_work_beyond_its_bound_before_any_launch():
+    # a 2 A cell with a 40 bohr cutoff needs 23^3 images: rejected by the argument checks,
+    # which run before the entry point touches a device (so this runs without a GPU)
+    lib = d3_b200.load_library()
+    f = lib.d3_coordination_numbers_noalloc
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+                  ctypes.c_void_p, ctypes.c_void_p]
+    dummy = (ctypes.c_double * 1)()
+    cell = (ctypes.c_double * 9)(2.0, 0, 0, 0, 2.0, 0, 0, 0, 2.0)
+    assert f(dummy, dummy, 10, cell, 40.0, 0, dummy, None) == 1
+    assert b"work bound" in lib.d3_last_error()
+    cell_ok = (ctypes.c_double * 9)(20.0, 0, 0, 0, 20.0, 0, 0, 0, 20.0)
+    assert f(dummy, dummy, 9000, cell_ok, 40.0, 0, dummy, None) == 1
+    assert b"exceed the maximum" in lib.d3_last_error()

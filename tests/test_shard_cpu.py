@@ -11,14 +11,16 @@ import pytest
 
 torch = pytest.importorskip("torch")
 
-N, S = 7, 1
+N = 7
 
 
 class LinearStages:
-    """Stand-in for a D3 handle: stage 1 writes G_r = a_r; stage 2 writes out_r = B_r G + c_r."""
+    """Stand-in for a D3 (S = 1) or D3Batch (S > 1) handle: stage 1 writes G_r = a_r; stage 2
+    writes out_r = B_r G + c_r over the 10 S + 3 N result values."""
 
-    def __init__(self, rank):
-        rng = np.random.default_rng(100 + rank)
+    def __init__(self, rank, S=1):
+        rng = np.random.default_rng(100 + rank + 10 * S)
+        self.S = S
         self.a = rng.normal(size=N)
         self.B = rng.normal(size=(10 * S + 3 * N, N))
         self.c = rng.normal(size=10 * S + 3 * N)
@@ -27,6 +29,9 @@ class LinearStages:
     def shard_length(self):
         return N
 
+    def shard_structures(self):
+        return self.S
+
     def shard_begin(self, rank, world, G_ptr, stream):
         g = torch.from_numpy(self.a.copy())
         _write(G_ptr, g)
@@ -34,6 +39,8 @@ class LinearStages:
     def shard_end(self, G_ptr, out_ptr, stream):
         G = _read(G_ptr, N)
         self.seen_G = G.copy()
+        S = self.S
+        assert _BUFS[out_ptr].numel() == 10 * S + 3 * N  # the buffer the evaluator sized
         _write(out_ptr, torch.from_numpy(self.B @ G + self.c))
 
 
@@ -48,14 +55,14 @@ def _read(ptr, n):
     return _BUFS[ptr][:n].numpy().copy()
 
 
-def _worker(rank, world, port, q):
+def _worker(rank, world, port, q, S=1):
     import torch.distributed as dist
 
     import d3_shard
 
     dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
     try:
-        h = LinearStages(rank)
+        h = LinearStages(rank, S)
         ev = d3_shard.ShardedEvaluator(h, device="cpu")
         _BUFS[ev.G.data_ptr()] = ev.G
         _BUFS[ev.out.data_ptr()] = ev.out
@@ -71,12 +78,14 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def test_two_rank_gloo_protocol():
+@pytest.mark.parametrize("S", [1, 3])
+def test_two_rank_gloo_protocol(S):
+    # S = 3: a batch handle; the results buffer must be sized from the handle
     world = 2
     ctx = torch.multiprocessing.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, S)) for r in range(world)]
     for p in procs:
         p.start()
     res = {}
@@ -86,12 +95,28 @@ def test_two_rank_gloo_protocol():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    hs = [LinearStages(r) for r in range(world)]
+    hs = [LinearStages(r, S) for r in range(world)]
     G = sum(h.a for h in hs)
     out = sum(h.B @ G + h.c for h in hs)
     for r in range(world):
         e, f, s, g = res[r]
         np.testing.assert_allclose(g, G, rtol=0, atol=1e-12)
-        np.testing.assert_allclose(e, out[0], rtol=0, atol=1e-12)
-        np.testing.assert_allclose(f.ravel(), out[S:S + 3 * N], rtol=0, atol=1e-12)
-        np.testing.assert_allclose(s.ravel(), out[S + 3 * N:S + 3 * N + 9], rtol=0, atol=1e-12)
+        np.testing.assert_allclose(np.ravel(e), out[:S], rtol=0, atol=1e-12)
+        np.testing.assert_allclose(np.ravel(f), out[S:S + 3 * N], rtol=0, atol=1e-12)
+        np.testing.assert_allclose(np.ravel(s), out[S + 3 * N:S + 3 * N + 9 * S], rtol=0, atol=1e-12)
+
+
+def test_structure_count_mismatch_is_rejected():
+    # an explicit count that disagrees with the handle would size the buffer wrongly
+    import torch.distributed as dist
+
+    import d3_shard
+
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % _free_port(), rank=0, world_size=1)
+    try:
+        with pytest.raises(ValueError):
+            d3_shard.ShardedEvaluator(LinearStages(0, 2), num_structures=1, device="cpu")
+        ev = d3_shard.ShardedEvaluator(LinearStages(0, 2), device="cpu")
+        assert ev.out.numel() == 10 * 2 + 3 * N
+    finally:
+        dist.destroy_process_group()

@@ -80,3 +80,36 @@ def test_sharded_without_atm_and_small_cell():
     o = (outs[0] + outs[1]).cpu().numpy()
     assert abs(o[0] - e0) <= 1e-12 * abs(e0)
     assert np.abs(o[1:1 + 3 * n].reshape(n, 3) - f0).max() <= 1e-10 * np.abs(f0).max()
+
+
+def test_sharded_batch_handle():
+    # a batch handle of three structures: results are 10 S + 3 n values, S taken from the handle
+    from d3_b200 import D3Batch
+
+    structs = [S.triclinic_box(200, seed=11), S.triclinic_box(150, seed=12), S.water_box(0)]
+    elements = sorted(set(int(z) for s in structs for z in s["Z"]))
+    n = sum(len(s["Z"]) for s in structs)
+
+    def batch():
+        b = D3Batch(elements, len(structs), n, rc=95.0, rc_cn=40.0, rc_atm=40.0)
+        b.set_structures(structs)
+        return b
+
+    e0, f0, s0 = batch().compute()
+    world = 2
+    hs = [batch() for _ in range(world)]
+    assert hs[0].shard_structures() == len(structs) and hs[0].shard_length() == n
+    Gs = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(world)]
+    outs = [torch.zeros(10 * len(structs) + 3 * n, dtype=torch.float64, device="cuda") for _ in range(world)]
+    for r, h in enumerate(hs):
+        h.shard_begin(r, world, Gs[r].data_ptr())
+    G = sum(Gs)
+    for r, h in enumerate(hs):
+        h.shard_end(G.data_ptr(), outs[r].data_ptr())
+    torch.cuda.synchronize()
+    o = sum(outs).cpu().numpy()
+    nS = len(structs)
+    np.testing.assert_allclose(o[:nS], e0, rtol=1e-12)
+    f1 = o[nS:nS + 3 * n].reshape(n, 3)
+    np.testing.assert_allclose(f1, np.concatenate(f0), rtol=0, atol=1e-10 * np.abs(np.concatenate(f0)).max())
+    np.testing.assert_allclose(o[nS + 3 * n:].reshape(nS, 3, 3), s0, rtol=0, atol=1e-10 * np.abs(s0).max())

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import d3_systems as S
-from d3_b200 import D3, load_library
+from d3_b200 import D3, TABLE_7REF, load_library
 
 pytestmark = pytest.mark.gpu
 
@@ -27,8 +27,8 @@ def _bind(lib):
     return f
 
 
-def _handle_cn(sys_, rc_cn):
-    d = D3(sys_["Z"], len(sys_["Z"]), rc=rc_cn, rc_cn=rc_cn)
+def _handle_cn(sys_, rc_cn, table=0):
+    d = D3(sys_["Z"], len(sys_["Z"]), rc=rc_cn, rc_cn=rc_cn, table=table)
     d.set_cell(sys_["cell"])
     d.set_atoms(sys_["pos"], sys_["Z"])
     d.compute()
@@ -37,7 +37,7 @@ def _handle_cn(sys_, rc_cn):
     return cn
 
 
-def _noalloc_cn(fn, sys_, rc_cn):
+def _noalloc_cn(fn, sys_, rc_cn, table=0):
     import torch
 
     pos = torch.from_numpy(np.ascontiguousarray(sys_["pos"], np.float64)).cuda()
@@ -45,7 +45,7 @@ def _noalloc_cn(fn, sys_, rc_cn):
     out = torch.full((len(sys_["Z"]),), -1.0, dtype=torch.float64, device="cuda")
     cell = np.ascontiguousarray(sys_["cell"], np.float64).reshape(9)
     stream = torch.cuda.current_stream().cuda_stream
-    rc = fn(pos.data_ptr(), z.data_ptr(), len(sys_["Z"]), cell.ctypes.data, rc_cn, 0, out.data_ptr(), stream)
+    rc = fn(pos.data_ptr(), z.data_ptr(), len(sys_["Z"]), cell.ctypes.data, rc_cn, table, out.data_ptr(), stream)
     assert rc == 0
     torch.cuda.synchronize()
     return out.cpu().numpy()
@@ -63,6 +63,22 @@ def test_noalloc_matches_handle_api_on_two_calls_in_a_row():
     np.testing.assert_allclose(got_small, want_small, rtol=1e-12, atol=1e-12)
 
 
+def test_noalloc_extended_table_and_element_outside_the_table():
+    # 7-reference layout (slots by Z - 1) against a handle built with that table; then one
+    # atom of an element outside the 5-reference table (Z = 100): its CN is NaN and it
+    # contributes nothing to the other atoms
+    fn = _bind(load_library())
+    sys_ = S.triclinic_box(400, seed=21)
+    np.testing.assert_allclose(_noalloc_cn(fn, sys_, 40.0, table=TABLE_7REF), _handle_cn(sys_, 40.0, TABLE_7REF),
+                               rtol=1e-12, atol=1e-12)
+    odd = dict(sys_)
+    odd["Z"] = np.concatenate([sys_["Z"], [100]])
+    odd["pos"] = np.concatenate([sys_["pos"], sys_["pos"][:1] + 0.9])
+    got = _noalloc_cn(fn, odd, 40.0)
+    assert np.isnan(got[-1])
+    np.testing.assert_allclose(got[:-1], _handle_cn(sys_, 40.0), rtol=1e-12, atol=1e-12)
+
+
 def test_noalloc_rejects_sizes_beyond_its_maximum():
     lib = load_library()
     fn = _bind(lib)
@@ -72,3 +88,4 @@ def test_noalloc_rejects_sizes_beyond_its_maximum():
     rc = fn(dummy.ctypes.data, dummy.ctypes.data, n, cell.ctypes.data, 40.0, 0, dummy.ctypes.data, None)
     assert rc == 1
     assert b"exceed the maximum" in lib.d3_last_error()
+
