@@ -116,8 +116,13 @@ enum {
     D3_OPT_BIN_DIVISOR = 4,      /* cell-list bin width = smallest cutoff / value (1..32, default 6) */
     D3_OPT_ATM_TILE = 5,         /* ATM partner tile entries (0 = automatic) */
     D3_OPT_ATM_CTAS_PER_SM = 6,  /* persistent ATM CTAs per SM (0 = occupancy limit) */
-    D3_OPT_ATM_SCHEDULE = 8      /* precision-form ATM: 0 (default) block pairs, each triplet
+    D3_OPT_ATM_SCHEDULE = 8,     /* precision-form ATM: 0 (default) block pairs, each triplet
                                     visited once; 1 mirror-symmetric, each triplet twice */
+    D3_OPT_ATM_LIST_CAPACITY = 9 /* ATM half-list capacity in entries (0 = estimated from the
+                                    density, the default). A synchronous evaluation whose
+                                    list overflows grows it and runs again; an asynchronous
+                                    one (d3_compute_async, graph replays) sets status bit 0
+                                    and leaves the ATM terms out instead */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);
 
@@ -154,6 +159,11 @@ int d3_set_positions_device(d3_handle_t *handle, const double *coords_dev, void 
    d3_compute_f64 or compute_dispersion_energy_from_handle_status first). */
 uint16_t d3_compute_async(d3_handle_t *handle, void *cuda_stream);
 const double *d3_device_results(d3_handle_t *handle);
+/* Status word of the last enqueued evaluation (synchronise its stream first): how an
+   asynchronous or graph-replayed evaluation reports a list overflow (bit 0) or bad input
+   (bit 1). d3_atm_list_capacity: the ATM half-list capacity now allocated (entries). */
+uint16_t d3_fetch_status(d3_handle_t *handle);
+int64_t d3_atm_list_capacity(d3_handle_t *handle);
 /* Stream-ordered device-to-device copy of the results of the last enqueued evaluation
    (energies [S], forces [n][3], stresses [S][9], double) to a caller buffer; it can be
    captured in a CUDA graph together with d3_compute_async (MD loops). */
@@ -294,6 +304,16 @@ const char *d3_last_error(void);
 int d3_debug_atom_arrays(d3_handle_t *handle, double *cn, double *dedcn, double *energy_atoms);
 int64_t d3_debug_atm_pairs(d3_handle_t *handle, int64_t *rows, int64_t cap);
 int d3_debug_bins(d3_handle_t *handle, int64_t *wrap_shift, int64_t *bin_index, int *num_bins);
+/* Per-pass terms of the last evaluation, D3_DEBUG_TERM_COLUMNS doubles per atom (caller
+   order; hartree and bohr, the reference's sign conventions): [0] two-body energy (half
+   of every ordered pair of the atom), [1] its dE/dCN, [2..4] its force, [5..10] its
+   virial; [11] ATM apex share (a third of the energy of every triplet whose largest
+   index is the atom), [12] the atom's dE/dCN from those triplets, [13..15] its force
+   from them, [16..21] their virial; [22..24] dE/dCN chain-rule force, [25..30] its
+   virial. Virials are xx yy zz xy xz yz, already divided by the cell volume (two-body
+   and chain rule: also by 2). Diagnostics for parity tests (no reference counterpart). */
+#define D3_DEBUG_TERM_COLUMNS 31
+int d3_debug_pass_terms(d3_handle_t *handle, double *terms);
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,16 @@ d3_handle_t *make_handle(const uint16_t *elements, uint64_t n_el, uint64_t max_l
     return reinterpret_cast<d3_handle_t *>(h);
 }
 
+std::string status_message(unsigned st) {
+    if (st & d3::ST_CUDA_ERROR) return "CUDA error during compute";
+    if (st & d3::ST_NOT_READY) return "atoms or cell not set";
+    if (st & d3::ST_BAD_CELL) return "degenerate cell (set_cell failed)";
+    if (st & d3::ST_BAD_INPUT) return "non-finite coordinate or cell";
+    if (st & d3::ST_SHIFT_RANGE) return "lattice shift outside the packed range";
+    if (st & d3::ST_LIST_OVERFLOW) return "ATM neighbour list overflow";
+    return "";
+}
+
 uint16_t compute_float(Handle *h, real_t *energy, real_t *force, real_t *stress) {
     if (d3::engine_num_structures(h->engine) > 1) {
         set_error("handle holds a batch of structures; use d3_compute_batch_f64");
@@ -59,8 +69,8 @@ uint16_t compute_float(Handle *h, real_t *energy, real_t *force, real_t *stress)
     h->f64_forces.resize(3 * n);
     double e = 0, s[9] = {0};
     uint16_t st = d3::engine_compute(h->engine, &e, h->f64_forces.data(), s, nullptr, true);
-    if (st & (d3::ST_CUDA_ERROR | d3::ST_NOT_READY)) {
-        set_error(st & d3::ST_NOT_READY ? "atoms or cell not set" : "CUDA error during compute");
+    if (st & (d3::ST_CUDA_ERROR | d3::ST_NOT_READY | d3::ST_BAD_CELL)) {
+        set_error(status_message(st));
         return st;
     }
     if (energy) *energy = (real_t)e;
@@ -216,8 +226,7 @@ uint16_t d3_compute_f64(d3_handle_t *handle, double *energy, double *force, doub
         return d3::ST_BAD_INPUT;
     }
     uint16_t st = d3::engine_compute(H(handle)->engine, energy, force, stress, nullptr, true);
-    if (st & (d3::ST_CUDA_ERROR | d3::ST_NOT_READY))
-        set_error(st & d3::ST_NOT_READY ? "atoms or cell not set" : "CUDA error during compute");
+    if (st) set_error(status_message(st));
     return st;
 }
 
@@ -247,6 +256,7 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
         }
         o.atm_schedule = value;
         break;
+    case D3_OPT_ATM_LIST_CAPACITY: o.atm_list_capacity = value < 0 ? 0 : value; break;
     case D3_OPT_PRECISION:
         if (value != 0 && value != 1) {
             set_error("D3_OPT_PRECISION takes 0 (FP64) or 1 (FP32 pair/triplet arithmetic)");
@@ -361,6 +371,21 @@ const double *d3_device_results(d3_handle_t *handle) {
     return handle ? d3::engine_device_results(H(handle)->engine) : nullptr;
 }
 
+uint16_t d3_fetch_status(d3_handle_t *handle) {
+    if (!handle) {
+        set_error("handle is NULL in d3_fetch_status");
+        return 1;
+    }
+    try {
+        return d3::engine_fetch_status(H(handle)->engine);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return d3::ST_CUDA_ERROR;
+    }
+}
+
+int64_t d3_atm_list_capacity(d3_handle_t *handle) { return handle ? d3::engine_atm_capacity(H(handle)->engine) : -1; }
+
 const char *d3_last_error(void) { return g_last_error.c_str(); }
 
 int d3_pass_times(d3_handle_t *handle, float *ms, int cap, uint64_t *counters) {
@@ -399,6 +424,16 @@ int d3_debug_atom_arrays(d3_handle_t *handle, double *cn, double *dedcn, double 
     if (!handle) return 1;
     try {
         return d3::engine_debug_atom_arrays(H(handle)->engine, cn, dedcn, energy_atoms);
+    } catch (const std::exception &ex) {
+        set_error(ex.what());
+        return 1;
+    }
+}
+
+int d3_debug_pass_terms(d3_handle_t *handle, double *terms) {
+    if (!handle || !terms) return 1;
+    try {
+        return d3::engine_debug_pass_terms(H(handle)->engine, terms);
     } catch (const std::exception &ex) {
         set_error(ex.what());
         return 1;

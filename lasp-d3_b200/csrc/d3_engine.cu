@@ -1114,6 +1114,7 @@ struct Engine {
     // state
     uint64_t n = 0;
     bool atoms_set = false, cell_set = false;
+    unsigned int cell_status = 0; // status of the last set_cell that failed (bad input / cell)
     int nstruct = 0;
     int nbins_total = 0;
     std::vector<SG> sg;          // per-structure geometry
@@ -1413,7 +1414,13 @@ void engine_destroy(Engine *e) {
 
 void engine_set_options(Engine *e, const Options &o) {
     const bool regrid = o.bin_divisor != e->opt.bin_divisor;
+    const bool recap = o.atm_list_capacity != e->opt.atm_list_capacity;
     e->opt = o;
+    if (recap && e->use_atm) {
+        // a given capacity replaces the estimate (0: estimate again at the next evaluation)
+        e->atm_cap = o.atm_list_capacity;
+        if (e->atm_cap > 0) e->atm_ent.ensure((size_t)e->atm_cap);
+    }
     if (regrid && e->cell_set && e->nstruct > 0) {
         const std::vector<uint64_t> c = e->counts;
         const std::vector<double> cl = e->cells;
@@ -1541,10 +1548,13 @@ int engine_set_cell(Engine *e, const double cell[9], const float cell_f[9], std:
         const uint64_t c = e->n;
         build_structures(e, 1, &c, cell, cell_f);
         e->cell_set = true;
+        e->cell_status = 0;
         return 0;
     } catch (const std::exception &ex) {
+        // an evaluation without a valid cell returns this status (not the generic "not set")
         e->cell_set = false;
         err = ex.what();
+        e->cell_status = err.find("non-finite") != std::string::npos ? ST_BAD_INPUT : ST_BAD_CELL;
         return 1;
     }
 }
@@ -2025,7 +2035,16 @@ static void ensure_atm_capacity(Engine *e) {
     e->atm_ent.ensure((size_t)e->atm_cap);
 }
 
+long long engine_atm_capacity(const Engine *e) { return e->use_atm ? e->atm_cap : 0; }
+
+uint16_t engine_fetch_status(Engine *e) {
+    unsigned int st = 0;
+    D3_CUDA(cudaMemcpy(&st, e->status.p, sizeof(unsigned int), cudaMemcpyDeviceToHost));
+    return (uint16_t)st;
+}
+
 uint16_t engine_compute(Engine *e, double *energy, double *forces, double *stress, cudaStream_t stream, bool sync) {
+    if (!e->cell_set && e->cell_status) return (uint16_t)e->cell_status;
     if (!e->atoms_set || !e->cell_set) return ST_NOT_READY;
     cudaStream_t s = stream ? stream : e->stream;
     try {
@@ -2082,6 +2101,35 @@ int engine_debug_atom_arrays(Engine *e, double *cn, double *dedcn, double *energ
         if (cn) cn[i] = a[s];
         if (dedcn) dedcn[i] = g[s];
         if (energy_atoms) energy_atoms[i] = b[s] + (e->use_atm ? c[s] + d[s] : 0.0);
+    }
+    return 0;
+}
+
+int engine_debug_pass_terms(Engine *e, double *out) {
+    // per atom (caller order), D3_DEBUG_TERM_COLUMNS doubles, internal units (hartree,
+    // bohr): two-body e, dE/dCN, force[3], virial[6]; ATM apex share e, dE/dCN, force[3],
+    // virial[6]; chain-rule force[3], virial[6]; virials as xx yy zz xy xz yz, already
+    // scaled by the pass's volume factor
+    const uint64_t n = e->n;
+    std::vector<int> orig(n);
+    D3_CUDA(cudaStreamSynchronize(e->stream));
+    D3_CUDA(cudaMemcpy(orig.data(), e->orig.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    struct Col {
+        const double *src;
+        int width, col;
+    };
+    const bool atm = e->use_atm;
+    const Col cols[] = {{e->e2.p, 1, 0}, {e->g2.p, 1, 1}, {e->f2.p, 3, 2}, {e->v2.p, 6, 5},
+                        {atm ? e->ea.p : nullptr, 1, 11}, {atm ? e->ga.p : nullptr, 1, 12},
+                        {atm ? e->fa.p : nullptr, 3, 13}, {atm ? e->va.p : nullptr, 6, 16},
+                        {e->fc.p, 3, 22}, {e->vc.p, 6, 25}};
+    constexpr int W = 31;
+    std::vector<double> buf(6 * n);
+    for (const Col &c : cols) {
+        if (c.src)
+            D3_CUDA(cudaMemcpy(buf.data(), c.src, sizeof(double) * c.width * n, cudaMemcpyDeviceToHost));
+        for (uint64_t s = 0; s < n; ++s)
+            for (int k = 0; k < c.width; ++k) out[(size_t)orig[s] * W + c.col + k] = c.src ? buf[s * c.width + k] : 0.0;
     }
     return 0;
 }

@@ -51,6 +51,8 @@ struct Options {
     bool atm_surrogate = false;    // learned ATM surrogate with exact fallback (needs a model)
     int atm_schedule = 0;          // precision-form ATM: 0 block pairs (each triplet once),
                                    // 1 mirror-symmetric full square (each triplet twice)
+    long long atm_list_capacity = 0; // ATM half-list entries to allocate (0: estimate from the
+                                     // density); a synchronous evaluation regrows on overflow
 };
 
 // Learned ATM surrogate: network parameters and normalisation (network in d3_mlp.h).
@@ -132,6 +134,9 @@ uint16_t engine_shard_end(Engine *e, const double *G_in, double *out_dev, cudaSt
 // in the caller's atom order; ATM list (caller indices and reference lattice shifts)
 int engine_debug_atom_arrays(Engine *e, double *cn, double *dedcn, double *energy_atoms);
 int64_t engine_debug_atm_pairs(Engine *e, int64_t *out, int64_t cap);
+int engine_debug_pass_terms(Engine *e, double *out);
+long long engine_atm_capacity(const Engine *e);
+uint16_t engine_fetch_status(Engine *e);
 int engine_debug_bins(Engine *e, int64_t *wrap_shift, int64_t *bin_index, int nb_out[3]);
 
 } // namespace d3

@@ -25,6 +25,7 @@ OPT_ATM_FORCE_SCALED, OPT_SMOOTH_CN, OPT_PRECISION = 1, 2, 3
 OPT_BIN_DIVISOR, OPT_ATM_TILE, OPT_ATM_CTAS_PER_SM = 4, 5, 6
 OPT_ATM_SURROGATE = 7
 OPT_ATM_SCHEDULE = 8
+OPT_ATM_LIST_CAPACITY = 9
 TABLE_5REF, TABLE_7REF = 0, 1
 
 _lib = None
@@ -98,6 +99,12 @@ def load_library(path=None):
     lib.d3_last_error.argtypes = []
     lib.d3_debug_atom_arrays.restype = ctypes.c_int
     lib.d3_debug_atom_arrays.argtypes = [vp, vp, vp, vp]
+    lib.d3_fetch_status.restype = ctypes.c_uint16
+    lib.d3_fetch_status.argtypes = [vp]
+    lib.d3_atm_list_capacity.restype = i64
+    lib.d3_atm_list_capacity.argtypes = [vp]
+    lib.d3_debug_pass_terms.restype = ctypes.c_int
+    lib.d3_debug_pass_terms.argtypes = [vp, vp]
     lib.d3_debug_atm_pairs.restype = i64
     lib.d3_debug_atm_pairs.argtypes = [vp, vp, i64]
     lib.d3_debug_bins.restype = ctypes.c_int
@@ -306,6 +313,20 @@ class D3(_Surrogate, _Shard):
         cn, g, e = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
         self.lib.d3_debug_atom_arrays(self.h, _ptr(cn), _ptr(g), _ptr(e))
         return cn, g, e
+
+    def fetch_status(self):
+        """Status word of the last enqueued evaluation (synchronise its stream first)."""
+        return int(self.lib.d3_fetch_status(self.h))
+
+    def atm_list_capacity(self):
+        return int(self.lib.d3_atm_list_capacity(self.h))
+
+    def pass_terms(self):
+        """Per-pass per-atom terms of the last evaluation ([n, 31], see d3_debug_pass_terms)."""
+        t = np.zeros((self.n, 31))
+        if self.lib.d3_debug_pass_terms(self.h, _ptr(t)):
+            raise RuntimeError(self.lib.d3_last_error().decode())
+        return t
 
     def atm_pairs(self):
         m = self.lib.d3_debug_atm_pairs(self.h, None, 0)

@@ -8,6 +8,8 @@ src/d3_cffi.py:96-120). Additions, all optional:
     (bohr) to enable the ATM three-body term (the reference's binding cannot reach it,
     src/d3_cffi.py:8-45 omits the declaration);
   * `compute_f64()` returns the FP64 results of the same evaluation path;
+  * `D3BatchCalculator` evaluates many independent periodic structures in one call
+    (d3_init_batch / d3_set_batch_f64 / d3_compute_batch_f64);
   * the library path can be overridden with the D3_LIBRARY environment variable.
 """
 import os
@@ -68,6 +70,14 @@ uint16_t compute_dispersion_energy_from_handle_status(
 
 uint16_t d3_compute_f64(d3_handle_t *handle, double *energy, double *force, double *stress);
 const char *d3_last_error(void);
+
+d3_handle_t *d3_init_batch(const uint16_t *elements, uint64_t n_elements, uint64_t max_structures,
+                           uint64_t max_total_atoms, double rc, double rc_cn, double rc_atm, int damping_type,
+                           int functional_type, int table);
+int d3_set_batch_f64(d3_handle_t *handle, uint64_t n_structures, const uint64_t *atom_counts, const double *coords,
+                     const uint16_t *elements, const double *cells);
+uint16_t d3_compute_batch_f64(d3_handle_t *handle, double *energies, double *forces, double *stresses);
+int d3_num_structures(d3_handle_t *handle);
 """)
 
 lib_path = os.environ.get("D3_LIBRARY") or os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libd3.so")
@@ -138,6 +148,55 @@ class D3Calculator:
 
     def __del__(self):
         """Clean up when the object is deleted."""
+        if hasattr(self, "handle") and self.handle != ffi.NULL:
+            lib.free_d3_handle(self.handle)
+            self.handle = ffi.NULL
+
+
+class D3BatchCalculator:
+    """Many independent periodic structures in one handle, FP64 in and out (cutoffs in
+    bohr, atm_cutoff None disables ATM)."""
+
+    def __init__(self, elements: list[int], max_structures: int, max_total_atoms: int, cutoff_radius: float = 95.0,
+                 cn_cutoff_radius: float = 40.0, atm_cutoff: float | None = None, damping_type: int = 1,
+                 functional_type: int = 0, table: int = 0):
+        el = np.array(sorted(set(int(z) for z in elements)), dtype=np.uint16)
+        self._el = el
+        self.handle = lib.d3_init_batch(ffi.cast("uint16_t*", el.ctypes.data), len(el), max_structures,
+                                        max_total_atoms, cutoff_radius, cn_cutoff_radius, atm_cutoff or 0.0,
+                                        damping_type, functional_type, table)
+        if self.handle == ffi.NULL:
+            raise RuntimeError("failed to initialise the D3 batch handle: " + ffi.string(lib.d3_last_error()).decode())
+        self.counts = None
+
+    def set_structures(self, structures):
+        """structures: sequence of (coords [n, 3] Angstrom, elements [n], cell [3, 3] Angstrom)."""
+        counts = np.array([len(z) for _, z, _ in structures], dtype=np.uint64)
+        coords = np.ascontiguousarray(np.concatenate([np.asarray(c, np.float64) for c, _, _ in structures]))
+        z = np.ascontiguousarray(np.concatenate([np.asarray(e, np.uint16) for _, e, _ in structures]))
+        cells = np.ascontiguousarray(np.stack([np.asarray(c, np.float64).reshape(9) for _, _, c in structures]))
+        if lib.d3_set_batch_f64(self.handle, len(counts), ffi.cast("uint64_t*", counts.ctypes.data),
+                                ffi.cast("double*", coords.ctypes.data), ffi.cast("uint16_t*", z.ctypes.data),
+                                ffi.cast("double*", cells.ctypes.data)):
+            raise RuntimeError(ffi.string(lib.d3_last_error()).decode())
+        self.counts = counts
+
+    def compute(self):
+        """Energies [S] (eV), forces per structure [n_s, 3] (eV/A), stresses [S, 3, 3] (eV/A^3)."""
+        S, n = len(self.counts), int(self.counts.sum())
+        e = np.zeros(S)
+        f = np.zeros((n, 3))
+        st = np.zeros((S, 9))
+        result = lib.d3_compute_batch_f64(self.handle, ffi.cast("double*", e.ctypes.data),
+                                          ffi.cast("double*", f.ctypes.data), ffi.cast("double*", st.ctypes.data))
+        if result == 0b01:
+            raise RuntimeError("Error computing dispersion energy: neighbor list overflow")
+        if result:
+            raise RuntimeError("d3_compute_batch_f64 status %d: %s" % (result, ffi.string(lib.d3_last_error()).decode()))
+        off = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        return e, [f[off[k]:off[k + 1]] for k in range(S)], st.reshape(S, 3, 3)
+
+    def __del__(self):
         if hasattr(self, "handle") and self.handle != ffi.NULL:
             lib.free_d3_handle(self.handle)
             self.handle = ffi.NULL

@@ -148,6 +148,14 @@ def triclinic_box(n=20000, seed=1, composition=MIX_HCNOCU):
     return random_box(n, cell, composition=composition, seed=seed)
 
 
+def cell_list_box(n=400, seed=31, edge=160.0, shear=0.0):
+    """A low-density box thick enough (every perpendicular height above 3 x 95 bohr) for
+    the reference's cell-list path. shear: the b vector's x component in units of the
+    edge, which makes the reference's grid cells along x thinner than the cutoff."""
+    cell = edge * np.array([[1.0, 0.0, 0.0], [shear, 1.0, 0.0], [0.0, 0.0, 1.0]])
+    return random_box(n, cell, composition=MIX_HCNOCU, seed=seed)
+
+
 def batch_structs(count=2048, seed=3, nmin=8, nmax=2000, density=0.1, tilt=0.1,
                   species=("H", "C", "N", "O", "Si", "Cu")):
     """Independent periodic structures: log-uniform atom counts, cubic edge for the given

@@ -248,6 +248,224 @@ static double cn_term(const oracle_params *p, double r, double rsum, double *dcn
     return 1.0 / (1.0 + e);
 }
 
+/* ------------------------------------------------------------------------ */
+/* per-atom pieces of the evaluation, shared by the full evaluation and the  */
+/* per-atom term export                                                      */
+
+/* CN of atom i over every atom and image (src/d3_kernel.cu:582-683) */
+static double cn_of_atom(const oracle_params *p, int64_t n, const double *pos, const int *types,
+                         const image_set *im, int64_t i) {
+    const double rcn2 = p->rc_cn * p->rc_cn;
+    double acc = 0;
+    double ri = p->rcov[types[i]];
+    for (int64_t j = 0; j < n; ++j) {
+        double rs = ri + p->rcov[types[j]];
+        for (int64_t b = 0; b < im->n_img; ++b) {
+            double dx = pos[3 * i] - (pos[3 * j] + im->shift[3 * b]);
+            double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im->shift[3 * b + 1]);
+            double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im->shift[3 * b + 2]);
+            double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 <= rcn2 && d2 > 0.0) {
+                double dd;
+                acc += cn_term(p, sqrt(d2), rs, &dd);
+            }
+        }
+    }
+    return acc;
+}
+
+/* growable half list of one apex: entry atoms and image positions */
+typedef struct {
+    int64_t cap, m;
+    int64_t *lj;
+    double *lv;
+} atm_list;
+
+static void atm_list_build(atm_list *L, int64_t n, const double *pos, const image_set *im, double ra2, int64_t a) {
+    /* L_a: (b, T_b) with b <= a, 1e-12 <= r_ab^2 <= rc_atm^2, ordered by (b, image) */
+    (void)n;
+    L->m = 0;
+    for (int64_t b = 0; b <= a; ++b)
+        for (int64_t t = 0; t < im->n_img; ++t) {
+            double px = pos[3 * b] + im->shift[3 * t], py = pos[3 * b + 1] + im->shift[3 * t + 1],
+                   pz = pos[3 * b + 2] + im->shift[3 * t + 2];
+            double rx = pos[3 * a] - px, ry = pos[3 * a + 1] - py, rz = pos[3 * a + 2] - pz;
+            double d2 = rx * rx + ry * ry + rz * rz;
+            if (d2 > ra2 || d2 < 1e-12) continue;
+            if (L->m == L->cap) {
+                L->cap = L->cap ? 2 * L->cap : 1024;
+                L->lj = (int64_t *)realloc(L->lj, sizeof(int64_t) * L->cap);
+                L->lv = (double *)realloc(L->lv, sizeof(double) * 3 * L->cap);
+            }
+            L->lj[L->m] = b;
+            L->lv[3 * L->m] = px;
+            L->lv[3 * L->m + 1] = py;
+            L->lv[3 * L->m + 2] = pz;
+            ++L->m;
+        }
+}
+
+/* every triplet of apex a (src/d3_kernel.cu:1235-1478): energy E/3 to each atom, dE/dCN,
+   forces into E[n], G[n], F[3n] and the virial into Vv[9] */
+static void atm_apex(const oracle_params *p, const c6_ctx *cc, const double *pos, const int *types, double V,
+                     const atm_list *L, int64_t a, double *E, double *G, double *F, double *Vv) {
+    const double ra2 = p->rc_atm * p->rc_atm;
+    const int64_t m = L->m;
+    const int64_t *lj = L->lj;
+    const double *lv = L->lv;
+    const double *xa = pos + 3 * a;
+    for (int64_t ib = 0; ib < m; ++ib) {
+        int64_t b = lj[ib];
+        double c6ab, dab_a, dab_b;
+        pair_c6(cc, a, b, &c6ab, &dab_a, &dab_b);
+        double r0ab = p->r0ab[types[a] * p->ne + types[b]];
+        double rab[3] = {xa[0] - lv[3 * ib], xa[1] - lv[3 * ib + 1], xa[2] - lv[3 * ib + 2]};
+        for (int64_t ic = 0; ic < m; ++ic) {
+            int64_t c = lj[ic];
+            if (c > b) break; /* entries are ordered by atom index */
+            double rac[3] = {xa[0] - lv[3 * ic], xa[1] - lv[3 * ic + 1], xa[2] - lv[3 * ic + 2]};
+            double rbc[3] = {lv[3 * ib] - lv[3 * ic], lv[3 * ib + 1] - lv[3 * ic + 1], lv[3 * ib + 2] - lv[3 * ic + 2]};
+            double d_ac2 = rac[0] * rac[0] + rac[1] * rac[1] + rac[2] * rac[2];
+            double d_bc2 = rbc[0] * rbc[0] + rbc[1] * rbc[1] + rbc[2] * rbc[2];
+            if (d_ac2 > ra2 || d_bc2 > ra2 || d_ac2 < 1e-12 || d_bc2 < 1e-12) continue;
+            double scale;
+            if (c == b && b == a)
+                scale = 1.0 / 6.0;
+            else if (c == b || c == a || b == a)
+                scale = 0.5;
+            else
+                scale = 1.0;
+            double c6ac, dac_a, dac_c, c6bc, dbc_b, dbc_c;
+            pair_c6(cc, a, c, &c6ac, &dac_a, &dac_c);
+            pair_c6(cc, b, c, &c6bc, &dbc_b, &dbc_c);
+            double r0ac = p->r0ab[types[a] * p->ne + types[c]];
+            double r0bc = p->r0ab[types[b] * p->ne + types[c]];
+
+            double ab2 = rab[0] * rab[0] + rab[1] * rab[1] + rab[2] * rab[2];
+            double ab = sqrt(ab2), ab3 = ab2 * ab, ab4 = ab2 * ab2;
+            double ac2 = d_ac2, ac = sqrt(ac2), ac3 = ac2 * ac, ac4 = ac2 * ac2;
+            double bc2 = d_bc2, bc = sqrt(bc2), bc3 = bc2 * bc, bc4 = bc2 * bc2;
+            double rsq = ab2 * ac2 * bc2, r = sqrt(rsq);
+            double t1 = ab2 + ac2 - bc2, t2 = ab2 - ac2 + bc2, t3 = -ab2 + ac2 + bc2;
+            double cosine = t1 * t2 * t3 / (8.0 * rsq);
+            double ang = (1.0 + 3.0 * cosine) / (rsq * r);
+            double dang_ab = 3.0 / 8.0 *
+                             (ab3 * ab3 + ab4 * (ac2 + bc2) + ab2 * (3.0 * bc2 * bc2 + 2.0 * bc2 * ac2 + 3.0 * ac2 * ac2) -
+                              5.0 * (bc2 - ac2) * (bc2 - ac2) * (bc2 + ac2)) /
+                             (rsq * rsq * r);
+            double dang_ac = 3.0 / 8.0 *
+                             (ac3 * ac3 + ac4 * (bc2 + ab2) + ac2 * (3.0 * bc2 * bc2 + 2.0 * bc2 * ab2 + 3.0 * ab2 * ab2) -
+                              5.0 * (bc2 - ab2) * (bc2 - ab2) * (bc2 + ab2)) /
+                             (rsq * rsq * r);
+            double dang_bc = 3.0 / 8.0 *
+                             (bc3 * bc3 + bc4 * (ac2 + ab2) + bc2 * (3.0 * ac2 * ac2 + 2.0 * ac2 * ab2 + 3.0 * ab2 * ab2) -
+                              5.0 * (ac2 - ab2) * (ac2 - ab2) * (ac2 + ab2)) /
+                             (rsq * rsq * r);
+            double C9 = -sqrt(c6ab * c6ac * c6bc);
+            double dC9_ab = -0.5 * C9 / c6ab, dC9_ac = -0.5 * C9 / c6ac, dC9_bc = -0.5 * C9 / c6bc;
+            double dC9a = dC9_ab * dab_a + dC9_ac * dac_a;
+            double dC9b = dC9_ab * dab_b + dC9_bc * dbc_b;
+            double dC9c = dC9_ac * dac_c + dC9_bc * dbc_c;
+            double ravg = pow(ab2 * ac2 * bc2, 1.0 / 6.0);
+            double r0 = pow(r0ab * r0ac * r0bc, 1.0 / 3.0);
+            double x16 = pow(4.0 / 3.0 * r0 / ravg, 16.0);
+            double fd = 1.0 / (1.0 + 6.0 * x16);
+            double dfd = 2.0 * 16.0 * x16 * fd * fd;
+            double e3 = C9 * ang * fd * scale / 3.0;
+            E[a] += e3;
+            E[b] += e3;
+            E[c] += e3;
+            G[a] += -dC9a * ang * fd * scale;
+            G[b] += -dC9b * ang * fd * scale;
+            G[c] += -dC9c * ang * fd * scale;
+            double fs = p->atm_force_scaled ? scale : 1.0;
+            double fab = -C9 * (dang_ab * fd - ang * dfd) / ab2;
+            double fac = -C9 * (dang_ac * fd - ang * dfd) / ac2;
+            double fbc = -C9 * (dang_bc * fd - ang * dfd) / bc2;
+            for (int k = 0; k < 3; ++k) {
+                for (int l = 0; l < 3; ++l)
+                    Vv[k * 3 + l] += (-1.0 * fab * rab[k] * rab[l] + -1.0 * fac * rac[k] * rac[l] +
+                                      -1.0 * fbc * rbc[k] * rbc[l]) /
+                                     V * scale;
+                F[3 * a + k] += (fab * rab[k] + fac * rac[k]) * fs;
+                F[3 * b + k] += (-fab * rab[k] + fbc * rbc[k]) * fs;
+                F[3 * c + k] += (-fac * rac[k] - fbc * rbc[k]) * fs;
+            }
+        }
+    }
+}
+
+/* two-body terms of central atom i over its ordered pairs (src/d3_kernel.cu:997-1197):
+   energy (E/2 per ordered pair), dE/dCN_i, force and virial */
+static void twobody_atom(const oracle_params *p, const c6_ctx *cc, int64_t n, const double *pos, const int *types,
+                         const image_set *im, double V, int64_t i, double *e_out, double *g_out, double *f_acc,
+                         double *v_acc) {
+    const double rc2 = p->rc * p->rc, s8 = p->s8, p1 = p->p1, p2 = p->p2;
+    double e_acc = 0, g_acc = 0;
+    for (int k = 0; k < 3; ++k) f_acc[k] = 0;
+    for (int k = 0; k < 9; ++k) v_acc[k] = 0;
+    int ti = types[i];
+    for (int64_t j = 0; j < n; ++j) {
+        int tj = types[j];
+        double c6, d1, d2;
+        pair_c6(cc, i, j, &c6, &d1, &d2);
+        double rr_i = p->r2r4[ti], rr_j = p->r2r4[tj];
+        double c8 = 3.0 * c6 * rr_i * rr_j, dc8 = 3.0 * d1 * rr_i * rr_j;
+        double R0 = p->damping == 1 ? sqrt(3.0 * rr_i * rr_j) : (double)p->r0ab[ti * p->ne + tj];
+        for (int64_t b = 0; b < im->n_img; ++b) {
+            double dx = pos[3 * i] - (pos[3 * j] + im->shift[3 * b]);
+            double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im->shift[3 * b + 1]);
+            double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im->shift[3 * b + 2]);
+            double d2r = dx * dx + dy * dy + dz * dz;
+            if (!(d2r < rc2 && d2r > 0.0)) continue;
+            double r = sqrt(d2r);
+            double r3 = d2r * r, r4 = d2r * d2r, r6 = r3 * r3, r7 = r6 * r, r8 = r4 * r4, r9 = r8 * r, r10 = r6 * r4;
+            double f6, f8, df6, df8;
+            damping(p->damping, r, R0, p1, p2, &f6, &f8, &df6, &df8);
+            double E6 = p->s6 * (c6 / r6) * f6, E8 = s8 * (c8 / r8) * f8;
+            e_acc += (E6 + E8) / 2.0;
+            g_acc += p->s6 * f6 * d1 / r6 + s8 * f8 * dc8 / r8;
+            double fsc = p->s6 * c6 * f6 * (-6.0) / r8 + s8 * c8 * f8 * (-8.0) / r10 + p->s6 * c6 * df6 / r7 +
+                         s8 * c8 * df8 / r9;
+            double d[3] = {dx, dy, dz};
+            for (int k = 0; k < 3; ++k) {
+                f_acc[k] += fsc * d[k];
+                for (int l = 0; l < 3; ++l) v_acc[k * 3 + l] += -1.0 * d[k] * fsc * d[l] / 2.0 / V;
+            }
+        }
+    }
+    *e_out = e_acc;
+    *g_out = g_acc;
+}
+
+/* chain-rule force and virial of atom i (src/d3_kernel.cu:1571-1698); v_acc not yet
+   divided by the volume */
+static void chain_atom(const oracle_params *p, int64_t n, const double *pos, const int *types, const image_set *im,
+                       const double *dedcn, int64_t i, double *f_acc, double *v_acc) {
+    const double rcn2 = p->rc_cn * p->rc_cn;
+    double ri = p->rcov[types[i]], gi = dedcn[i];
+    for (int k = 0; k < 3; ++k) f_acc[k] = 0;
+    for (int k = 0; k < 9; ++k) v_acc[k] = 0;
+    for (int64_t j = 0; j < n; ++j) {
+        double rs = ri + p->rcov[types[j]], g = gi + dedcn[j];
+        for (int64_t b = 0; b < im->n_img; ++b) {
+            double dx = pos[3 * i] - (pos[3 * j] + im->shift[3 * b]);
+            double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im->shift[3 * b + 1]);
+            double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im->shift[3 * b + 2]);
+            double d2r = dx * dx + dy * dy + dz * dz;
+            if (!(d2r <= rcn2 && d2r > 0.0)) continue;
+            double dcn;
+            cn_term(p, sqrt(d2r), rs, &dcn);
+            double dE = g * dcn;
+            double d[3] = {dx, dy, dz};
+            for (int k = 0; k < 3; ++k) {
+                f_acc[k] += dE * d[k];
+                for (int l = 0; l < 3; ++l) v_acc[k * 3 + l] += (-1.0 * d[k] * dE * d[l]) / 2.0;
+            }
+        }
+    }
+}
+
 /*
  * Full evaluation. pos: [n][3] bohr (unwrapped, in the caller's order), types: handle
  * slot per atom, cell: 3x3 rows = lattice vectors (bohr), mcb: image counts per
@@ -263,8 +481,7 @@ int oracle_compute(const oracle_params *p, int64_t n, const double *pos, const i
     image_set im;
     make_images(cell, mcb, &im);
     const double V = cell_volume(cell);
-    const double rc2 = p->rc * p->rc, rcn2 = p->rc_cn * p->rc_cn, ra2 = p->rc_atm * p->rc_atm;
-    const double s8 = p->s8;
+    const double ra2 = p->rc_atm * p->rc_atm;
     int64_t ncent = subset ? n_subset : n;
 
     memset(out->energy, 0, sizeof(double) * n);
@@ -274,24 +491,7 @@ int oracle_compute(const oracle_params *p, int64_t n, const double *pos, const i
 
     /* ---- CN (every atom) ---- */
 #pragma omp parallel for schedule(dynamic, 4)
-    for (int64_t i = 0; i < n; ++i) {
-        double acc = 0;
-        double ri = p->rcov[types[i]];
-        for (int64_t j = 0; j < n; ++j) {
-            double rs = ri + p->rcov[types[j]];
-            for (int64_t b = 0; b < im.n_img; ++b) {
-                double dx = pos[3 * i] - (pos[3 * j] + im.shift[3 * b]);
-                double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im.shift[3 * b + 1]);
-                double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im.shift[3 * b + 2]);
-                double d2 = dx * dx + dy * dy + dz * dz;
-                if (d2 <= rcn2 && d2 > 0.0) {
-                    double dd;
-                    acc += cn_term(p, sqrt(d2), rs, &dd);
-                }
-            }
-        }
-        out->cn[i] = acc;
-    }
+    for (int64_t i = 0; i < n; ++i) out->cn[i] = cn_of_atom(p, n, pos, types, &im, i);
 
     atom_weights *aw = NULL;
     if (p->c6_mode == 1) {
@@ -320,121 +520,19 @@ int oracle_compute(const oracle_params *p, int64_t n, const double *pos, const i
 #endif
             double *E = th_e + (size_t)tid * n, *G = th_g + (size_t)tid * n, *F = th_f + (size_t)tid * n * 3;
             double *Vv = th_v + (size_t)tid * 9;
-            int64_t cap = 1024;
-            int64_t *lj = (int64_t *)malloc(sizeof(int64_t) * cap);
-            double *lv = (double *)malloc(sizeof(double) * 3 * cap);
+            atm_list L = {0, 0, NULL, NULL};
 #pragma omp for schedule(dynamic, 1)
             for (int64_t s = 0; s < ncent; ++s) {
                 int64_t a = subset ? subset[s] : (n - 1 - s);
-                /* L_a: (b, T_b) with b <= a, 1e-12 <= r_ab^2 <= rc_atm^2, ordered by (b, image) */
-                int64_t m = 0;
-                for (int64_t b = 0; b <= a; ++b)
-                    for (int64_t t = 0; t < im.n_img; ++t) {
-                        double px = pos[3 * b] + im.shift[3 * t], py = pos[3 * b + 1] + im.shift[3 * t + 1],
-                               pz = pos[3 * b + 2] + im.shift[3 * t + 2];
-                        double rx = pos[3 * a] - px, ry = pos[3 * a + 1] - py, rz = pos[3 * a + 2] - pz;
-                        double d2 = rx * rx + ry * ry + rz * rz;
-                        if (d2 > ra2 || d2 < 1e-12) continue;
-                        if (m == cap) {
-                            cap *= 2;
-                            lj = (int64_t *)realloc(lj, sizeof(int64_t) * cap);
-                            lv = (double *)realloc(lv, sizeof(double) * 3 * cap);
-                        }
-                        lj[m] = b;
-                        lv[3 * m] = px;
-                        lv[3 * m + 1] = py;
-                        lv[3 * m + 2] = pz;
-                        ++m;
-                    }
-                const double *xa = pos + 3 * a;
-                for (int64_t ib = 0; ib < m; ++ib) {
-                    int64_t b = lj[ib];
-                    double c6ab, dab_a, dab_b;
-                    pair_c6(&cc, a, b, &c6ab, &dab_a, &dab_b);
-                    double r0ab = p->r0ab[types[a] * p->ne + types[b]];
-                    double rab[3] = {xa[0] - lv[3 * ib], xa[1] - lv[3 * ib + 1], xa[2] - lv[3 * ib + 2]};
-                    for (int64_t ic = 0; ic < m; ++ic) {
-                        int64_t c = lj[ic];
-                        if (c > b) break; /* entries are ordered by atom index */
-                        double rac[3] = {xa[0] - lv[3 * ic], xa[1] - lv[3 * ic + 1], xa[2] - lv[3 * ic + 2]};
-                        double rbc[3] = {lv[3 * ib] - lv[3 * ic], lv[3 * ib + 1] - lv[3 * ic + 1],
-                                         lv[3 * ib + 2] - lv[3 * ic + 2]};
-                        double d_ac2 = rac[0] * rac[0] + rac[1] * rac[1] + rac[2] * rac[2];
-                        double d_bc2 = rbc[0] * rbc[0] + rbc[1] * rbc[1] + rbc[2] * rbc[2];
-                        if (d_ac2 > ra2 || d_bc2 > ra2 || d_ac2 < 1e-12 || d_bc2 < 1e-12) continue;
-                        double scale;
-                        if (c == b && b == a)
-                            scale = 1.0 / 6.0;
-                        else if (c == b || c == a || b == a)
-                            scale = 0.5;
-                        else
-                            scale = 1.0;
-                        double c6ac, dac_a, dac_c, c6bc, dbc_b, dbc_c;
-                        pair_c6(&cc, a, c, &c6ac, &dac_a, &dac_c);
-                        pair_c6(&cc, b, c, &c6bc, &dbc_b, &dbc_c);
-                        double r0ac = p->r0ab[types[a] * p->ne + types[c]];
-                        double r0bc = p->r0ab[types[b] * p->ne + types[c]];
-
-                        double ab2 = rab[0] * rab[0] + rab[1] * rab[1] + rab[2] * rab[2];
-                        double ab = sqrt(ab2), ab3 = ab2 * ab, ab4 = ab2 * ab2;
-                        double ac2 = d_ac2, ac = sqrt(ac2), ac3 = ac2 * ac, ac4 = ac2 * ac2;
-                        double bc2 = d_bc2, bc = sqrt(bc2), bc3 = bc2 * bc, bc4 = bc2 * bc2;
-                        double rsq = ab2 * ac2 * bc2, r = sqrt(rsq);
-                        double t1 = ab2 + ac2 - bc2, t2 = ab2 - ac2 + bc2, t3 = -ab2 + ac2 + bc2;
-                        double cosine = t1 * t2 * t3 / (8.0 * rsq);
-                        double ang = (1.0 + 3.0 * cosine) / (rsq * r);
-                        double dang_ab = 3.0 / 8.0 *
-                                         (ab3 * ab3 + ab4 * (ac2 + bc2) + ab2 * (3.0 * bc2 * bc2 + 2.0 * bc2 * ac2 + 3.0 * ac2 * ac2) -
-                                          5.0 * (bc2 - ac2) * (bc2 - ac2) * (bc2 + ac2)) /
-                                         (rsq * rsq * r);
-                        double dang_ac = 3.0 / 8.0 *
-                                         (ac3 * ac3 + ac4 * (bc2 + ab2) + ac2 * (3.0 * bc2 * bc2 + 2.0 * bc2 * ab2 + 3.0 * ab2 * ab2) -
-                                          5.0 * (bc2 - ab2) * (bc2 - ab2) * (bc2 + ab2)) /
-                                         (rsq * rsq * r);
-                        double dang_bc = 3.0 / 8.0 *
-                                         (bc3 * bc3 + bc4 * (ac2 + ab2) + bc2 * (3.0 * ac2 * ac2 + 2.0 * ac2 * ab2 + 3.0 * ab2 * ab2) -
-                                          5.0 * (ac2 - ab2) * (ac2 - ab2) * (ac2 + ab2)) /
-                                         (rsq * rsq * r);
-                        double C9 = -sqrt(c6ab * c6ac * c6bc);
-                        double dC9_ab = -0.5 * C9 / c6ab, dC9_ac = -0.5 * C9 / c6ac, dC9_bc = -0.5 * C9 / c6bc;
-                        double dC9a = dC9_ab * dab_a + dC9_ac * dac_a;
-                        double dC9b = dC9_ab * dab_b + dC9_bc * dbc_b;
-                        double dC9c = dC9_ac * dac_c + dC9_bc * dbc_c;
-                        double ravg = pow(ab2 * ac2 * bc2, 1.0 / 6.0);
-                        double r0 = pow(r0ab * r0ac * r0bc, 1.0 / 3.0);
-                        double x16 = pow(4.0 / 3.0 * r0 / ravg, 16.0);
-                        double fd = 1.0 / (1.0 + 6.0 * x16);
-                        double dfd = 2.0 * 16.0 * x16 * fd * fd;
-                        double e3 = C9 * ang * fd * scale / 3.0;
-                        E[a] += e3;
-                        E[b] += e3;
-                        E[c] += e3;
-                        G[a] += -dC9a * ang * fd * scale;
-                        G[b] += -dC9b * ang * fd * scale;
-                        G[c] += -dC9c * ang * fd * scale;
-                        double fs = p->atm_force_scaled ? scale : 1.0;
-                        double fab = -C9 * (dang_ab * fd - ang * dfd) / ab2;
-                        double fac = -C9 * (dang_ac * fd - ang * dfd) / ac2;
-                        double fbc = -C9 * (dang_bc * fd - ang * dfd) / bc2;
-                        for (int k = 0; k < 3; ++k) {
-                            for (int l = 0; l < 3; ++l)
-                                Vv[k * 3 + l] += (-1.0 * fab * rab[k] * rab[l] + -1.0 * fac * rac[k] * rac[l] +
-                                                  -1.0 * fbc * rbc[k] * rbc[l]) /
-                                                 V * scale;
-                            F[3 * a + k] += (fab * rab[k] + fac * rac[k]) * fs;
-                            F[3 * b + k] += (-fab * rab[k] + fbc * rbc[k]) * fs;
-                            F[3 * c + k] += (-fac * rac[k] - fbc * rbc[k]) * fs;
-                        }
-                    }
-                }
+                atm_list_build(&L, n, pos, &im, ra2, a);
+                atm_apex(p, &cc, pos, types, V, &L, a, E, G, F, Vv);
             }
-            free(lj);
-            free(lv);
+            free(L.lj);
+            free(L.lv);
         }
     }
 
     /* ---- two-body (src/d3_kernel.cu:997-1197) ---- */
-    const double p1 = p->p1, p2 = p->p2;
 #pragma omp parallel
     {
         int tid = 0;
@@ -445,38 +543,8 @@ int oracle_compute(const oracle_params *p, int64_t n, const double *pos, const i
 #pragma omp for schedule(dynamic, 4)
         for (int64_t s = 0; s < ncent; ++s) {
             int64_t i = subset ? subset[s] : s;
-            double e_acc = 0, g_acc = 0, f_acc[3] = {0, 0, 0}, v_acc[9] = {0};
-            int ti = types[i];
-            for (int64_t j = 0; j < n; ++j) {
-                int tj = types[j];
-                double c6, d1, d2;
-                pair_c6(&cc, i, j, &c6, &d1, &d2);
-                double rr_i = p->r2r4[ti], rr_j = p->r2r4[tj];
-                double c8 = 3.0 * c6 * rr_i * rr_j, dc8 = 3.0 * d1 * rr_i * rr_j;
-                double R0 = p->damping == 1 ? sqrt(3.0 * rr_i * rr_j) : (double)p->r0ab[ti * p->ne + tj];
-                for (int64_t b = 0; b < im.n_img; ++b) {
-                    double dx = pos[3 * i] - (pos[3 * j] + im.shift[3 * b]);
-                    double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im.shift[3 * b + 1]);
-                    double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im.shift[3 * b + 2]);
-                    double d2r = dx * dx + dy * dy + dz * dz;
-                    if (!(d2r < rc2 && d2r > 0.0)) continue;
-                    double r = sqrt(d2r);
-                    double r3 = d2r * r, r4 = d2r * d2r, r6 = r3 * r3, r7 = r6 * r, r8 = r4 * r4, r9 = r8 * r,
-                           r10 = r6 * r4;
-                    double f6, f8, df6, df8;
-                    damping(p->damping, r, R0, p1, p2, &f6, &f8, &df6, &df8);
-                    double E6 = p->s6 * (c6 / r6) * f6, E8 = s8 * (c8 / r8) * f8;
-                    e_acc += (E6 + E8) / 2.0;
-                    g_acc += p->s6 * f6 * d1 / r6 + s8 * f8 * dc8 / r8;
-                    double fsc = p->s6 * c6 * f6 * (-6.0) / r8 + s8 * c8 * f8 * (-8.0) / r10 + p->s6 * c6 * df6 / r7 +
-                                 s8 * c8 * df8 / r9;
-                    double d[3] = {dx, dy, dz};
-                    for (int k = 0; k < 3; ++k) {
-                        f_acc[k] += fsc * d[k];
-                        for (int l = 0; l < 3; ++l) v_acc[k * 3 + l] += -1.0 * d[k] * fsc * d[l] / 2.0 / V;
-                    }
-                }
-            }
+            double e_acc, g_acc, f_acc[3], v_acc[9];
+            twobody_atom(p, &cc, n, pos, types, &im, V, i, &e_acc, &g_acc, f_acc, v_acc);
             out->energy[i] += e_acc;
             out->dedcn[i] += g_acc;
             for (int k = 0; k < 3; ++k) out->forces[3 * i + k] += f_acc[k];
@@ -505,26 +573,8 @@ int oracle_compute(const oracle_params *p, int64_t n, const double *pos, const i
 #pragma omp for schedule(dynamic, 4)
         for (int64_t s = 0; s < ncent; ++s) {
             int64_t i = subset ? subset[s] : s;
-            double ri = p->rcov[types[i]], gi = out->dedcn[i];
-            double f_acc[3] = {0, 0, 0}, v_acc[9] = {0};
-            for (int64_t j = 0; j < n; ++j) {
-                double rs = ri + p->rcov[types[j]], g = gi + out->dedcn[j];
-                for (int64_t b = 0; b < im.n_img; ++b) {
-                    double dx = pos[3 * i] - (pos[3 * j] + im.shift[3 * b]);
-                    double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im.shift[3 * b + 1]);
-                    double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im.shift[3 * b + 2]);
-                    double d2r = dx * dx + dy * dy + dz * dz;
-                    if (!(d2r <= rcn2 && d2r > 0.0)) continue;
-                    double dcn;
-                    cn_term(p, sqrt(d2r), rs, &dcn);
-                    double dE = g * dcn;
-                    double d[3] = {dx, dy, dz};
-                    for (int k = 0; k < 3; ++k) {
-                        f_acc[k] += dE * d[k];
-                        for (int l = 0; l < 3; ++l) v_acc[k * 3 + l] += (-1.0 * d[k] * dE * d[l]) / 2.0;
-                    }
-                }
-            }
+            double f_acc[3], v_acc[9];
+            chain_atom(p, n, pos, types, &im, out->dedcn, i, f_acc, v_acc);
             for (int k = 0; k < 3; ++k) out->forces[3 * i + k] += f_acc[k];
             for (int k = 0; k < 9; ++k) Vv[k] += v_acc[k] / V;
         }
@@ -538,6 +588,148 @@ int oracle_compute(const oracle_params *p, int64_t n, const double *pos, const i
     free(th_v);
     free(th_v2);
     free(aw);
+    free(im.shift);
+    return 0;
+}
+
+/*
+ * Per-atom terms of each pass for the atoms subset[0..n_subset), in the column layout
+ * of the engine's diagnostic export (31 doubles per atom, hartree and bohr):
+ *   [0] two-body energy, [1] its dE/dCN, [2..4] force, [5..10] virial (xx yy zz xy xz yz);
+ *   [11] a third of the energy of every triplet whose apex (largest index) is the atom,
+ *   [12] the apex's dE/dCN from those triplets, [13..15] its force from them, [16..21]
+ *   their virial; [22..24] chain-rule force and [25..30] virial given dedcn_in (the
+ *   complete dE/dCN of every atom; skipped when NULL).
+ * cn_out receives the CN of every atom. Used by the parity tests on boxes too large for a
+ * full oracle evaluation.
+ */
+int oracle_terms(const oracle_params *p, int64_t n, const double *pos, const int *types, const double *cell,
+                 const int64_t *mcb, const int64_t *subset, int64_t n_subset, const double *dedcn_in, int nthreads,
+                 double *cn_out, double *terms) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    image_set im;
+    make_images(cell, mcb, &im);
+    const double V = cell_volume(cell);
+    const double ra2 = p->rc_atm * p->rc_atm;
+    static const int vidx[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t i = 0; i < n; ++i) cn_out[i] = cn_of_atom(p, n, pos, types, &im, i);
+    atom_weights *aw = NULL;
+    if (p->c6_mode == 1) {
+        aw = (atom_weights *)malloc(sizeof(atom_weights) * n);
+        for (int64_t i = 0; i < n; ++i) atom_weights_of(p, types[i], cn_out[i], &aw[i]);
+    }
+    c6_ctx cc = {p, aw, types, cn_out};
+    memset(terms, 0, sizeof(double) * 31 * (size_t)n_subset);
+#pragma omp parallel
+    {
+        double *E = (double *)calloc((size_t)n, sizeof(double)), *G = (double *)calloc((size_t)n, sizeof(double));
+        double *F = (double *)calloc((size_t)n * 3, sizeof(double));
+        atm_list L = {0, 0, NULL, NULL};
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t s = 0; s < n_subset; ++s) {
+            const int64_t i = subset[s];
+            double *t = terms + 31 * (size_t)s;
+            double f[3], v[9];
+            twobody_atom(p, &cc, n, pos, types, &im, V, i, &t[0], &t[1], f, v);
+            for (int k = 0; k < 3; ++k) t[2 + k] = f[k];
+            for (int k = 0; k < 6; ++k) t[5 + k] = v[3 * vidx[k][0] + vidx[k][1]];
+            if (p->use_atm) {
+                double Vv[9] = {0};
+                atm_list_build(&L, n, pos, &im, ra2, i);
+                atm_apex(p, &cc, pos, types, V, &L, i, E, G, F, Vv);
+                /* the apex's share, then clear what the apex's triplets touched */
+                double etot = E[i];
+                E[i] = 0;
+                for (int64_t q = 0; q < L.m; ++q) {
+                    const int64_t b = L.lj[q];
+                    etot += E[b];
+                    E[b] = 0;
+                }
+                t[11] = etot / 3.0;
+                t[12] = G[i];
+                for (int k = 0; k < 3; ++k) t[13 + k] = F[3 * i + k];
+                for (int k = 0; k < 6; ++k) t[16 + k] = Vv[3 * vidx[k][0] + vidx[k][1]];
+                G[i] = 0;
+                F[3 * i] = F[3 * i + 1] = F[3 * i + 2] = 0;
+                for (int64_t q = 0; q < L.m; ++q) {
+                    const int64_t b = L.lj[q];
+                    G[b] = 0;
+                    F[3 * b] = F[3 * b + 1] = F[3 * b + 2] = 0;
+                }
+            }
+            if (dedcn_in) {
+                chain_atom(p, n, pos, types, &im, dedcn_in, i, f, v);
+                for (int k = 0; k < 3; ++k) t[22 + k] = f[k];
+                for (int k = 0; k < 6; ++k) t[25 + k] = v[3 * vidx[k][0] + vidx[k][1]] / V;
+            }
+        }
+        free(E);
+        free(G);
+        free(F);
+        free(L.lj);
+        free(L.lv);
+    }
+    free(aw);
+    free(im.shift);
+    return 0;
+}
+
+/*
+ * Exact work counts of the reference's enumeration over every atom (integers):
+ * counts[0] CN ordered pairs (i, j, T) with 0 < r^2 <= rc_CN^2; counts[1] two-body
+ * ordered pairs with 0 < r^2 < rc^2; counts[2] ATM triplets: over every apex a,
+ * unordered pairs of distinct entries of its half list (b <= a, 1e-12 <= r_ab^2 <=
+ * rc_ATM^2) whose own distance is in [1e-12, rc_ATM^2] (0 when ATM is off).
+ */
+int oracle_counts(const oracle_params *p, int64_t n, const double *pos, const double *cell, const int64_t *mcb,
+                  int nthreads, int64_t *counts) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    image_set im;
+    make_images(cell, mcb, &im);
+    const double rc2 = p->rc * p->rc, rcn2 = p->rc_cn * p->rc_cn, ra2 = p->rc_atm * p->rc_atm;
+    int64_t ncn = 0, n2 = 0, n3 = 0;
+#pragma omp parallel for schedule(dynamic, 8) reduction(+ : ncn, n2)
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t j = 0; j < n; ++j)
+            for (int64_t b = 0; b < im.n_img; ++b) {
+                double dx = pos[3 * i] - (pos[3 * j] + im.shift[3 * b]);
+                double dy = pos[3 * i + 1] - (pos[3 * j + 1] + im.shift[3 * b + 1]);
+                double dz = pos[3 * i + 2] - (pos[3 * j + 2] + im.shift[3 * b + 2]);
+                double d2 = dx * dx + dy * dy + dz * dz;
+                ncn += (d2 <= rcn2 && d2 > 0.0);
+                n2 += (d2 < rc2 && d2 > 0.0);
+            }
+    if (p->use_atm) {
+#pragma omp parallel reduction(+ : n3)
+        {
+            atm_list L = {0, 0, NULL, NULL};
+#pragma omp for schedule(dynamic, 1)
+            for (int64_t a = 0; a < n; ++a) {
+                atm_list_build(&L, n, pos, &im, ra2, a);
+                const double *lv = L.lv;
+                for (int64_t ib = 1; ib < L.m; ++ib) {
+                    const double bx = lv[3 * ib], by = lv[3 * ib + 1], bz = lv[3 * ib + 2];
+                    int64_t c = 0;
+                    for (int64_t ic = 0; ic < ib; ++ic) {
+                        double dx = bx - lv[3 * ic], dy = by - lv[3 * ic + 1], dz = bz - lv[3 * ic + 2];
+                        double d2 = dx * dx + dy * dy + dz * dz;
+                        c += (d2 <= ra2 && d2 >= 1e-12);
+                    }
+                    n3 += c;
+                }
+            }
+            free(L.lj);
+            free(L.lv);
+        }
+    }
+    counts[0] = ncn;
+    counts[1] = n2;
+    counts[2] = n3;
     free(im.shift);
     return 0;
 }

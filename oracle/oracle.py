@@ -91,6 +91,10 @@ def _libs():
         vp, i64 = ctypes.c_void_p, ctypes.c_int64
         _lib.oracle_compute.restype = ctypes.c_int
         _lib.oracle_compute.argtypes = [vp, i64, vp, vp, vp, vp, vp, i64, ctypes.c_int, vp]
+        _lib.oracle_terms.restype = ctypes.c_int
+        _lib.oracle_terms.argtypes = [vp, i64, vp, vp, vp, vp, vp, i64, vp, ctypes.c_int, vp, vp]
+        _lib.oracle_counts.restype = ctypes.c_int
+        _lib.oracle_counts.argtypes = [vp, i64, vp, vp, vp, ctypes.c_int, vp]
         _lib.oracle_cell_box.restype = ctypes.c_int
         _lib.oracle_cell_box.argtypes = [vp, ctypes.c_float, ctypes.c_float, vp, vp]
         _lib.oracle_grid_assign.restype = None
@@ -158,19 +162,10 @@ def grid_assign(cell_ang, pos_ang_f32, num_grid):
     return gi, si
 
 
-def compute(pos_ang, elements, cell_ang, rc=95.0, rc_cn=40.0, rc_atm=None, damping=BJ_DAMPING, functional=0,
-            init_elements=None, extended=False, atm_force_scaled=False, c6_mode=0, smooth_cn=False, nthreads=0,
-            subset=None, mcb=None, raw=False):
-    """FP64 oracle evaluation.
-
-    pos_ang: [n,3] Angstrom (converted to bohr in double); cell_ang: 3x3 rows = vectors.
-    Cutoffs in bohr (passed through unconverted, as in the reference ABI).
-    Returns dict with energy (eV), forces (eV/A, caller order), stress (eV/A^3, 3x3),
-    plus cn and dedcn (internal units) and the image box used.
-    """
-    lib, _ = _libs()
+def _setup(pos_ang, elements, cell_ang, rc, rc_cn, rc_atm, damping, functional, init_elements, extended,
+           atm_force_scaled, c6_mode, smooth_cn, mcb):
+    """Per-handle tables, parameter block, bohr positions and cell, image box."""
     pos_ang = np.asarray(pos_ang, np.float64).reshape(-1, 3)
-    n = pos_ang.shape[0]
     elements = [int(z) for z in elements]
     uniq, c6, r0, rcv, rr4 = handle_tables(init_elements if init_elements is not None else elements, extended)
     types = np.array([uniq.index(z) for z in elements], np.int32)
@@ -190,6 +185,25 @@ def compute(pos_ang, elements, cell_ang, rc=95.0, rc_cn=40.0, rc_atm=None, dampi
                   c6_mode=int(c6_mode), smooth_cn=1 if smooth_cn else 0)
     pos = np.ascontiguousarray(pos_ang * ANG2BOHR)
     cell = np.ascontiguousarray(np.asarray(cell_ang, np.float64).reshape(9) * ANG2BOHR)
+    # the arrays the parameter block points into must outlive the call
+    keep = (c6, r0, rcv, rr4)
+    return prm, keep, types, pos, cell, mcb
+
+
+def compute(pos_ang, elements, cell_ang, rc=95.0, rc_cn=40.0, rc_atm=None, damping=BJ_DAMPING, functional=0,
+            init_elements=None, extended=False, atm_force_scaled=False, c6_mode=0, smooth_cn=False, nthreads=0,
+            subset=None, mcb=None, raw=False):
+    """FP64 oracle evaluation.
+
+    pos_ang: [n,3] Angstrom (converted to bohr in double); cell_ang: 3x3 rows = vectors.
+    Cutoffs in bohr (passed through unconverted, as in the reference ABI).
+    Returns dict with energy (eV), forces (eV/A, caller order), stress (eV/A^3, 3x3),
+    plus cn and dedcn (internal units) and the image box used.
+    """
+    lib, _ = _libs()
+    prm, keep, types, pos, cell, mcb = _setup(pos_ang, elements, cell_ang, rc, rc_cn, rc_atm, damping, functional,
+                                              init_elements, extended, atm_force_scaled, c6_mode, smooth_cn, mcb)
+    n = len(types)
     e = np.zeros(n)
     f = np.zeros((n, 3))
     v = np.zeros(9)
@@ -211,3 +225,101 @@ def compute(pos_ang, elements, cell_ang, rc=95.0, rc_cn=40.0, rc_atm=None, dampi
     res["forces"] = f * HARTREE_EV * ANG2BOHR
     res["stress"] = (v * HARTREE_EV * ANG2BOHR ** 3).reshape(3, 3)
     return res
+
+
+def terms(pos_ang, elements, cell_ang, subset, rc=95.0, rc_cn=40.0, rc_atm=None, damping=BJ_DAMPING, functional=0,
+          extended=False, dedcn=None, c6_mode=1, nthreads=0, mcb=None):
+    """Per-pass per-atom terms of the atoms in `subset` ([len(subset), 31], the column
+    layout of the engine's d3_debug_pass_terms, hartree and bohr) and the CN of every
+    atom. dedcn: complete dE/dCN of every atom for the chain-rule columns (else zero)."""
+    lib, _ = _libs()
+    prm, keep, types, pos, cell, mcb = _setup(pos_ang, elements, cell_ang, rc, rc_cn, rc_atm, damping, functional,
+                                              None, extended, False, c6_mode, False, mcb)
+    n = len(types)
+    sub = np.ascontiguousarray(subset, np.int64)
+    cn = np.zeros(n)
+    t = np.zeros((len(sub), 31))
+    g = None if dedcn is None else np.ascontiguousarray(dedcn, np.float64)
+    lib.oracle_terms(ctypes.byref(prm), ctypes.c_int64(n), pos.ctypes.data, types.ctypes.data, cell.ctypes.data,
+                     mcb.ctypes.data, sub.ctypes.data, ctypes.c_int64(len(sub)),
+                     ctypes.c_void_p(None if g is None else g.ctypes.data), ctypes.c_int(nthreads), cn.ctypes.data,
+                     t.ctypes.data)
+    return t, cn
+
+
+def counts(pos_ang, cell_ang, rc=95.0, rc_cn=40.0, rc_atm=None, nthreads=0, mcb=None):
+    """Exact counts of the reference enumeration over every atom: (CN ordered pairs,
+    two-body ordered pairs, ATM triplets)."""
+    lib, _ = _libs()
+    pos_ang = np.asarray(pos_ang, np.float64).reshape(-1, 3)
+    n = pos_ang.shape[0]
+    prm, keep, types, pos, cell, mcb = _setup(pos_ang, [1] * n, cell_ang, rc, rc_cn, rc_atm, BJ_DAMPING, 0, None,
+                                              False, False, 0, False, mcb)
+    out = np.zeros(3, np.int64)
+    lib.oracle_counts(ctypes.byref(prm), ctypes.c_int64(n), pos.ctypes.data, cell.ctypes.data, mcb.ctypes.data,
+                      ctypes.c_int(nthreads), out.ctypes.data)
+    return tuple(int(x) for x in out)
+
+
+def cell_list_pairs(cell_ang, pos_ang, rc, rc_cn, r2max, inclusive):
+    """The pair set of the reference's CELL_LIST path (test infrastructure): the grid of
+    set_cell (counts floor(1 / |row k of the cell inverse| / max(rc, rc_CN)),
+    src/d3_buffer.cu:443-461), atoms wrapped and binned as construct_grids does
+    (:496-634, here through grid_assign), and for each atom the 27 neighbouring grid cells
+    with their periodic shift flags (calculate_neighboring_grids, src/d3_kernel.cu:437-485).
+    Returns the set of (i, j, Tx, Ty, Tz) with 0 < r^2 < r2max (<= when inclusive), T the
+    lattice shift in the positions as given: r = x_i - (x_j + T h)."""
+    mode, mcb, ng = cell_box(cell_ang, rc, rc_cn)
+    if mode != 1:
+        raise ValueError("not a cell-list box (grid %s)" % (ng.tolist(),))
+    pos32 = np.asarray(pos_ang, np.float32).reshape(-1, 3)
+    gi, si = grid_assign(cell_ang, pos32, ng)
+    f = np.float32(1.0) / np.float32(BOHR_ANG)
+    cell = (np.asarray(cell_ang, np.float32).reshape(3, 3) * f).astype(np.float64)
+    pos = (pos32 * f).astype(np.float32).astype(np.float64)
+    wrapped = pos - si @ cell
+    g3 = np.stack([gi % ng[0], (gi // ng[0]) % ng[1], gi // (ng[0] * ng[1])], 1)
+    by_cell = {}
+    for i, g in enumerate(gi.tolist()):
+        by_cell.setdefault(g, []).append(i)
+    out = set()
+    for i in range(len(pos)):
+        for oz in (-1, 0, 1):
+            for oy in (-1, 0, 1):
+                for ox in (-1, 0, 1):
+                    nb = g3[i] + np.array([ox, oy, oz])
+                    S = np.where(nb < 0, -1, np.where(nb >= ng, 1, 0))
+                    nb = nb - S * ng
+                    for j in by_cell.get(int(nb[0] + nb[1] * ng[0] + nb[2] * ng[0] * ng[1]), []):
+                        d = wrapped[i] - (wrapped[j] + S @ cell)
+                        d2 = float(d @ d)
+                        if d2 > 0.0 and (d2 <= r2max if inclusive else d2 < r2max):
+                            T = S + si[i] - si[j]
+                            out.add((i, j, int(T[0]), int(T[1]), int(T[2])))
+    return out
+
+
+def all_pairs(cell_ang, pos_ang, r2max, inclusive, reach=(2, 2, 2), float_input=True):
+    """Every (i, j, T) with 0 < r^2 < r2max (<= when inclusive) over the images
+    T in [-reach, reach] per direction of the positions as given; bohr from Angstrom in
+    float as the reference's float ABI converts them (float_input), else in double as
+    the FP64 oracle does."""
+    if float_input:
+        f = np.float32(1.0) / np.float32(BOHR_ANG)
+        cell = (np.asarray(cell_ang, np.float32).reshape(3, 3) * f).astype(np.float64)
+        pos = (np.asarray(pos_ang, np.float32).reshape(-1, 3) * f).astype(np.float32).astype(np.float64)
+    else:
+        cell = np.asarray(cell_ang, np.float64).reshape(3, 3) * ANG2BOHR
+        pos = np.asarray(pos_ang, np.float64).reshape(-1, 3) * ANG2BOHR
+    reach = np.broadcast_to(np.asarray(reach, int), (3,))
+    T = np.array([(x, y, z) for z in range(-reach[2], reach[2] + 1) for y in range(-reach[1], reach[1] + 1)
+                  for x in range(-reach[0], reach[0] + 1)])
+    sh = T @ cell
+    out = set()
+    for i in range(len(pos)):
+        d = pos[i][None, None, :] - (pos[None, :, :] + sh[:, None, :])
+        d2 = (d * d).sum(-1)
+        ok = (d2 > 0.0) & ((d2 <= r2max) if inclusive else (d2 < r2max))
+        for t, j in zip(*np.nonzero(ok)):
+            out.add((i, int(j), *T[t].tolist()))
+    return out

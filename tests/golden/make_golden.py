@@ -5,7 +5,8 @@ reference library through its C ABI (init_d3_handle[_with_atm], set_atoms, set_c
 compute_dispersion_energy_from_handle_status) and stores inputs and float outputs in
 tests/golden/reference_outputs.npz. Fixtures: the reference's own property-test
 systems (test/d3_test.cpp:343-417) with and without ATM, the 96-atom water box, small
-triclinic boxes of the benchmark generator with the 5- and 7-reference tables.
+triclinic boxes of the benchmark generator with the 5- and 7-reference tables, and two
+low-density boxes on the reference's cell-list path (cubic, and strongly sheared).
 
     python tests/golden/make_golden.py [out.npz]
 """
@@ -46,6 +47,11 @@ def fixtures():
     tric = S.triclinic_box(300, seed=5)
     out.append(("tric300_5ref", tric, dict(rc=60.0, rc_cn=40.0, rc_atm=40.0, damping=1, functional=0)))
     out.append(("tric300_7ref", tric, dict(rc=60.0, rc_cn=40.0, rc_atm=40.0, damping=1, functional=0, extended=True)))
+    # boxes thick enough for the reference's cell-list path (every height above 3 x 95
+    # bohr): cubic, and sheared so that its grid cells along x are thinner than the cutoff
+    cfg = dict(rc=95.0, rc_cn=40.0, rc_atm=40.0, damping=1, functional=0)
+    out.append(("celllist_cubic", S.cell_list_box(400, seed=31, edge=160.0), dict(cfg)))
+    out.append(("celllist_sheared", S.cell_list_box(500, seed=31, edge=250.0, shear=1.0), dict(cfg)))
     return out
 
 

@@ -82,3 +82,33 @@ def test_noalloc_entry_point_rejects_work_beyond_its_bound_before_any_launch():
     cell_ok = (ctypes.c_double * 9)(20.0, 0, 0, 0, 20.0, 0, 0, 0, 20.0)
     assert f(dummy, dummy, 9000, cell_ok, 40.0, 0, dummy, None) == 1
     assert b"exceed the maximum" in lib.d3_last_error()
+
+
+def test_cffi_cdef_keeps_the_reference_signatures():
+    # every function the reference's own cffi binding declares (src/d3_cffi.py:8-45) is
+    # declared with the same parameter types here; skipped where the reference tree is absent
+    import re
+
+    ref = os.environ.get("LASP_D3_REFERENCE", "/root/reference")
+    path = os.path.join(ref, "src", "d3_cffi.py")
+    if not os.path.exists(path):
+        pytest.skip("reference sources not present")
+    pytest.importorskip("cffi")
+    import d3_cffi
+
+    def decls(text):
+        body = re.search(r'cdef\(\s*"""(.*?)"""', text, re.S).group(1)
+        body = re.sub(r"//.*", "", body)
+        out = {}
+        for m in re.finditer(r"([A-Za-z_][\w\s\*]*?)\b(\w+)\s*\(([^)]*)\)\s*;", body):
+            params = [re.sub(r"\s+", " ", p.strip()) for p in m.group(3).split(",")]
+            types = [re.sub(r"\s*\b\w+\s*(\[.*)?$", lambda q: q.group(1) or "", p).replace(" *", "*") for p in params]
+            out[m.group(2)] = (re.sub(r"\s+", " ", m.group(1).strip()), types)
+        return out
+
+    mine = decls(open(d3_cffi.__file__).read())
+    theirs = decls(open(path).read())
+    assert theirs, "no declarations parsed from the reference binding"
+    for name, sig in theirs.items():
+        assert name in mine, name
+        assert mine[name] == sig, (name, mine[name], sig)
