@@ -118,11 +118,14 @@ enum {
     D3_OPT_ATM_CTAS_PER_SM = 6,  /* persistent ATM CTAs per SM (0 = occupancy limit) */
     D3_OPT_ATM_SCHEDULE = 8,     /* precision-form ATM: 0 (default) block pairs, each triplet
                                     visited once; 1 mirror-symmetric, each triplet twice */
-    D3_OPT_ATM_LIST_CAPACITY = 9 /* ATM half-list capacity in entries (0 = estimated from the
+    D3_OPT_ATM_LIST_CAPACITY = 9, /* ATM half-list capacity in entries (0 = estimated from the
                                     density, the default). A synchronous evaluation whose
                                     list overflows grows it and runs again; an asynchronous
                                     one (d3_compute_async, graph replays) sets status bit 0
                                     and leaves the ATM terms out instead */
+    D3_OPT_PAIR_KERNEL = 10      /* two-body pass: 0 (default) compact groups of 32 atoms with
+                                    staged partners; 1 one warp per atom (also used for
+                                    sharded evaluations and handles of more than 8 elements) */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);
 

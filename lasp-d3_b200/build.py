@@ -18,7 +18,7 @@ NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["d3_engine.cu", "d3_noalloc.cu", "d3_mlp.cu"]
 CXX_SOURCES = ["d3_geometry.cpp", "d3_api.cpp"]
-HEADERS = ["d3_engine.h", "d3_geometry.h", "d3_synth_params.h", "d3_mlp.h", "d3_atm.cuh", "d3_atm32.cuh", "d3_atm32b.cuh",
+HEADERS = ["d3_engine.h", "d3_pairs.cuh", "d3_geometry.h", "d3_synth_params.h", "d3_mlp.h", "d3_atm.cuh", "d3_atm32.cuh", "d3_atm32b.cuh",
            "d3_surrogate.cuh"]
 
 

@@ -257,6 +257,13 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
         o.atm_schedule = value;
         break;
     case D3_OPT_ATM_LIST_CAPACITY: o.atm_list_capacity = value < 0 ? 0 : value; break;
+    case D3_OPT_PAIR_KERNEL:
+        if (value != 0 && value != 1) {
+            set_error("D3_OPT_PAIR_KERNEL takes 0 (atom groups) or 1 (one warp per atom)");
+            return 1;
+        }
+        o.pair_kernel = value;
+        break;
     case D3_OPT_PRECISION:
         if (value != 0 && value != 1) {
             set_error("D3_OPT_PRECISION takes 0 (FP64) or 1 (FP32 pair/triplet arithmetic)");

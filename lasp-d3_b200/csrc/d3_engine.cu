@@ -61,6 +61,7 @@ struct SG {
     int half[3];              // image box half-widths
     int atom_base, natoms;    // atom range in caller order
     int st2_off, st2_n, stc_off, stc_n, sta_off, sta_n; // stencil rows (two-body, CN, ATM)
+    int st2b_off, st2b_n;     // two-body stencil of a block of gy x gz bin rows (atom groups)
     int atm_simple;           // every cell height > 2 rc_ATM: no atom twice in an ATM list
 };
 
@@ -131,6 +132,15 @@ struct KP {
     // work counters: [0] ATM in-range visits (2 per triplet), [1] two-body in-range
     // ordered pairs, [2] CN in-range ordered pairs
     unsigned long long *counters;
+    // atom groups of the two-body pass (d3_pairs.cuh): super-rows, groups and their
+    // count, stencil-row slices per group, per-slice partial sums, work counter
+    int *anyshift;           // per structure: some atom was given outside the cell
+    const int4 *srows;
+    int nsrow;
+    int4 *groups;
+    int *gcount, *gwork;
+    int gslices;
+    double *gpart;
 };
 
 __device__ __forceinline__ int floordiv(int a, int b) {
@@ -256,6 +266,7 @@ __global__ void k_bin(KP p) {
         b[k] = min(max(bk, 0), g.nb[k] - 1);
     }
     if (bad) atomicOr(p.status, ST_BAD_INPUT);
+    if ((s[0] | s[1] | s[2]) != 0) atomicOr(&p.anyshift[p.sid_in[i]], 1);
     const int bin = g.bin_base + b[0] + g.nb[0] * (b[1] + g.nb[1] * b[2]);
     double xw = x - (s[0] * g.h[0] + s[1] * g.h[3] + s[2] * g.h[6]);
     double yw = y - (s[0] * g.h[1] + s[1] * g.h[4] + s[2] * g.h[7]);
@@ -876,6 +887,7 @@ __global__ void k_chain32(KP p, const double *Gd) {
     }
 }
 
+#include "d3_pairs.cuh"
 #include "d3_atm.cuh"
 #include "d3_atm32.cuh"
 #include "d3_atm32b.cuh"
@@ -1145,6 +1157,13 @@ struct Engine {
     DBuf<int2> atm_ent;
     long long atm_cap = 0;
     DBuf<int4> st_dev;
+    // two-body atom groups: super-row table (host-built per geometry), groups, counters
+    // ([0] group count, [1] work items taken), per-slice partial sums, per-structure flags
+    std::vector<int4> srow_host;
+    DBuf<int4> srows, groups;
+    DBuf<int> gctl, anyshift;
+    DBuf<double> gpart;
+    size_t group_bound = 0;
     DBuf<double> out;
     DBuf<unsigned int> status;
     DBuf<unsigned long long> counters;
@@ -1158,7 +1177,7 @@ struct Engine {
         const void *fn = nullptr;
         size_t sm = 0;
         int blocks = 1;
-    } atm_occ_cache[5];
+    } atm_occ_cache[8];
     SurrState surr;
     int shard_rank = 0, shard_world = 0; // set by engine_shard_begin
 
@@ -1182,6 +1201,11 @@ struct Engine {
         atm_off.release();
         atm_ent.release();
         st_dev.release();
+        srows.release();
+        groups.release();
+        gctl.release();
+        anyshift.release();
+        gpart.release();
         sg_dev.release();
         status.release();
         counters.release();
@@ -1453,7 +1477,7 @@ static void build_structures(Engine *e, int nstruct, const uint64_t *counts, con
                              const float *cells_f) {
     std::vector<SG> sg(nstruct);
     std::vector<CellGeom> geoms(nstruct);
-    std::vector<int4> rows;
+    std::vector<int4> rows, srow;
     std::vector<int> sid;
     int bin_base = 0, atom_base = 0;
     const double rmin = std::min(e->rc_cn, e->use_atm ? std::min(e->rc, e->rc_atm) : e->rc);
@@ -1494,6 +1518,23 @@ static void build_structures(Engine *e, int nstruct, const uint64_t *counts, con
         add(e->rc, r.st2_off, r.st2_n);
         add(e->rc_cn, r.stc_off, r.stc_n);
         if (e->use_atm) add(e->rc_atm, r.sta_off, r.sta_n);
+        // two-body atom groups: blocks of gy x gz bin rows holding about 16 atoms per
+        // column, so that a group of 32 spans one or two columns
+        {
+            const double per_bin = (double)counts[k] / std::max(1, r.nbins);
+            const int gb = std::max(1, std::min(4, (int)std::lround(std::sqrt(16.0 / std::max(per_bin, 1e-3)))));
+            const int gy = std::min(gb, r.nb[1]), gz = std::min(gb, r.nb[2]);
+            std::vector<StencilRow> s2;
+            for (int q = r.st2_off; q < r.st2_off + r.st2_n; ++q)
+                s2.push_back({rows[q].x, rows[q].y, rows[q].z, rows[q].w});
+            const auto blk = merge_block_stencil(s2, gy, gz);
+            r.st2b_off = (int)rows.size();
+            r.st2b_n = (int)blk.size();
+            for (auto &x : blk) rows.push_back(make_int4(x.dy, x.dz, x.dxlo, x.dxhi));
+            for (int bz = 0; bz < r.nb[2]; bz += gz)
+                for (int by = 0; by < r.nb[1]; by += gy)
+                    srow.push_back(make_int4(k, by, bz, std::min(gy, r.nb[1] - by) | (std::min(gz, r.nb[2] - bz) << 8)));
+        }
         sid.insert(sid.end(), counts[k], k);
     }
     e->sg = sg;
@@ -1502,6 +1543,17 @@ static void build_structures(Engine *e, int nstruct, const uint64_t *counts, con
     e->cells.assign(cells, cells + 9 * (size_t)nstruct);
     e->cells_f.assign(cells_f, cells_f + 9 * (size_t)nstruct);
     e->stencil_rows = rows;
+    e->srow_host = srow;
+    // groups: at most ceil(atoms of a super-row / 32) per super-row
+    e->group_bound = 0;
+    for (int k = 0; k < nstruct; ++k) e->group_bound += counts[k] / 32;
+    e->group_bound += srow.size() + 1;
+    e->srows.ensure(std::max<size_t>(1, srow.size()));
+    if (!srow.empty())
+        D3_CUDA(cudaMemcpy(e->srows.p, srow.data(), sizeof(int4) * srow.size(), cudaMemcpyHostToDevice));
+    e->groups.ensure(e->group_bound);
+    e->gctl.ensure(2);
+    e->anyshift.ensure(std::max(1, nstruct));
     e->nstruct = nstruct;
     e->nbins_total = bin_base;
     e->sg_dev.ensure(nstruct);
@@ -1637,6 +1689,40 @@ static AtmbShape blockpair_shape(const Engine *e) {
 }
 static int blockpair_warps(const Engine *e) { return blockpair_shape(e).warps; }
 
+// the two-body pass on atom groups (d3_pairs.cuh), unless chosen off or the handle has more
+// element types than the staged rows hold; sharded evaluations (which split by central
+// atom) take the per-atom kernels whatever this says
+static bool pairs_grouped(const Engine *e) { return e->opt.pair_kernel == 0 && e->ne <= PAIRS_MAX_TYPES; }
+
+static size_t pairs_smem(const Engine *e) {
+    const bool f64 = e->opt.precision == 0;
+    const size_t rsz = f64 ? sizeof(double) : sizeof(float);
+    const size_t tab = ((size_t)3 * e->ne * e->ne * rsz + 15) & ~(size_t)15;
+    return tab + PAIRS_WARPS * (f64 ? pairs_warp_bytes<true>(e->ne, e->nref) : pairs_warp_bytes<false>(e->ne, e->nref));
+}
+
+static const void *pairs_kernel(const Engine *e) {
+    const bool f64 = e->opt.precision == 0;
+    if (e->nref == 5) return f64 ? (const void *)k_twobody_g<5, true> : (const void *)k_twobody_g<5, false>;
+    return f64 ? (const void *)k_twobody_g<7, true> : (const void *)k_twobody_g<7, false>;
+}
+
+// CTAs per SM of the grouped two-body kernel (attribute and query cached, so that an
+// evaluation inside a graph capture makes no such call)
+static int pairs_occupancy(Engine *e) {
+    auto &c = e->atm_occ_cache[5];
+    const void *fn = pairs_kernel(e);
+    const size_t sm = pairs_smem(e);
+    if (c.fn == fn && c.sm == sm) return c.blocks;
+    D3_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int blocks = 0;
+    D3_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, PAIRS_WARPS * 32, sm));
+    c.fn = fn;
+    c.sm = sm;
+    c.blocks = std::max(1, blocks);
+    return c.blocks;
+}
+
 static KP make_kp(Engine *e) {
     KP p;
     memset(&p, 0, sizeof(p));
@@ -1690,6 +1776,23 @@ static KP make_kp(Engine *e) {
         p.YD32 = e->YD32.p;
     }
     p.atm_force_scaled = e->opt.atm_force_scaled ? 1 : 0;
+    p.anyshift = e->anyshift.p;
+    p.srows = e->srows.p;
+    p.nsrow = (int)e->srow_host.size();
+    p.groups = e->groups.p;
+    p.gcount = e->gctl.p;
+    p.gwork = e->gctl.p + 1;
+    p.gslices = 0;
+    p.gpart = nullptr;
+    if (pairs_grouped(e)) {
+        // slices per group: about six work items per resident warp, so that the items
+        // taken last are short against the pass
+        const int warps = e->dev_sms * pairs_occupancy(e) * PAIRS_WARPS;
+        const long long want = (6LL * warps + (long long)e->group_bound - 1) / std::max<long long>(1, e->group_bound);
+        p.gslices = (int)std::max<long long>(1, std::min<long long>(64, want));
+        e->gpart.ensure((size_t)p.gslices * e->max_atoms * PAIRS_NSUM);
+        p.gpart = e->gpart.p;
+    }
     p.pos_in = e->pos_in.p;
     p.type_in = e->type_in.p;
     p.bin_in = e->bin_in.p;
@@ -1786,6 +1889,7 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
     if (stage != 2) {
         D3_CUDA(cudaEventRecord(ev[0], s));
         D3_CUDA(cudaMemsetAsync(p.counters, 0, sizeof(unsigned long long) * 4, s));
+        D3_CUDA(cudaMemsetAsync(p.anyshift, 0, sizeof(int) * p.nstruct, s));
         D3_CUDA(cudaMemsetAsync(p.bin_cnt, 0, sizeof(int) * p.nbins_total, s));
         D3_CUDA(cudaMemsetAsync(p.bin_fill, 0, sizeof(int) * p.nbins_total, s));
         k_bin<<<gb, T, 0, s>>>(p);
@@ -1807,7 +1911,16 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
             D3_CUDA(cudaMemsetAsync(p.f2, 0, sizeof(double) * 3 * n, s));
             D3_CUDA(cudaMemsetAsync(p.v2, 0, sizeof(double) * 6 * n, s));
         }
-        if (p.precision)
+        if (p.gslices > 0 && p.shard_world <= 1) {
+            D3_CUDA(cudaMemsetAsync(e->gctl.p, 0, 2 * sizeof(int), s));
+            k_groups<<<(p.nsrow + 127) / 128, 128, 0, s>>>(p);
+            const int grid = e->dev_sms * pairs_occupancy(e);
+            if (p.precision)
+                k_twobody_g<NR, false><<<grid, PAIRS_WARPS * 32, pairs_smem(e), s>>>(p);
+            else
+                k_twobody_g<NR, true><<<grid, PAIRS_WARPS * 32, pairs_smem(e), s>>>(p);
+            k_pairs_reduce<<<gb, T, 0, s>>>(p);
+        } else if (p.precision)
             k_twobody32<NR><<<gw, T, (size_t)p.ne * p.ne * sizeof(float4), s>>>(p);
         else
             k_twobody<NR><<<gw, T, 0, s>>>(p);
@@ -1933,9 +2046,10 @@ int engine_pass_times(Engine *e, float *ms, int cap, unsigned long long *counter
 }
 
 int engine_launches_per_eval(const Engine *e) {
-    if (!e->use_atm) return 12;
-    if (e->opt.atm_surrogate && e->surr.loaded) return 20;
-    return blockpair_warps(e) > 0 ? 17 : 16;
+    const int pairs = pairs_grouped(e) ? 2 : 0; // group cut and slice reduction
+    if (!e->use_atm) return 12 + pairs;
+    if (e->opt.atm_surrogate && e->surr.loaded) return 20 + pairs;
+    return (blockpair_warps(e) > 0 ? 17 : 16) + pairs;
 }
 
 // Accuracy check of the Newton-refined helpers used by the ATM kernel against CUDA's

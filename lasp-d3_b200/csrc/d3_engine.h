@@ -53,6 +53,8 @@ struct Options {
                                    // 1 mirror-symmetric full square (each triplet twice)
     long long atm_list_capacity = 0; // ATM half-list entries to allocate (0: estimate from the
                                      // density); a synchronous evaluation regrows on overflow
+    int pair_kernel = 0;           // two-body pass: 0 atom groups with staged partners,
+                                   // 1 one warp per atom
 };
 
 // Learned ATM surrogate: network parameters and normalisation (network in d3_mlp.h).

@@ -1,9 +1,11 @@
+#include <map>
 // Host-side cell geometry (see d3_geometry.h).
 #include "d3_geometry.h"
 
 #include <algorithm>
 #include <cmath>
 #include <limits>
+#include <map>
 
 namespace d3 {
 
@@ -164,6 +166,26 @@ std::vector<StencilRow> build_stencil(const CellGeom &g, const int nb[3], double
             if (lo <= hi) rows.push_back({dy, dz, lo, hi});
         }
     return rows;
+}
+
+std::vector<StencilRow> merge_block_stencil(const std::vector<StencilRow> &st, int gy, int gz) {
+    std::map<std::pair<int, int>, std::pair<int, int>> m; // (dz, dy) -> (lo, hi)
+    for (int oz = 0; oz < gz; ++oz)
+        for (int oy = 0; oy < gy; ++oy)
+            for (const StencilRow &r : st) {
+                const auto key = std::make_pair(r.dz + oz, r.dy + oy);
+                auto it = m.find(key);
+                if (it == m.end())
+                    m.emplace(key, std::make_pair(r.dxlo, r.dxhi));
+                else {
+                    it->second.first = std::min(it->second.first, r.dxlo);
+                    it->second.second = std::max(it->second.second, r.dxhi);
+                }
+            }
+    std::vector<StencilRow> out;
+    out.reserve(m.size());
+    for (const auto &kv : m) out.push_back({kv.first.second, kv.first.first, kv.second.first, kv.second.second});
+    return out;
 }
 
 } // namespace d3

@@ -35,4 +35,9 @@ void choose_bins(const CellGeom &g, double target_width, int64_t max_bins, int n
 // compressed into x-rows. Exact convex-QP distance between parallelepiped bins.
 std::vector<StencilRow> build_stencil(const CellGeom &g, const int nb[3], double r);
 
+// Stencil of a block of gy x gz bin rows (offsets relative to the block's first row): for
+// every row offset the union of the x ranges its member rows need (the block's own x
+// extent is added at run time). Each row offset appears once.
+std::vector<StencilRow> merge_block_stencil(const std::vector<StencilRow> &st, int gy, int gz);
+
 } // namespace d3

@@ -1,0 +1,332 @@
+// Two-body pass on spatially compact atom groups (included by d3_engine.cu after the
+// per-atom pair kernels; replaces the reference's two_body_kernel, src/d3_kernel.cu:997-1197).
+//
+// Groups. The bins of a structure are taken in super-rows of gy x gz bin rows (y, z);
+// within a super-row the atoms are ordered column by column along x (column = the gy gz
+// bins of one x index) and cut into consecutive groups of 32. A group is therefore a
+// compact block of about 32 atoms (2 x 2 rows and one or two columns for the benchmark
+// box) whose candidate partners are given by one merged stencil: for every row offset
+// (dy, dz) relative to the super-row's first row, the union of the x ranges its member
+// rows need, widened by the group's own x extent. Every candidate (j, image) appears once
+// in that stencil, so a distance test per (i, j) pair is the only filter.
+//
+// Work. A work item is (group, slice of the stencil rows): one warp, lane L owns the
+// group's atom L, partners are staged 32 at a time in the warp's shared memory (position
+// and the C6 rows of the partner at every type: lanes of different types read distinct
+// banks, lanes of one type the same word) and visited by all lanes together. Items are
+// taken from a counter by persistent warps. Each item writes its lanes' sums (energy,
+// dE/dCN, force, virial) to its slice's row of a partial array; k_pairs_reduce adds the
+// slices of every atom in a fixed order, so results do not depend on scheduling.
+
+constexpr int PAIRS_MAX_TYPES = 8;    // staged C6 rows per partner: ne * NR values
+constexpr int PAIRS_WARPS = 8;        // warps per CTA
+constexpr int PAIRS_NSUM = 11;        // e, g, f[3], v[6] per atom and slice
+
+// one super-row: structure, first bin row (y, z) and its row counts (ny | nz << 8)
+// one group:     super-row, bx_lo | bx_hi << 16, position of the first atom in column
+//                bx_lo's atom sequence, atom count (<= 32)
+
+// Cut the super-rows into groups (one thread per super-row).
+__global__ void k_groups(KP p) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= p.nsrow) return;
+    const int4 sr = p.srows[r];
+    const SG &g = p.sg[sr.x];
+    const int ny = sr.w & 0xff, nz = (sr.w >> 8) & 0xff;
+    const int *bs = p.bin_start + g.bin_base;
+    int lo = 0, skip = 0, cnt = 0, last = 0;
+    for (int bx = 0; bx < g.nb[0]; ++bx) {
+        int c = 0;
+        for (int oz = 0; oz < nz; ++oz)
+            for (int oy = 0; oy < ny; ++oy) {
+                const int rb = g.nb[0] * ((sr.y + oy) + g.nb[1] * (sr.z + oz));
+                c += bs[rb + bx + 1] - bs[rb + bx];
+            }
+        int used = 0;
+        while (used < c) {
+            if (cnt == 0) {
+                lo = bx;
+                skip = used;
+            }
+            const int take = min(32 - cnt, c - used);
+            cnt += take;
+            used += take;
+            last = bx;
+            if (cnt == 32) {
+                const int slot = atomicAdd(p.gcount, 1);
+                p.groups[slot] = make_int4(r, lo | (bx << 16), skip, 32);
+                cnt = 0;
+            }
+        }
+    }
+    if (cnt > 0) {
+        const int slot = atomicAdd(p.gcount, 1);
+        p.groups[slot] = make_int4(r, lo | (last << 16), skip, cnt);
+    }
+}
+
+// binned index of atom q (0-based, q < group count) of a group
+__device__ __forceinline__ int group_atom(const KP &p, const SG &g, int4 sr, int bx_lo, int skip, int q) {
+    const int ny = sr.w & 0xff, nz = (sr.w >> 8) & 0xff;
+    const int *bs = p.bin_start + g.bin_base;
+    q += skip;
+    for (int bx = bx_lo; bx < g.nb[0]; ++bx)
+        for (int oz = 0; oz < nz; ++oz)
+            for (int oy = 0; oy < ny; ++oy) {
+                const int b = g.nb[0] * ((sr.y + oy) + g.nb[1] * (sr.z + oz)) + bx;
+                const int c = bs[b + 1] - bs[b];
+                if (q < c) return bs[b] + q;
+                q -= c;
+            }
+    return -1;
+}
+
+template <bool F64>
+struct PairReal;
+template <>
+struct PairReal<false> {
+    using R = float;
+    using R4 = float4;
+};
+template <>
+struct PairReal<true> {
+    using R = double;
+    using R4 = double4;
+};
+
+// One (i, j) pair of the two-body term: energy (half), dE/dCN_i, force scalar fs with
+// F_i += fs r_ij and virial += fs r_ij (x) r_ij. y: partner's C6 row at the type of i.
+template <int NR, typename R>
+__device__ __forceinline__ void pair_term(const KP &p, R r2, const R *y, const R *wi, const R *dwi, R A6_or_R0,
+                                          R A8, R rr, R &e_half, R &G, R &fs) {
+    R c6 = 0, dc6 = 0;
+#pragma unroll
+    for (int b = 0; b < NR; ++b) {
+        c6 = fma(y[b], wi[b], c6);
+        dc6 = fma(y[b], dwi[b], dc6);
+    }
+    const R c8 = c6 * rr, dc8 = dc6 * rr;
+    const R s6 = (R)p.s6, s8 = (R)p.s8;
+    R E6, E8;
+    if (p.damping == 1) {
+        const R r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
+        R i6, i8;
+        if constexpr (sizeof(R) == 4) {
+            i6 = __fdividef(1.0f, r6 + A6_or_R0);
+            i8 = __fdividef(1.0f, r8 + A8);
+        } else {
+            i6 = 1.0 / (r6 + A6_or_R0);
+            i8 = 1.0 / (r8 + A8);
+        }
+        E6 = s6 * c6 * i6;
+        E8 = s8 * c8 * i8;
+        G = s6 * dc6 * i6 + s8 * dc8 * i8;
+        fs = (R)-6 * E6 * r4 * i6 - (R)8 * E8 * r6 * i8;
+    } else {
+        R ir;
+        if constexpr (sizeof(R) == 4)
+            ir = rsqrtf(r2);
+        else
+            ir = 1.0 / sqrt(r2);
+        const R ir2 = ir * ir, ir6 = ir2 * ir2 * ir2, ir8 = ir6 * ir2;
+        const R R0 = A6_or_R0;
+        const R x6 = (R)p.p1 * R0 * ir, x8 = (R)p.p2 * R0 * ir;
+        const R x6_2 = x6 * x6, x6_4 = x6_2 * x6_2, x6_8 = x6_4 * x6_4, x6_14 = x6_8 * x6_4 * x6_2;
+        const R x8_2 = x8 * x8, x8_4 = x8_2 * x8_2, x8_8 = x8_4 * x8_4, x8_16 = x8_8 * x8_8;
+        R f6, f8;
+        if constexpr (sizeof(R) == 4) {
+            f6 = __fdividef(1.0f, fmaf(6.0f, x6_14, 1.0f));
+            f8 = __fdividef(1.0f, fmaf(6.0f, x8_16, 1.0f));
+        } else {
+            f6 = 1.0 / (1.0 + 6.0 * x6_14);
+            f8 = 1.0 / (1.0 + 6.0 * x8_16);
+        }
+        const R df6 = (R)84 * f6 * f6 * x6_14 * ir, df8 = (R)96 * f8 * f8 * x8_16 * ir;
+        E6 = s6 * c6 * f6 * ir6;
+        E8 = s8 * c8 * f8 * ir8;
+        G = s6 * f6 * dc6 * ir6 + s8 * f8 * dc8 * ir8;
+        fs = s6 * c6 * ((R)-6 * f6 * ir8 + df6 * ir6 * ir) + s8 * c8 * ((R)-8 * f8 * ir8 * ir2 + df8 * ir8 * ir);
+    }
+    e_half = (R)0.5 * (E6 + E8);
+}
+
+// shared memory of one warp: 32 partner positions and their C6 rows at every type
+template <bool F64>
+__host__ __device__ constexpr size_t pairs_warp_bytes(int ne, int NR) {
+    return 32 * (F64 ? sizeof(double4) : sizeof(float4)) + (size_t)32 * ne * NR * (F64 ? sizeof(double) : sizeof(float));
+}
+
+template <int NR, bool F64>
+__global__ void __launch_bounds__(PAIRS_WARPS * 32) k_twobody_g(KP p) {
+    using R = typename PairReal<F64>::R;
+    using R4 = typename PairReal<F64>::R4;
+    extern __shared__ __align__(16) unsigned char smp[];
+    const int ne = p.ne;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // per type pair: BJ A^6, A^8 (zero damping: R0) and 3 r2r4_i r2r4_j
+    R *ptab = reinterpret_cast<R *>(smp);
+    for (int k = threadIdx.x; k < ne * ne; k += blockDim.x) {
+        const double *pa = p.pairA + (size_t)k * 4;
+        ptab[3 * k] = (R)pa[0];
+        ptab[3 * k + 1] = (R)pa[1];
+        ptab[3 * k + 2] = (R)(3.0 * p.r2r4[k / ne] * p.r2r4[k % ne]);
+    }
+    __syncthreads();
+    const size_t tab_bytes = ((size_t)3 * ne * ne * sizeof(R) + 15) & ~(size_t)15;
+    unsigned char *wb = smp + tab_bytes + (size_t)warp * pairs_warp_bytes<F64>(ne, NR);
+    R4 *sP = reinterpret_cast<R4 *>(wb);
+    R *sY = reinterpret_cast<R *>(wb + 32 * sizeof(R4));
+    const R4 *xsrc = F64 ? reinterpret_cast<const R4 *>(p.xs) : reinterpret_cast<const R4 *>(p.xs32);
+    const R *Ysrc = F64 ? reinterpret_cast<const R *>(p.Y) : reinterpret_cast<const R *>(p.Y32);
+    const R *wsrc = F64 ? reinterpret_cast<const R *>(p.w) : reinterpret_cast<const R *>(p.w32);
+    const R *dwsrc = F64 ? reinterpret_cast<const R *>(p.dw) : reinterpret_cast<const R *>(p.dw32);
+    const int rowlen = ne * NR;
+    const R rc2 = (R)p.rc2;
+    const int S = p.gslices;
+    const int items = *p.gcount * S;
+    unsigned long long npair = 0;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(p.gwork, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= items) break;
+        const int gi = it / S, sl = it - gi * S;
+        const int4 grp = p.groups[gi];
+        const int4 sr = p.srows[grp.x];
+        const SG &g = p.sg[sr.x];
+        const int bx_lo = grp.y & 0xffff, bx_hi = grp.y >> 16;
+        const int i = lane < grp.w ? group_atom(p, g, sr, bx_lo, grp.z, lane) : -1;
+        const bool iv = i >= 0;
+        R4 xi;
+        int ti = 0;
+        R wi[NR], dwi[NR];
+        int4 si = make_int4(0, 0, 0, 0);
+        if (iv) {
+            xi = xsrc[i];
+            ti = (int)xi.w;
+            si = p.shift[i];
+#pragma unroll
+            for (int b = 0; b < NR; ++b) {
+                wi[b] = wsrc[(size_t)i * NR + b];
+                dwi[b] = dwsrc[(size_t)i * NR + b];
+            }
+        } else {
+            xi.x = xi.y = xi.z = (R)0;
+            xi.w = (R)0;
+#pragma unroll
+            for (int b = 0; b < NR; ++b) wi[b] = dwi[b] = (R)0;
+        }
+        // exact image-box test per pair only when atoms were given outside the cell
+        const bool box_pair = g.box_mode && p.anyshift[sr.x];
+        double E = 0, Gd = 0, FX = 0, FY = 0, FZ = 0, V[6] = {0, 0, 0, 0, 0, 0};
+        const int nb0 = g.nb[0], nb1 = g.nb[1], nb2 = g.nb[2];
+        const int *bstart = p.bin_start + g.bin_base;
+        const int4 *rows = p.stencils + g.st2b_off;
+        for (int r = sl; r < g.st2b_n; r += S) {
+            const int4 row = rows[r];
+            const int yy = sr.y + row.x, zz = sr.z + row.y;
+            const int Ty = floordiv(yy, nb1), Tz = floordiv(zz, nb2);
+            const int byy = yy - Ty * nb1, bzz = zz - Tz * nb2;
+            const int xlo = bx_lo + row.z, xhi = bx_hi + row.w;
+            const int plo = floordiv(xlo, nb0), phi = floordiv(xhi, nb0);
+            const int rowbase = nb0 * (byy + nb1 * bzz);
+            for (int px = plo; px <= phi; ++px) {
+                if (g.box_mode && !box_pair &&
+                    (abs(px) > g.half[0] || abs(Ty) > g.half[1] || abs(Tz) > g.half[2]))
+                    continue; // outside the reference's image box for every pair of the range
+                const int a = max(xlo, px * nb0) - px * nb0;
+                const int b = min(xhi, px * nb0 + nb0 - 1) - px * nb0;
+                const int jlo = bstart[rowbase + a], jhi = bstart[rowbase + b + 1];
+                if (jlo >= jhi) continue;
+                const double shx = px * g.h[0] + Ty * g.h[3] + Tz * g.h[6];
+                const double shy = px * g.h[1] + Ty * g.h[4] + Tz * g.h[7];
+                const double shz = px * g.h[2] + Ty * g.h[5] + Tz * g.h[8];
+                // origin of this range: x_i - T h (rounded once)
+                const R ox = (R)((double)xi.x - shx), oy = (R)((double)xi.y - shy), oz = (R)((double)xi.z - shz);
+                for (int base = jlo; base < jhi; base += 32) {
+                    const int m = min(32, jhi - base);
+                    __syncwarp();
+                    if (lane < m) sP[lane] = xsrc[base + lane];
+                    {
+                        const R *src = Ysrc + (size_t)base * rowlen;
+                        const int tot = m * rowlen;
+                        for (int k = lane; k < tot; k += 32) sY[k] = src[k];
+                    }
+                    __syncwarp();
+                    R e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+                    for (int jj = 0; jj < m; ++jj) {
+                        const R4 xj = sP[jj];
+                        const R dx = ox - xj.x, dy = oy - xj.y, dz = oz - xj.z;
+                        const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                        bool act = iv && r2 < rc2 && r2 > (R)0;
+                        if (box_pair && act) act = in_box(g, si, p.shift[base + jj], px, Ty, Tz);
+                        if (!act) continue;
+                        ++npair;
+                        const int tj = (int)xj.w;
+                        const R *tp = ptab + 3 * (ti * ne + tj);
+                        R eh, Gt, fs;
+                        pair_term<NR, R>(p, r2, sY + jj * rowlen + ti * NR, wi, dwi, tp[0], tp[1], tp[2], eh, Gt, fs);
+                        e += eh;
+                        Gd += (double)Gt;
+                        fx = fma(fs, dx, fx);
+                        fy = fma(fs, dy, fy);
+                        fz = fma(fs, dz, fz);
+                        const R fdx = fs * dx, fdy = fs * dy;
+                        vxx = fma(fdx, dx, vxx);
+                        vyy = fma(fdy, dy, vyy);
+                        vzz = fma(fs * dz, dz, vzz);
+                        vxy = fma(fdx, dy, vxy);
+                        vxz = fma(fdx, dz, vxz);
+                        vyz = fma(fdy, dz, vyz);
+                    }
+                    // blocked summation: 32-partner sums carried in FP64
+                    E += e;
+                    FX += fx;
+                    FY += fy;
+                    FZ += fz;
+                    V[0] += vxx;
+                    V[1] += vyy;
+                    V[2] += vzz;
+                    V[3] += vxy;
+                    V[4] += vxz;
+                    V[5] += vyz;
+                }
+            }
+        }
+        if (iv) {
+            double *o = p.gpart + ((size_t)sl * p.n + i) * PAIRS_NSUM;
+            o[0] = E;
+            o[1] = Gd;
+            o[2] = FX;
+            o[3] = FY;
+            o[4] = FZ;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) o[5 + k] = V[k];
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+    if (lane == 0 && npair) atomicAdd(&p.counters[1], npair);
+}
+
+// per atom: the slices' sums in a fixed order -> two-body energy, dE/dCN, force, virial
+__global__ void k_pairs_reduce(KP p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.n) return;
+    double acc[PAIRS_NSUM];
+#pragma unroll
+    for (int k = 0; k < PAIRS_NSUM; ++k) acc[k] = 0.0;
+    for (int s = 0; s < p.gslices; ++s) {
+        const double *o = p.gpart + ((size_t)s * p.n + i) * PAIRS_NSUM;
+#pragma unroll
+        for (int k = 0; k < PAIRS_NSUM; ++k) acc[k] += o[k];
+    }
+    p.e2[i] = acc[0];
+    p.g2[i] = acc[1];
+    p.f2[3 * i] = acc[2];
+    p.f2[3 * i + 1] = acc[3];
+    p.f2[3 * i + 2] = acc[4];
+    const double sc = -1.0 / (2.0 * p.sg[p.sid[i]].vol);
+    double *v = p.v2 + 6 * (size_t)i;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v[k] = acc[5 + k] * sc;
+}

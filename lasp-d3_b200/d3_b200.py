@@ -26,6 +26,7 @@ OPT_BIN_DIVISOR, OPT_ATM_TILE, OPT_ATM_CTAS_PER_SM = 4, 5, 6
 OPT_ATM_SURROGATE = 7
 OPT_ATM_SCHEDULE = 8
 OPT_ATM_LIST_CAPACITY = 9
+OPT_PAIR_KERNEL = 10
 TABLE_5REF, TABLE_7REF = 0, 1
 
 _lib = None
