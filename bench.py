@@ -166,6 +166,16 @@ def run_cpu_baseline(sys_, sample=48, seed=7, rc_atm=RC_ATM, extended=False):
                       "atoms/s = 1 / (t_sample/%d + t_cn/%d)" % (n, t_cn, sample, t_sub, sample, n)}
 
 
+def apply_options(handle, args):
+    """--option NAME=VALUE: engine options (d3_b200.OPT_*) set on a handle."""
+    import d3_b200
+
+    for kv in args.option:
+        name, val = kv.split("=")
+        key = name if name.startswith("OPT_") else "OPT_" + name.upper()
+        handle.set_option(getattr(d3_b200, key), int(val))
+
+
 def time_form(d, args, flush, stream, barrier):
     """Warm-up and K timed evaluations of one engine handle on `stream` (device time by
     CUDA events, L2 flushed between steps). Returns per-step ms, ATM ms, passes, counters."""
@@ -240,6 +250,7 @@ def engine_arm(args, world, rank, local):
     sampler.start()
     for form, prec in (("plain", 0), ("precision", 1)):
         d = D3(sys_["Z"], n, rc=RC, rc_cn=RC_CN, rc_atm=rc_atm, damping=1, functional=0, table=table)
+        apply_options(d, args)
         d.set_option(OPT_PRECISION, prec)
         d.set_cell(sys_["cell"])
         d.set_atoms(sys_["pos"], sys_["Z"])
@@ -281,6 +292,11 @@ def engine_arm(args, world, rank, local):
         h = lib.init_d3_handle_with_atm(z16.ctypes.data, n, n, RC, RC_CN, RC_ATM, 1, 0)
     else:
         h = lib.init_d3_handle(z16.ctypes.data, n, n, RC, RC_CN, 1, 0)
+    import d3_b200
+
+    for kv in args.option:
+        name, val = kv.split("=")
+        lib.d3_set_option(h, getattr(d3_b200, name if name.startswith("OPT_") else "OPT_" + name.upper()), int(val))
     lib.d3_set_option(h, OPT_PRECISION, 1 if chosen == "precision" else 0)
     lib.set_cell(h, cellf.ctypes.data)
     ef = np.zeros(1, np.float32)
@@ -347,7 +363,7 @@ def engine_arm(args, world, rank, local):
             "config": workload_config(n, "%s form (%s)" % (chosen, "FP64 throughout" if fp64 else
                                                          "FP32 pair/triplet arithmetic, FP64 C6 weights, dE/dCN "
                                                          "and reductions"), args),
-            "chosen_form": chosen, "forms": forms_out,
+            "chosen_form": chosen, "forms": forms_out, "options": args.option,
             "roofline": roofline, "e2e": e2e, "gpu_launches": ch["launches"] * args.steps, "clocks": clocks,
             "counters": {"atm_triplets": triplets, "twobody_ordered_pairs": int(ch["counters"][1]),
                          "cn_ordered_pairs": int(ch["counters"][2])}}
@@ -502,7 +518,7 @@ def batch_mode(args):
         t.set_option(OPT_PRECISION, prec)
         t.set_structures(sub)
         key = d3_autotune.workload_key(ntot / len(sts), vol / len(sts), RC, RC_CN, RC_ATM, prec) + "|batch"
-        tuned = d3_autotune.tune(t, key, repeats=1)
+        tuned = d3_autotune.tune(t, key, repeats=1, precision=bool(prec))
         t.close()
         b = D3Batch(elements, len(sts), ntot, rc=RC, rc_cn=RC_CN, rc_atm=RC_ATM, damping=1, functional=0)
         b.set_option(OPT_PRECISION, prec)
@@ -548,7 +564,7 @@ def md_mode(args):
     d.set_cell(sys_["cell"])
     d.set_atoms(sys_["pos"], sys_["Z"])
     vol = abs(np.linalg.det(sys_["cell"]))
-    tuned = d3_autotune.tune(d, d3_autotune.workload_key(n, vol, RC, RC_CN, RC_ATM, 1), repeats=1)
+    tuned = d3_autotune.tune(d, d3_autotune.workload_key(n, vol, RC, RC_CN, RC_ATM, 1), repeats=1, precision=True)
     d.compute()  # list capacity for the trajectory (the list grows on overflow only outside capture)
     pos = torch.tensor(sys_["pos"], dtype=torch.float64, device="cuda")
     noise = torch.empty_like(pos)
@@ -689,6 +705,8 @@ def main():
     ap.add_argument("--batch", type=int, default=2048)
     ap.add_argument("--tune-structs", type=int, default=128)
     ap.add_argument("--md-steps", type=int, default=200)
+    ap.add_argument("--option", action="append", default=[], metavar="NAME=VALUE",
+                    help="engine option for every handle of the run (name as in d3_b200: OPT_..., repeatable)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.mode in ("batch", "md"):

@@ -123,9 +123,17 @@ enum {
                                     list overflows grows it and runs again; an asynchronous
                                     one (d3_compute_async, graph replays) sets status bit 0
                                     and leaves the ATM terms out instead */
-    D3_OPT_PAIR_KERNEL = 10      /* two-body pass: 0 (default) compact groups of 32 atoms with
-                                    staged partners; 1 one warp per atom (also used for
-                                    sharded evaluations and handles of more than 8 elements) */
+    D3_OPT_PAIR_KERNEL = 10,     /* two-body pass: 0 (default) compact groups of 32 atoms with
+                                    staged partners (one thread per atom); 1 one warp per atom
+                                    (also used for sharded evaluations and handles of more
+                                    than 8 elements) */
+    D3_OPT_ATMB_WARPS = 11,      /* precision-form block-pair ATM kernel: warps per CTA, 0 =
+                                    automatic (8), 2..12; above 8 each warp stages one y
+                                    block at a time instead of two. With
+                                    D3_OPT_ATM_CTAS_PER_SM = 2, two CTAs per SM when they fit */
+    D3_OPT_ATMB_LIST_CAPACITY = 12 /* longest half list (entries) the block-pair kernel takes,
+                                    0 = as many as the shared memory allows (4,096..8,192);
+                                    longer lists go to the mirror-symmetric kernel */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);
 

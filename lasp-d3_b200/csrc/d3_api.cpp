@@ -257,6 +257,14 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
         o.atm_schedule = value;
         break;
     case D3_OPT_ATM_LIST_CAPACITY: o.atm_list_capacity = value < 0 ? 0 : value; break;
+    case D3_OPT_ATMB_WARPS:
+        if (value < 0 || value > 12) {
+            set_error("D3_OPT_ATMB_WARPS takes 0 (automatic) or 2..12");
+            return 1;
+        }
+        o.atmb_warps = value;
+        break;
+    case D3_OPT_ATMB_LIST_CAPACITY: o.atmb_mcap = value < 0 ? 0 : value; break;
     case D3_OPT_PAIR_KERNEL:
         if (value != 0 && value != 1) {
             set_error("D3_OPT_PAIR_KERNEL takes 0 (atom groups) or 1 (one warp per atom)");

@@ -43,7 +43,9 @@
 // 512 in [ATMB_MCAP_MIN, ATMB_MCAP_MAX], as large as the shared memory left by the warps allows
 constexpr int ATMB_MCAP_MIN = 4096, ATMB_MCAP_MAX = 8192;
 constexpr int ATMB_GRID = 8;      // spatial grid per dimension for the entry sort
-constexpr int ATMB_MAXW = 8;      // warps per CTA at most
+constexpr int ATMB_MAXW = 8;      // warps per CTA at most with two y buffers per warp
+constexpr int ATMB_MAXW1 = 12;    // warps per CTA at most with one y buffer per warp (168
+                                  // registers per thread: three warps per scheduler)
 constexpr int ATMB_CTAS_PER_SM = 2; // preferred CTAs per SM (of four warps each)
 
 // global scratch per CTA (float4 units): per-entry records sA, sB, sJ and the per-entry
@@ -68,8 +70,8 @@ __host__ __device__ inline size_t atmb_buf_quads(int ne, int NR) { return 32 * (
 // and the current block's positions / per-entry constants with entries k, k + 1 side by
 // side ([4][32] float4)
 constexpr int ATMB_NCARRY = 19;
-__host__ __device__ inline size_t atmb_smem_warp(int ne, int NR) {
-    return 2 * atmb_buf_quads(ne, NR) * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double) + 4 * 32 * sizeof(float4);
+__host__ __device__ inline size_t atmb_smem_warp(int ne, int NR, int nbuf = 2) {
+    return nbuf * atmb_buf_quads(ne, NR) * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double) + 4 * 32 * sizeof(float4);
 }
 
 // a lane's view of FP64 carries kept in shared memory ([q][32] doubles): they change once
@@ -353,8 +355,11 @@ __device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 
     }
 }
 
-template <int NR>
-__global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scratch) {
+// NBUF = 2: the next y block is copied while the current one is visited (up to 8 warps
+// per CTA fit the shared memory); NBUF = 1: copy, wait, visit, which leaves room for 12
+// warps (three per scheduler) whose visits hide each other's copies
+template <int NR, int NBUF>
+__global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) k_atm32b(KP p, float4 *scratch) {
     extern __shared__ __align__(16) unsigned char smb[];
     const int ne = p.ne;
     const int nw = blockDim.x >> 5;
@@ -366,13 +371,13 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
     int *cellpos = reinterpret_cast<int *>(bbhi + mcap / 32);            // [512]
     float *r0sq = reinterpret_cast<float *>(cellpos + 512);              // [ne][ne]
     double *yapex = reinterpret_cast<double *>(r0sq + ((ne * ne + 3) & ~3)); // [ne][NR]
-    unsigned char *wbase = smb + atmb_smem_fixed(ne, NR, mcap) + (size_t)warp * atmb_smem_warp(ne, NR);
+    unsigned char *wbase = smb + atmb_smem_fixed(ne, NR, mcap) + (size_t)warp * atmb_smem_warp(ne, NR, NBUF);
     constexpr int RQ = atmb_row_floats(NR) / 4;                          // float4 quads per row
     // buffer layout: [ne][RQ][32] rows of the y block, [32] vx vy vz d2, [32] ir id2 s g
     float4 *ybuf0 = reinterpret_cast<float4 *>(wbase);
     const size_t bufq = atmb_buf_quads(ne, NR);
     __shared__ int s_item, s_row;
-    __shared__ double red[ATMB_MAXW][12];
+    __shared__ double red[NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1][12];
     float4 *sA = scratch + (size_t)blockIdx.x * atmb_scratch_per_cta(mcap); // vx vy vz d2
     float4 *sB = sA + mcap;                                              // ir id2 s g
     float4 *sJ = sB + mcap;                                              // j t lam_ea lam_ae
@@ -496,11 +501,11 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
         __syncthreads();
         // ---- 2./3. block pairs
         // apex force (3) and virial (6) of this lane, and the row sums of its x entry
-        const AtmbCarry apx{reinterpret_cast<double *>(wbase + 2 * bufq * sizeof(float4)) + lane};
+        const AtmbCarry apx{reinterpret_cast<double *>(wbase + NBUF * bufq * sizeof(float4)) + lane};
         const AtmbCarry xs{apx.p + 9 * 32}; // SE SD SF Wx Wy Wz SA Ux Uy Uz
         // positions (x, x', y, y'), (z, z', d2, d2') and constants (ir, ir', id2, id2'),
         // (s, s', g, g') of the current y block, entries k and k + 1 at slot k
-        float4 *yP0 = reinterpret_cast<float4 *>(wbase + 2 * bufq * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double));
+        float4 *yP0 = reinterpret_cast<float4 *>(wbase + NBUF * bufq * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double));
         float4 *yP1 = yP0 + 32, *yQ0 = yP1 + 32, *yQ1 = yQ0 + 32;
 #pragma unroll
         for (int q = 0; q < 9; ++q) apx[q] = 0.0;
@@ -597,16 +602,24 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
             };
             int B = next_near(A);
             int cur = 0;
-            __syncwarp(); // the previous row's visits are done with both buffers
-            if (B < nb) stage(B, ybuf0);
-            atmb_cp_commit();
+            __syncwarp(); // the previous row's visits are done with every buffer
+            if (NBUF == 2) {
+                if (B < nb) stage(B, ybuf0);
+                atmb_cp_commit();
+            }
             while (B < nb) {
                 const int Bn = next_near(B + 1);
-                __syncwarp(); // every lane is done with the other buffer
-                if (Bn < nb) stage(Bn, ybuf0 + (cur ^ 1) * bufq);
-                atmb_cp_commit();
-                atmb_cp_wait<1>(); // this lane's copies of block B have landed
-                __syncwarp();      // ... and every lane's
+                __syncwarp(); // every lane is done with the buffer about to be filled
+                if (NBUF == 2) {
+                    if (Bn < nb) stage(Bn, ybuf0 + (cur ^ 1) * bufq);
+                    atmb_cp_commit();
+                    atmb_cp_wait<1>(); // this lane's copies of block B have landed
+                } else {
+                    stage(B, ybuf0);
+                    atmb_cp_commit();
+                    atmb_cp_wait<0>();
+                }
+                __syncwarp(); // ... and every lane's
                 const float4 *yrow = ybuf0 + cur * bufq;
                 const float4 *yA = yrow + ne * RQ * 32;
                 const float4 *yB = yA + 32;
@@ -706,7 +719,7 @@ __global__ void __launch_bounds__(ATMB_MAXW * 32, 1) k_atm32b(KP p, float4 *scra
                     xs[9] -= xt.Uz.x + xt.Uz.y;
                 }
                 B = Bn;
-                cur ^= 1;
+                if (NBUF == 2) cur ^= 1;
             }
             atmb_cp_wait<0>();
             if (xvalid) {

@@ -1666,26 +1666,40 @@ void engine_fetch_results(Engine *e, double *energies, double *forces, double *s
 // (plain form, surrogate, mirror schedule chosen, or the type count leaves too little
 // shared memory)
 struct AtmbShape {
-    int warps, ctas, mcap; // warps per CTA (0: kernel not used), CTAs per SM, longest list
+    int warps, ctas, mcap, nbuf; // warps per CTA (0: kernel not used), CTAs per SM, longest
+                                 // list, y buffers per warp
 };
 static AtmbShape blockpair_shape(const Engine *e) {
-    if (!e->use_atm || !e->opt.precision || e->opt.atm_schedule != 0) return {0, 0, 0};
-    if (e->opt.atm_surrogate && e->surr.loaded) return {0, 0, 0};
+    if (!e->use_atm || !e->opt.precision || e->opt.atm_schedule != 0) return {0, 0, 0, 0};
+    if (e->opt.atm_surrogate && e->surr.loaded) return {0, 0, 0, 0};
+    const size_t limit = 227 * 1024 - 2048; // opt-in maximum minus the static arrays
+    // a requested shape (autotuner): warps per CTA (more than 8 with one y buffer per
+    // warp), CTAs per SM (2 when both fit), list capacity; kept only if it fits
+    if (e->opt.atmb_warps > 0) {
+        const int w = std::min(e->opt.atmb_warps, ATMB_MAXW1);
+        const int nbuf = w > ATMB_MAXW ? 1 : 2;
+        const size_t per = atmb_smem_warp(e->ne, e->nref, nbuf);
+        const int ctas = e->opt.atm_ctas_per_sm == 2 ? 2 : 1;
+        const size_t cap_sm = ctas == 2 ? (228 * 1024) / 2 - 2048 : limit;
+        int mcap = e->opt.atmb_mcap > 0 ? std::max(ATMB_MCAP_MIN, std::min(ATMB_MCAP_MAX, e->opt.atmb_mcap & ~511))
+                                        : ATMB_MCAP_MAX;
+        while (mcap >= ATMB_MCAP_MIN && atmb_smem_fixed(e->ne, e->nref, mcap) + w * per > cap_sm) mcap -= 512;
+        if (w >= 2 && mcap >= ATMB_MCAP_MIN) return {w, ctas, mcap, nbuf};
+    }
     const size_t per = atmb_smem_warp(e->ne, e->nref);
     // two CTAs of four warps per SM, so that one CTA's per-apex sort and set-up overlap the
     // other's block pairs, when both fit the SM's 228 KB (each with 2 KB for the static
     // arrays and the system's share)
     if (ATMB_CTAS_PER_SM == 2 && 2 * (atmb_smem_fixed(e->ne, e->nref, ATMB_MCAP_MIN) + 4 * per + 2048) <= 228 * 1024)
-        return {4, 2, ATMB_MCAP_MIN};
+        return {4, 2, ATMB_MCAP_MIN, 2};
     // else one CTA of up to ATMB_MAXW warps; the shared memory they leave sets the list
     // capacity (longer lists go to the mirror kernel)
-    const size_t limit = 227 * 1024 - 1024; // opt-in maximum minus the static arrays
     for (int w = ATMB_MAXW; w >= 2; --w) {
         int mcap = ATMB_MCAP_MAX;
         while (mcap >= ATMB_MCAP_MIN && atmb_smem_fixed(e->ne, e->nref, mcap) + w * per > limit) mcap -= 512;
-        if (mcap >= ATMB_MCAP_MIN) return {w, 1, mcap};
+        if (mcap >= ATMB_MCAP_MIN) return {w, 1, mcap, 2};
     }
-    return {0, 0, 0};
+    return {0, 0, 0, 0};
 }
 static int blockpair_warps(const Engine *e) { return blockpair_shape(e).warps; }
 
@@ -1980,9 +1994,15 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
                 const int nwb = shb.warps;
                 if (nwb > 0 && !surr) {
                     // lists up to shb.mcap entries: block-pair schedule; longer ones below
-                    const size_t smb = atmb_smem_fixed(p.ne, NR, shb.mcap) + (size_t)nwb * atmb_smem_warp(p.ne, NR);
-                    atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR>);
-                    k_atm32b<NR><<<e->dev_sms * shb.ctas, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
+                    const size_t smb =
+                        atmb_smem_fixed(p.ne, NR, shb.mcap) + (size_t)nwb * atmb_smem_warp(p.ne, NR, shb.nbuf);
+                    if (shb.nbuf == 2) {
+                        atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR, 2>);
+                        k_atm32b<NR, 2><<<e->dev_sms * shb.ctas, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
+                    } else {
+                        atm_occupancy(e, 6, smb, (const void *)k_atm32b<NR, 1>);
+                        k_atm32b<NR, 1><<<e->dev_sms * shb.ctas, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
+                    }
                     D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
                     pc.atm_min_m = shb.mcap;
                 }

@@ -55,6 +55,9 @@ struct Options {
                                      // density); a synchronous evaluation regrows on overflow
     int pair_kernel = 0;           // two-body pass: 0 atom groups with staged partners,
                                    // 1 one warp per atom
+    int atmb_warps = 0;            // block-pair ATM: warps per CTA (0: automatic; above 8
+                                   // with one y buffer per warp)
+    int atmb_mcap = 0;             // block-pair ATM: longest list it takes (0: automatic)
 };
 
 // Learned ATM surrogate: network parameters and normalisation (network in d3_mlp.h).

@@ -1,13 +1,21 @@
 """Autotuner for the engine's launch parameters.
 
 Tunables (engine options):
-  D3_OPT_BIN_DIVISOR      cell-list bin width = smallest cutoff / divisor  (pair passes)
-  D3_OPT_ATM_TILE         ATM partner-tile entries                           (ATM pass)
-  D3_OPT_ATM_CTAS_PER_SM  persistent ATM CTAs per SM                         (ATM pass)
+  D3_OPT_BIN_DIVISOR        cell-list bin width = smallest cutoff / divisor   (pair passes)
+  D3_OPT_PAIR_KERNEL        two-body threads per atom: 1 (groups of 32 atoms,  (two-body)
+                            one lane each) or 32 (one warp per atom)
+  D3_OPT_ATMB_WARPS         block-pair ATM kernel: warps per CTA (8 with two   (ATM pass,
+                            y buffers per warp, 12 with one)                     precision)
+  D3_OPT_ATM_CTAS_PER_SM    CTAs per SM (block-pair: 2 CTAs of 4 warps when they fit;
+                            mirror / FP64 kernels: persistent CTAs per SM)
+  D3_OPT_ATMB_LIST_CAPACITY longest list of the block-pair kernel (the rest go to the
+                            mirror kernel)
+  D3_OPT_ATM_TILE           partner-tile entries of the mirror and FP64 ATM kernels
 
-`tune(handle_factory, ...)` times each candidate with the engine's per-pass CUDA-event
-timers (d3_pass_times) on the caller's own workload and keeps the fastest; the pair
-passes and the ATM pass are tuned independently (bin width first, then tile and CTAs).
+`tune(handle, key)` times each candidate with the engine's per-pass CUDA-event timers
+(d3_pass_times) on the caller's own workload and keeps the fastest; the pair passes and
+the ATM pass are tuned independently (bin width and pair kernel first, then the ATM
+kernel's shape: block-pair shapes in the precision form, tile and CTAs in the FP64 form).
 Results are cached in a JSON file keyed by GPU name, atom-count bucket (powers of two),
 density bucket, cutoffs, ATM on/off and precision form, so a workload of the same kind
 reuses them without timing. Cache path: $D3_AUTOTUNE_CACHE or
@@ -17,11 +25,15 @@ import json
 import math
 import os
 
-from d3_b200 import OPT_ATM_CTAS_PER_SM, OPT_ATM_TILE, OPT_BIN_DIVISOR, OPT_PRECISION
+from d3_b200 import (OPT_ATM_CTAS_PER_SM, OPT_ATM_TILE, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_WARPS, OPT_BIN_DIVISOR,
+                     OPT_PAIR_KERNEL)
 
 BIN_DIVISORS = (3, 4, 6, 8)
+PAIR_KERNELS = (0, 1)
 ATM_TILES = (64, 128, 256)
 ATM_CTAS = (0, 2, 3)
+# block-pair shapes: (warps per CTA, CTAs per SM, list capacity; 0 = automatic)
+ATMB_SHAPES = ((0, 0, 0), (12, 0, 0), (6, 0, 0), (4, 2, 0), (8, 0, 4096))
 
 
 def cache_path():
@@ -42,7 +54,8 @@ def workload_key(n_atoms, volume_a3, rc, rc_cn, rc_atm, precision):
     nb = int(round(math.log2(max(n_atoms, 1))))
     rho = n_atoms / max(volume_a3, 1e-9)
     rb = round(math.log2(rho) * 2) / 2 if rho > 0 else 0
-    return "%s|n2^%d|rho2^%.1f|rc%.1f/%.1f/%.1f|p%d" % (gpu_name(), nb, rb, rc, rc_cn, rc_atm or 0.0, precision)
+    # v2: the parameter set includes the pair kernel and the block-pair ATM shape
+    return "v2|%s|n2^%d|rho2^%.1f|rc%.1f/%.1f/%.1f|p%d" % (gpu_name(), nb, rb, rc, rc_cn, rc_atm or 0.0, precision)
 
 
 def _load():
@@ -62,8 +75,11 @@ def _save(db):
 
 def apply(handle, params):
     handle.set_option(OPT_BIN_DIVISOR, params["bin_divisor"])
+    handle.set_option(OPT_PAIR_KERNEL, params.get("pair_kernel", 0))
     handle.set_option(OPT_ATM_TILE, params["atm_tile"])
     handle.set_option(OPT_ATM_CTAS_PER_SM, params["atm_ctas_per_sm"])
+    handle.set_option(OPT_ATMB_WARPS, params.get("atmb_warps", 0))
+    handle.set_option(OPT_ATMB_LIST_CAPACITY, params.get("atmb_mcap", 0))
 
 
 def _time(handle, repeats):
@@ -75,38 +91,57 @@ def _time(handle, repeats):
     return best
 
 
-def tune(handle, key, repeats=2, use_cache=True, atm=True):
-    """Choose bin divisor, ATM tile and ATM CTAs/SM for `handle` (a D3 or D3Batch whose
-    structures are set); applies and returns the parameters."""
+def tune(handle, key, repeats=2, use_cache=True, atm=True, precision=None):
+    """Choose bin divisor, pair kernel and the ATM kernel's shape for `handle` (a D3 or
+    D3Batch whose structures are set); applies and returns the parameters. precision: the
+    handle's form (taken from `key` when None)."""
     db = _load() if use_cache else {}
     if key in db:
         apply(handle, db[key])
         return dict(db[key], cached=True)
-    params = {"bin_divisor": 6, "atm_tile": 0, "atm_ctas_per_sm": 0}
+    if precision is None:
+        precision = key.endswith("|p1")
+    params = {"bin_divisor": 6, "pair_kernel": 0, "atm_tile": 0, "atm_ctas_per_sm": 0, "atmb_warps": 0,
+              "atmb_mcap": 0}
     apply(handle, params)
     pair_passes = ("bin", "cn", "twobody", "atm_list", "chain")
     best = None
     trials = []
     for bd in BIN_DIVISORS:
-        handle.set_option(OPT_BIN_DIVISOR, bd)
-        pt = _time(handle, repeats)
-        t = sum(pt[k] for k in pair_passes)
-        trials.append({"bin_divisor": bd, "pair_ms": t})
-        if best is None or t < best[0]:
-            best = (t, bd)
-    params["bin_divisor"] = best[1]
-    handle.set_option(OPT_BIN_DIVISOR, best[1])
+        for pk in PAIR_KERNELS:
+            handle.set_option(OPT_BIN_DIVISOR, bd)
+            handle.set_option(OPT_PAIR_KERNEL, pk)
+            pt = _time(handle, repeats)
+            t = sum(pt[k] for k in pair_passes)
+            trials.append({"bin_divisor": bd, "pair_kernel": pk, "pair_ms": t})
+            if best is None or t < best[0]:
+                best = (t, bd, pk)
+    params["bin_divisor"], params["pair_kernel"] = best[1], best[2]
+    apply(handle, params)
     if atm:
         best = None
-        for tile in ATM_TILES:
-            for ctas in ATM_CTAS:
-                handle.set_option(OPT_ATM_TILE, tile)
-                handle.set_option(OPT_ATM_CTAS_PER_SM, ctas)
+        if precision:
+            # the block-pair kernel takes the lists up to its capacity, the mirror kernel
+            # (tile, CTAs per SM at their defaults) the longer ones
+            for w, c, m in ATMB_SHAPES:
+                handle.set_option(OPT_ATMB_WARPS, w)
+                handle.set_option(OPT_ATM_CTAS_PER_SM, c)
+                handle.set_option(OPT_ATMB_LIST_CAPACITY, m)
                 t = _time(handle, repeats)["atm"]
-                trials.append({"atm_tile": tile, "atm_ctas_per_sm": ctas, "atm_ms": t})
+                trials.append({"atmb_warps": w, "atm_ctas_per_sm": c, "atmb_mcap": m, "atm_ms": t})
                 if best is None or t < best[0]:
-                    best = (t, tile, ctas)
-        params["atm_tile"], params["atm_ctas_per_sm"] = best[1], best[2]
+                    best = (t, w, c, m)
+            params["atmb_warps"], params["atm_ctas_per_sm"], params["atmb_mcap"] = best[1], best[2], best[3]
+        else:
+            for tile in ATM_TILES:
+                for ctas in ATM_CTAS:
+                    handle.set_option(OPT_ATM_TILE, tile)
+                    handle.set_option(OPT_ATM_CTAS_PER_SM, ctas)
+                    t = _time(handle, repeats)["atm"]
+                    trials.append({"atm_tile": tile, "atm_ctas_per_sm": ctas, "atm_ms": t})
+                    if best is None or t < best[0]:
+                        best = (t, tile, ctas)
+            params["atm_tile"], params["atm_ctas_per_sm"] = best[1], best[2]
     apply(handle, params)
     if use_cache:
         db = _load()

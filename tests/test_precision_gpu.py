@@ -110,3 +110,38 @@ def test_atm_schedules_agree(case):
     assert np.abs(s0 - s1).max() <= 1e-6 * np.abs(s1).max() + 1e-12
     # per-atom energy shares (E/3 of every triplet through the atom) agree as well
     assert np.abs(a0 - a1).max() <= 1e-6 * np.abs(a1).max()
+
+
+@pytest.mark.parametrize("shape", [(12, 0, 0), (4, 2, 0), (6, 0, 4096), (12, 0, 4096)])
+@pytest.mark.parametrize("case", ["tric", "fe"])
+def test_block_pair_shapes_agree(case, shape):
+    """Launch shapes of the block-pair ATM kernel (warps per CTA, CTAs per SM, list
+    capacity; 12 warps stage one y block at a time) against the default shape: the same
+    in-range triplets and the same results to FP32 level. A 4,096-entry capacity sends the
+    longest lists of the 3,000-atom box (up to about 4,100 entries at rc_ATM 40) to the
+    mirror kernel."""
+    from d3_b200 import OPT_ATM_CTAS_PER_SM, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_WARPS
+
+    if case == "tric":
+        sys_, kw = S.triclinic_box(3000, seed=5), dict(rc=95.0, rc_cn=40.0, rc_atm=40.0)
+    else:
+        sys_ = S.gtest_bcc_fe(True)
+        sys_["pos"] = sys_["pos"] + np.random.default_rng(1).uniform(-0.1, 0.1, sys_["pos"].shape)
+        kw = dict(rc=30.0, rc_cn=30.0, rc_atm=30.0)
+    out = []
+    for opts in ((), ((OPT_ATMB_WARPS, shape[0]), (OPT_ATM_CTAS_PER_SM, shape[1]), (OPT_ATMB_LIST_CAPACITY, shape[2]))):
+        d = D3(sys_["Z"], len(sys_["Z"]), damping=1, functional=0, **kw)
+        d.set_option(OPT_PRECISION, 1)
+        for o, v in opts:
+            d.set_option(o, v)
+        d.set_cell(sys_["cell"])
+        d.set_atoms(sys_["pos"], sys_["Z"])
+        e, f, s = d.compute()
+        _, cnt = d.pass_times()
+        out.append((e, f, s, int(cnt[0])))
+        d.close()
+    (e0, f0, s0, c0), (e1, f1, s1, c1) = out
+    assert c0 == c1 and c0 > 0
+    assert abs(e0 - e1) <= 1e-7 * abs(e0)
+    assert np.abs(f0 - f1).max() <= 1e-5 * np.abs(f0).max() + 1e-9
+    assert np.abs(s0 - s1).max() <= 1e-6 * np.abs(s0).max() + 1e-12
