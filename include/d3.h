@@ -131,9 +131,13 @@ enum {
                                     automatic (8), 2..12; above 8 each warp stages one y
                                     block at a time instead of two. With
                                     D3_OPT_ATM_CTAS_PER_SM = 2, two CTAs per SM when they fit */
-    D3_OPT_ATMB_LIST_CAPACITY = 12 /* longest half list (entries) the block-pair kernel takes,
+    D3_OPT_ATMB_LIST_CAPACITY = 12, /* longest half list (entries) the block-pair kernel takes,
                                     0 = as many as the shared memory allows (4,096..8,192);
                                     longer lists go to the mirror-symmetric kernel */
+    D3_OPT_ATMB_SPLIT = 13       /* CTAs of the block-pair kernel sharing one apex, each taking
+                                    every S-th block row (0 = automatic: more than one only
+                                    when the apexes are fewer than about 4 per CTA, e.g. the
+                                    96-atom water box; 1..64) */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);
 

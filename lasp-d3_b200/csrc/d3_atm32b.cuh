@@ -396,7 +396,11 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         __syncthreads();
         if (tid == 0) s_item = atomicAdd(p.work, 1);
         __syncthreads();
-        const int item = s_item * p.shard_world + p.shard_rank;
+        // work item = (apex, split): with split count S > 1 (systems with fewer apexes than
+        // CTAs can hold) several CTAs share an apex, each taking its rows split, split + S, ...
+        const int S = p.atmb_split;
+        const int split = s_item % S;
+        const int item = (s_item / S) * p.shard_world + p.shard_rank;
         if (item >= p.n) break;
         const int a = p.sorted_of[p.n - 1 - item];
         const long long e0 = p.atm_off[a];
@@ -513,7 +517,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         // first and the cheapest close the apex, shortening the wait at its barrier)
         for (;;) {
             int A = 0;
-            if (lane == 0) A = atomicAdd(&s_row, 1);
+            if (lane == 0) A = split + S * atomicAdd(&s_row, 1);
             A = __shfl_sync(0xffffffffu, A, 0);
             if (A >= nb) break;
             const int xe = A * 32 + lane;
@@ -781,13 +785,20 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                 tot[k] = 0;
                 for (int w2 = 0; w2 < nw; ++w2) tot[k] += red[w2][k];
             }
-            p.ea[a] = tot[0];
-            p.ga[a] = tot[1];
-            p.fa[3 * a] = tot[2];
-            p.fa[3 * a + 1] = tot[3];
-            p.fa[3 * a + 2] = tot[4];
             const double sc = -1.0 / g.vol;
-            for (int k = 0; k < 6; ++k) p.va[6 * (size_t)a + k] = tot[5 + k] * sc;
+            if (S == 1) {
+                p.ea[a] = tot[0];
+                p.ga[a] = tot[1];
+                p.fa[3 * a] = tot[2];
+                p.fa[3 * a + 1] = tot[3];
+                p.fa[3 * a + 2] = tot[4];
+                for (int k = 0; k < 6; ++k) p.va[6 * (size_t)a + k] = tot[5 + k] * sc;
+            } else { // the apex's other splits add theirs (the arrays start at zero)
+                atomicAdd(&p.ea[a], tot[0]);
+                atomicAdd(&p.ga[a], tot[1]);
+                for (int k = 0; k < 3; ++k) atomicAdd(&p.fa[3 * a + k], tot[2 + k]);
+                for (int k = 0; k < 6; ++k) atomicAdd(&p.va[6 * (size_t)a + k], tot[5 + k] * sc);
+            }
         }
     }
     for (int o = 16; o > 0; o >>= 1) visits += __shfl_xor_sync(0xffffffffu, visits, o);

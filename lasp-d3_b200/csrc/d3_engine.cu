@@ -125,6 +125,7 @@ struct KP {
                     // the type pair, the row of the weight derivatives, the atom index bits
     int atm_min_m;  // k_atm32 takes only apexes with longer lists (the rest: k_atm32b)
     int atmb_mcap;  // longest list k_atm32b takes
+    int atmb_split; // CTAs of k_atm32b sharing one apex (each a share of its block rows)
     // sharded evaluation: this process computes the two-body and chain-rule terms of central
     // atoms i = shard_rank + k shard_world (binned order) and the ATM apexes of work items
     // shard_rank + k shard_world; CN and weights for every atom
@@ -1782,12 +1783,18 @@ static KP make_kp(Engine *e) {
     p.Y32 = e->Y32.p;
     p.YD32 = nullptr;
     p.atm_min_m = 0;
+    p.atmb_split = 1;
     if (blockpair_warps(e) > 0) {
         e->YD32.ensure((size_t)e->max_atoms * e->ne * atmb_row_floats(e->nref));
         const AtmbShape sh = blockpair_shape(e);
         e->atmb_scratch.ensure((size_t)e->dev_sms * sh.ctas * atmb_scratch_per_cta(sh.mcap));
         p.atmb_mcap = sh.mcap;
         p.YD32 = e->YD32.p;
+        // few apexes (small structures): split each apex's block rows over several CTAs so
+        // that about four work items per CTA exist
+        const int ctas = e->dev_sms * sh.ctas;
+        p.atmb_split = e->opt.atmb_split > 0 ? std::min(e->opt.atmb_split, 64)
+                                             : std::max(1, std::min(16, (4 * ctas + p.n - 1) / std::max(1, p.n)));
     }
     p.atm_force_scaled = e->opt.atm_force_scaled ? 1 : 0;
     p.anyshift = e->anyshift.p;

@@ -58,6 +58,8 @@ struct Options {
     int atmb_warps = 0;            // block-pair ATM: warps per CTA (0: automatic; above 8
                                    // with one y buffer per warp)
     int atmb_mcap = 0;             // block-pair ATM: longest list it takes (0: automatic)
+    int atmb_split = 0;            // block-pair ATM: CTAs sharing one apex (0: automatic,
+                                   // more than one only when apexes are fewer than CTAs)
 };
 
 // Learned ATM surrogate: network parameters and normalisation (network in d3_mlp.h).

@@ -112,15 +112,17 @@ def test_atm_schedules_agree(case):
     assert np.abs(a0 - a1).max() <= 1e-6 * np.abs(a1).max()
 
 
-@pytest.mark.parametrize("shape", [(12, 0, 0), (4, 2, 0), (6, 0, 4096), (12, 0, 4096)])
+@pytest.mark.parametrize("shape", [(12, 0, 0, 0), (4, 2, 0, 0), (6, 0, 4096, 0), (12, 0, 4096, 0), (0, 0, 0, 3),
+                                   (12, 0, 0, 5)])
 @pytest.mark.parametrize("case", ["tric", "fe"])
 def test_block_pair_shapes_agree(case, shape):
     """Launch shapes of the block-pair ATM kernel (warps per CTA, CTAs per SM, list
-    capacity; 12 warps stage one y block at a time) against the default shape: the same
-    in-range triplets and the same results to FP32 level. A 4,096-entry capacity sends the
-    longest lists of the 3,000-atom box (up to about 4,100 entries at rc_ATM 40) to the
-    mirror kernel."""
-    from d3_b200 import OPT_ATM_CTAS_PER_SM, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_WARPS
+    capacity, CTAs sharing an apex; 12 warps stage one y block at a time) against the
+    default shape: the same in-range triplets and the same results to FP32 level. A
+    4,096-entry capacity sends the longest lists of the 3,000-atom box (up to about 4,100
+    entries at rc_ATM 40) to the mirror kernel; a split of 3 or 5 makes several CTAs add
+    their shares of each apex."""
+    from d3_b200 import OPT_ATM_CTAS_PER_SM, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_SPLIT, OPT_ATMB_WARPS
 
     if case == "tric":
         sys_, kw = S.triclinic_box(3000, seed=5), dict(rc=95.0, rc_cn=40.0, rc_atm=40.0)
@@ -129,7 +131,8 @@ def test_block_pair_shapes_agree(case, shape):
         sys_["pos"] = sys_["pos"] + np.random.default_rng(1).uniform(-0.1, 0.1, sys_["pos"].shape)
         kw = dict(rc=30.0, rc_cn=30.0, rc_atm=30.0)
     out = []
-    for opts in ((), ((OPT_ATMB_WARPS, shape[0]), (OPT_ATM_CTAS_PER_SM, shape[1]), (OPT_ATMB_LIST_CAPACITY, shape[2]))):
+    for opts in ((), ((OPT_ATMB_WARPS, shape[0]), (OPT_ATM_CTAS_PER_SM, shape[1]), (OPT_ATMB_LIST_CAPACITY, shape[2]),
+                      (OPT_ATMB_SPLIT, shape[3]))):
         d = D3(sys_["Z"], len(sys_["Z"]), damping=1, functional=0, **kw)
         d.set_option(OPT_PRECISION, 1)
         for o, v in opts:
