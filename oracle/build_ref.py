@@ -21,7 +21,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF_SRC = "/root/reference/src"
+# the reference tree: $LASP_D3_REFERENCE (default: the path the build container mounts)
+REF_SRC = os.path.join(os.environ.get("LASP_D3_REFERENCE", "/root/reference"), "src")
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 REF_FLAGS = ["-std=c++17", "-O2", "-lineinfo", "--maxrregcount=64", "-rdc=true", "-Xcompiler", "-fPIC"]

@@ -15,7 +15,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF = "/root/reference"
+# the reference tree: $LASP_D3_REFERENCE (default: the path the build container mounts)
+REF = os.environ.get("LASP_D3_REFERENCE", "/root/reference")
 OUT = os.path.join(HERE, "_ref", "d3_test_ref")
 
 

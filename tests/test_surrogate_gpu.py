@@ -256,3 +256,29 @@ def test_surrogate_rejects_uncovered_element():
     d = D3(Z, len(Z), rc=95.0, rc_cn=40.0, rc_atm=40.0)
     with pytest.raises(RuntimeError):
         d.set_surrogate(random_model(seed=0))
+
+
+def test_trained_model_beats_dropping_atm():
+    # the shipped model on a held-out box of the benchmark generator (3,000 atoms): its
+    # error against the exact ATM term is far below the error of leaving ATM out, and
+    # within the surrogate bars (0.5 meV/atom energy, 5 meV/A forces)
+    import os
+
+    path = os.path.join(os.path.dirname(SU.__file__), "surrogate", "atm_hcnosicu.d3s")
+    model = SU.Model.load(path)
+    sys_ = S.triclinic_box(3000, seed=41)
+    n = len(sys_["Z"])
+    e_x, f_x, _, _, _ = run_with(sys_, None, None, precision=1, force_scaled=True)
+    e_s, f_s, _, flagged, _ = run_with(sys_, model, 1e9, precision=1)
+    assert flagged == 0
+    d0 = D3(sys_["Z"], n, rc=95.0, rc_cn=40.0, rc_atm=None)
+    d0.set_option(OPT_PRECISION, 1)
+    d0.set_cell(sys_["cell"])
+    d0.set_atoms(sys_["pos"], sys_["Z"])
+    e_0, f_0, _ = d0.compute()
+    d0.close()
+    err_s, err_0 = abs(e_s - e_x) / n, abs(e_0 - e_x) / n
+    ferr_s, ferr_0 = np.abs(f_s - f_x).max(), np.abs(f_0 - f_x).max()
+    assert err_s <= 5e-4 and ferr_s <= 5e-3, (err_s, ferr_s)
+    assert err_s <= 0.1 * err_0, (err_s, err_0)
+    assert ferr_s <= 0.5 * ferr_0, (ferr_s, ferr_0)
