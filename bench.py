@@ -59,7 +59,9 @@ def system_for(args, seed):
     return S.triclinic_box(args.atoms, seed=seed)
 
 
-def workload_config(n, form, args=None):
+def workload_config(n, args=None):
+    """The workload: identical in the engine arm and the reference arm (the form each arm
+    computes in is reported beside it, under "form")."""
     water = args is not None and args.system == "water"
     table = 7 if (args is not None and args.table == 7) else 5
     atm = not (args is not None and args.no_atm)
@@ -74,7 +76,6 @@ def workload_config(n, form, args=None):
                     "energy+forces+stress" % (box, "+ATM" if atm else " (two-body + CN, no ATM)", table,
                                                " / rc_ATM 40" if atm else ""),
         "atoms_per_gpu": n,
-        "form": form,
         "l2": "flushed between timed steps (256 MiB device write)",
         "parallelism": "replicas: one box per GPU, no collective",
     }
@@ -360,9 +361,9 @@ def engine_arm(args, world, rank, local):
     line = {"metric": METRIC, "value": ch["value"], "unit": "atoms/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ch["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if fp64 else "f32", "data": "synthetic",
-            "config": workload_config(n, "%s form (%s)" % (chosen, "FP64 throughout" if fp64 else
-                                                         "FP32 pair/triplet arithmetic, FP64 C6 weights, dE/dCN "
-                                                         "and reductions"), args),
+            "config": workload_config(n, args),
+            "form": "%s form (%s)" % (chosen, "FP64 throughout" if fp64 else
+                                      "FP32 pair/triplet arithmetic, FP64 C6 weights, dE/dCN and reductions"),
             "chosen_form": chosen, "forms": forms_out, "options": args.option,
             "roofline": roofline, "e2e": e2e, "gpu_launches": ch["launches"] * args.steps, "clocks": clocks,
             "counters": {"atm_triplets": triplets, "twobody_ordered_pairs": int(ch["counters"][1]),
@@ -425,7 +426,8 @@ def shard_arm(args, world, rank, local):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
-                "config": dict(workload_config(n, "precision form, sharded", args),
+                "form": "precision form, sharded",
+                "config": dict(workload_config(n, args),
                                parallelism="shard%d: central atoms and ATM apexes split round-robin over ranks; "
                                            "all-reduce of dE/dCN (n doubles) and of the results (NCCL)" % world,
                                l2="not flushed; the inputs are larger than L2 (ATM half lists about 330 MB at "
@@ -479,8 +481,9 @@ def reference_arm(args, world, rank, local):
     line = {"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": workload_config(full_n, "reference CUDA build%s" % (
-                "" if n == full_n else ", bounded sample of %d atoms" % n), args),
+            "config": workload_config(full_n, args),
+            "form": "reference CUDA build (float)%s" % ("" if n == full_n else ", each step a bounded sample: the "
+                                                                             "same generator at %d atoms" % n),
             "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": 1, "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "clocks": clocks, "energy_ev": e}

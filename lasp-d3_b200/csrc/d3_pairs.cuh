@@ -157,7 +157,7 @@ __host__ __device__ constexpr size_t pairs_warp_bytes(int ne, int NR) {
 }
 
 template <int NR, bool F64>
-__global__ void __launch_bounds__(PAIRS_WARPS * 32) k_twobody_g(KP p) {
+__global__ void __launch_bounds__(PAIRS_WARPS * 32, F64 ? 1 : 2) k_twobody_g(KP p) {
     using R = typename PairReal<F64>::R;
     using R4 = typename PairReal<F64>::R4;
     extern __shared__ __align__(16) unsigned char smp[];
