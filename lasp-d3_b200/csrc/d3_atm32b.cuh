@@ -2,8 +2,9 @@
 // Included by d3_engine.cu after k_atm32 (same per-entry set-up, weights and outputs).
 //
 // Per apex a (persistent CTAs take apexes from a work counter, largest lists first):
-//  1. The entries of the half list are counting-sorted by a Morton key of an 8^3 grid over
-//     [-rc, rc]^3 around the apex, so 32 consecutive entries ("a block") are close in space.
+//  1. The entries of the half list are counting-sorted by the Hilbert-curve position of their
+//     cell in a 16^3 grid over [-rc, rc]^3 around the apex, so 32 consecutive entries ("a
+//     block") are close in space.
 //     Per-entry set-up (FP64 C6 of the apex pair, its CN derivatives, damping ratio) is
 //     written once per apex, in sorted order, to this CTA's slot of a global scratch array.
 //  2. Block pairs (A, B), B >= A, whose bounding boxes are within rc_ATM of each other are
@@ -42,7 +43,8 @@
 // longest list this kernel takes (longer lists: k_atm32): chosen per launch, a multiple of
 // 512 in [ATMB_MCAP_MIN, ATMB_MCAP_MAX], as large as the shared memory left by the warps allows
 constexpr int ATMB_MCAP_MIN = 4096, ATMB_MCAP_MAX = 8192;
-constexpr int ATMB_GRID = 8;      // spatial grid per dimension for the entry sort
+constexpr int ATMB_GRID = 16;     // spatial grid per dimension for the entry sort
+constexpr int ATMB_CELLS = ATMB_GRID * ATMB_GRID * ATMB_GRID;
 constexpr int ATMB_MAXW = 8;      // warps per CTA at most with two y buffers per warp
 constexpr int ATMB_MAXW1 = 12;    // warps per CTA at most with one y buffer per warp (168
                                   // registers per thread: three warps per scheduler)
@@ -56,7 +58,6 @@ __host__ __device__ inline size_t atmb_scratch_per_cta(int mcap) { return 3 * (s
 __host__ __device__ inline size_t atmb_smem_fixed(int ne, int NR, int mcap) {
     size_t b = (size_t)mcap * sizeof(int);                    // atom of each sorted entry
     b += 2 * (size_t)(mcap / 32) * sizeof(float4);            // block bounding boxes
-    b += 512 * sizeof(int);                                   // sort cells
     b += (size_t)((ne * ne + 3) & ~3) * sizeof(float);        // r0^2
     b += (size_t)((ne * NR + 1) & ~1) * sizeof(double);       // apex C6 rows
     return (b + 15) & ~(size_t)15;
@@ -91,11 +92,40 @@ __device__ __forceinline__ void atmb_cp_commit() { asm volatile("cp.async.commit
 template <int N>
 __device__ __forceinline__ void atmb_cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-__device__ __forceinline__ int atmb_morton(int x, int y, int z) {
-    int k = 0;
+// Position of cell (x, y, z) of the 16^3 grid along a Hilbert curve (Skilling's transform
+// of the axes to the transposed Hilbert index, then bit interleaving). Consecutive entries in
+// this order stay spatially adjacent (no jumps), so 32 consecutive entries form tighter
+// blocks than in Morton order: a simulation of uniform apex spheres gives 0.57-0.62 of the
+// visit slots of surviving block pairs in range, against 0.53-0.57 with Morton order on 8^3.
+__device__ __forceinline__ int atmb_hilbert(int x, int y, int z) {
+    int X[3] = {x, y, z};
+    constexpr int M = ATMB_GRID >> 1;
 #pragma unroll
-    for (int b = 0; b < 3; ++b) k |= (((x >> b) & 1) << (3 * b)) | (((y >> b) & 1) << (3 * b + 1)) | (((z >> b) & 1) << (3 * b + 2));
-    return k;
+    for (int Q = M; Q > 1; Q >>= 1) {
+        const int P = Q - 1;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            if (X[i] & Q) {
+                X[0] ^= P;
+            } else {
+                const int t = (X[0] ^ X[i]) & P;
+                X[0] ^= t;
+                X[i] ^= t;
+            }
+        }
+    }
+    X[1] ^= X[0];
+    X[2] ^= X[1];
+    int t = 0;
+#pragma unroll
+    for (int Q = M; Q > 1; Q >>= 1)
+        if (X[2] & Q) t ^= Q - 1;
+    int h = 0;
+#pragma unroll
+    for (int b = 3; b >= 0; --b)
+#pragma unroll
+        for (int i = 0; i < 3; ++i) h = (h << 1) | (((X[i] ^ t) >> b) & 1);
+    return h;
 }
 
 // one row of the table (atmb_row_floats(NR) floats as float4 quads): C6 row Y, r0^2 of the
@@ -368,13 +398,15 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
     int *sjy = reinterpret_cast<int *>(smb);                             // [mcap] atom of each sorted entry
     float4 *bblo = reinterpret_cast<float4 *>(sjy + mcap);               // [mcap/32]
     float4 *bbhi = bblo + mcap / 32;
-    int *cellpos = reinterpret_cast<int *>(bbhi + mcap / 32);            // [512]
-    float *r0sq = reinterpret_cast<float *>(cellpos + 512);              // [ne][ne]
+    float *r0sq = reinterpret_cast<float *>(bbhi + mcap / 32);           // [ne][ne]
     double *yapex = reinterpret_cast<double *>(r0sq + ((ne * ne + 3) & ~3)); // [ne][NR]
     unsigned char *wbase = smb + atmb_smem_fixed(ne, NR, mcap) + (size_t)warp * atmb_smem_warp(ne, NR, NBUF);
     constexpr int RQ = atmb_row_floats(NR) / 4;                          // float4 quads per row
     // buffer layout: [ne][RQ][32] rows of the y block, [32] vx vy vz d2, [32] ir id2 s g
     float4 *ybuf0 = reinterpret_cast<float4 *>(wbase);
+    // the sort's cell counters use the warps' staging area, idle between block-pair phases
+    // (every warp region is at least 9 KB and there are at least two warps)
+    int *cellpos = reinterpret_cast<int *>(smb + atmb_smem_fixed(ne, NR, mcap)); // [ATMB_CELLS]
     const size_t bufq = atmb_buf_quads(ne, NR);
     __shared__ int s_item, s_row;
     __shared__ double red[NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1][12];
@@ -411,7 +443,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         const SG &g = p.sg[p.sid[a]];
         const bool simple = g.atm_simple != 0;
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
-        for (int k = tid; k < 512; k += blockDim.x) cellpos[k] = 0;
+        for (int k = tid; k < ATMB_CELLS; k += blockDim.x) cellpos[k] = 0;
         if (tid == 0) s_row = 0;
         for (int q = 0; q < 6; ++q)
             for (int e = tid; e < m; e += blockDim.x) __stcg(&acc[q * mcap + e], 0.f);
@@ -428,27 +460,22 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             const int cx = min(ATMB_GRID - 1, max(0, (int)((xj.x + sx - xa.x + rc) * cinv)));
             const int cy = min(ATMB_GRID - 1, max(0, (int)((xj.y + sy - xa.y + rc) * cinv)));
             const int cz = min(ATMB_GRID - 1, max(0, (int)((xj.z + sz - xa.z + rc) * cinv)));
-            atomicAdd(&cellpos[atmb_morton(cx, cy, cz)], 1);
+            atomicAdd(&cellpos[atmb_hilbert(cx, cy, cz)], 1);
         }
         __syncthreads();
         if (warp == 0) {
-            int c[16], s = 0;
+            // exclusive scan of the cell counts, 32 cells per step (conflict-free rows)
+            int carry = 0;
+            for (int r = 0; r < ATMB_CELLS; r += 32) {
+                const int v = cellpos[r + lane];
+                int incl = v;
 #pragma unroll
-            for (int t = 0; t < 16; ++t) {
-                c[t] = cellpos[lane * 16 + t];
-                s += c[t];
-            }
-            int incl = s;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            int run = incl - s;
-#pragma unroll
-            for (int t = 0; t < 16; ++t) {
-                cellpos[lane * 16 + t] = run;
-                run += c[t];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += u;
+                }
+                cellpos[r + lane] = carry + incl - v;
+                carry += __shfl_sync(0xffffffffu, incl, 31);
             }
         }
         __syncthreads();
@@ -463,7 +490,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             const int cx = min(ATMB_GRID - 1, max(0, (int)((vx + rc) * cinv)));
             const int cy = min(ATMB_GRID - 1, max(0, (int)((vy + rc) * cinv)));
             const int cz = min(ATMB_GRID - 1, max(0, (int)((vz + rc) * cinv)));
-            const int pos = atomicAdd(&cellpos[atmb_morton(cx, cy, cz)], 1);
+            const int pos = atomicAdd(&cellpos[atmb_hilbert(cx, cy, cz)], 1);
             const double d2 = vx * vx + vy * vy + vz * vz;
             const double *ya = yapex + tp * NR;                   // C6_ae = y_{a,tp} . w_e
             const double *yq = p.Y + ((size_t)jp * ne + ta) * NR; // dC6_ae/dCN_a = y_{e,ta} . dw_a

@@ -1685,7 +1685,8 @@ static AtmbShape blockpair_shape(const Engine *e) {
         int mcap = e->opt.atmb_mcap > 0 ? std::max(ATMB_MCAP_MIN, std::min(ATMB_MCAP_MAX, e->opt.atmb_mcap & ~511))
                                         : ATMB_MCAP_MAX;
         while (mcap >= ATMB_MCAP_MIN && atmb_smem_fixed(e->ne, e->nref, mcap) + w * per > cap_sm) mcap -= 512;
-        if (w >= 2 && mcap >= ATMB_MCAP_MIN) return {w, ctas, mcap, nbuf};
+        // the entry sort's cell counters live in the warps' staging area
+        if (w >= 2 && mcap >= ATMB_MCAP_MIN && w * per >= ATMB_CELLS * sizeof(int)) return {w, ctas, mcap, nbuf};
     }
     const size_t per = atmb_smem_warp(e->ne, e->nref);
     // two CTAs of four warps per SM, so that one CTA's per-apex sort and set-up overlap the
