@@ -62,6 +62,7 @@ struct SG {
     int atom_base, natoms;    // atom range in caller order
     int st2_off, st2_n, stc_off, stc_n, sta_off, sta_n; // stencil rows (two-body, CN, ATM)
     int st2b_off, st2b_n;     // two-body stencil of a block of gy x gz bin rows (atom groups)
+    int stcb_off, stcb_n;     // CN / chain-rule stencil of the same blocks
     int atm_simple;           // every cell height > 2 rc_ATM: no atom twice in an ATM list
 };
 
@@ -139,7 +140,7 @@ struct KP {
     const int4 *srows;
     int nsrow;
     int4 *groups;
-    int *gcount, *gwork;
+    int *gcount;             // groups cut this evaluation (the passes' work counters follow)
     int gslices;
     double *gpart;
 };
@@ -643,13 +644,22 @@ __device__ __forceinline__ int sext8(int v) { return (v << 24) >> 24; }
 // in FP32 within one stencil row and carried across rows in FP64 (blocked summation);
 // dE/dCN is accumulated in FP64.
 // ------------------------------------------------------------------------------------
-__device__ __forceinline__ float cn_term32(float r2, float rsum, float *dcn_over_r) {
+// FP32 CN term: value and (d CN / d r) / r, with the optional tanh^3 smooth cutoff (the
+// reference's SMOOTH_CUTOFF_CN) as in the FP64 term
+__device__ __forceinline__ float cn_term32(const KP &p, float r2, float rsum, float *dcn_over_r) {
     const float ir = rsqrtf(r2);
     const float e = __expf(-16.0f * fmaf(rsum, ir, -1.0f));
-    const float ope = 1.0f + e;
-    const float inv = __fdividef(1.0f, ope);
-    *dcn_over_r = -16.0f * e * rsum * ir * ir * ir * inv * inv;
-    return inv;
+    const float inv = __fdividef(1.0f, 1.0f + e);
+    float d = -16.0f * e * rsum * ir * ir * ir * inv * inv;
+    float v = inv;
+    if (p.smooth_cn) {
+        const float t = tanhf((float)p.rc_cn - r2 * ir);
+        const float sc = t * t * t;
+        d = d * sc - 3.0f * t * t * (1.0f - t * t) * inv * ir;
+        v = inv * sc;
+    }
+    *dcn_over_r = d;
+    return v;
 }
 
 __global__ void k_cn32(KP p) {
@@ -674,7 +684,7 @@ __global__ void k_cn32(KP p) {
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (d2 <= rcn2 && d2 > 0.0f) {
                 float dd;
-                part += cn_term32(d2, ri + (float)p.rcov[(int)xj.w], &dd);
+                part += cn_term32(p, d2, ri + (float)p.rcov[(int)xj.w], &dd);
                 ++npair;
             }
         },
@@ -839,7 +849,7 @@ __global__ void k_chain32(KP p, const double *Gd) {
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             if (!(d2 <= rcn2 && d2 > 0.0f)) return;
             float dcn;
-            cn_term32(d2, ri + (float)p.rcov[(int)xj.w], &dcn);
+            cn_term32(p, d2, ri + (float)p.rcov[(int)xj.w], &dcn);
             const float dE = (float)(gi + Gd[j]) * dcn;
             const float fdx = dE * dx, fdy = dE * dy;
             fx += fdx;
@@ -1532,6 +1542,13 @@ static void build_structures(Engine *e, int nstruct, const uint64_t *counts, con
             r.st2b_off = (int)rows.size();
             r.st2b_n = (int)blk.size();
             for (auto &x : blk) rows.push_back(make_int4(x.dy, x.dz, x.dxlo, x.dxhi));
+            std::vector<StencilRow> sc;
+            for (int q = r.stc_off; q < r.stc_off + r.stc_n; ++q)
+                sc.push_back({rows[q].x, rows[q].y, rows[q].z, rows[q].w});
+            const auto blkc = merge_block_stencil(sc, gy, gz);
+            r.stcb_off = (int)rows.size();
+            r.stcb_n = (int)blkc.size();
+            for (auto &x : blkc) rows.push_back(make_int4(x.dy, x.dz, x.dxlo, x.dxhi));
             for (int bz = 0; bz < r.nb[2]; bz += gz)
                 for (int by = 0; by < r.nb[1]; by += gy)
                     srow.push_back(make_int4(k, by, bz, std::min(gy, r.nb[1] - by) | (std::min(gz, r.nb[2] - bz) << 8)));
@@ -1553,7 +1570,7 @@ static void build_structures(Engine *e, int nstruct, const uint64_t *counts, con
     if (!srow.empty())
         D3_CUDA(cudaMemcpy(e->srows.p, srow.data(), sizeof(int4) * srow.size(), cudaMemcpyHostToDevice));
     e->groups.ensure(e->group_bound);
-    e->gctl.ensure(2);
+    e->gctl.ensure(4); // [0] groups, [1..3] work counters of the CN, two-body and chain passes
     e->anyshift.ensure(std::max(1, nstruct));
     e->nstruct = nstruct;
     e->nbins_total = bin_base;
@@ -1803,7 +1820,6 @@ static KP make_kp(Engine *e) {
     p.nsrow = (int)e->srow_host.size();
     p.groups = e->groups.p;
     p.gcount = e->gctl.p;
-    p.gwork = e->gctl.p + 1;
     p.gslices = 0;
     p.gpart = nullptr;
     if (pairs_grouped(e)) {
@@ -1919,8 +1935,19 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
         k_scatter<<<gb, T, 0, s>>>(p);
         k_binsort<<<(p.nbins_total + T - 1) / T, T, 0, s>>>(p);
         k_gather<<<gb, T, 0, s>>>(p);
+        if (p.gslices > 0) {
+            D3_CUDA(cudaMemsetAsync(e->gctl.p, 0, 4 * sizeof(int), s));
+            k_groups<<<(p.nsrow + 127) / 128, 128, 0, s>>>(p);
+        }
         D3_CUDA(cudaEventRecord(ev[1], s));
-        if (p.precision)
+        if (p.gslices > 0) {
+            const size_t sm = 64 + PAIRS_WARPS * 32 * (p.precision ? sizeof(float4) : sizeof(double4));
+            if (p.precision)
+                k_cn_g<false><<<e->dev_sms * 2, PAIRS_WARPS * 32, sm, s>>>(p, e->gctl.p + 1);
+            else
+                k_cn_g<true><<<e->dev_sms * 2, PAIRS_WARPS * 32, sm, s>>>(p, e->gctl.p + 1);
+            k_group_reduce<<<gb, T, 0, s>>>(p, 1);
+        } else if (p.precision)
             k_cn32<<<gw, T, 0, s>>>(p);
         else
             k_cn<<<gw, T, 0, s>>>(p);
@@ -1934,14 +1961,12 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
             D3_CUDA(cudaMemsetAsync(p.v2, 0, sizeof(double) * 6 * n, s));
         }
         if (p.gslices > 0 && p.shard_world <= 1) {
-            D3_CUDA(cudaMemsetAsync(e->gctl.p, 0, 2 * sizeof(int), s));
-            k_groups<<<(p.nsrow + 127) / 128, 128, 0, s>>>(p);
             const int grid = e->dev_sms * pairs_occupancy(e);
             if (p.precision)
-                k_twobody_g<NR, false><<<grid, PAIRS_WARPS * 32, pairs_smem(e), s>>>(p);
+                k_twobody_g<NR, false><<<grid, PAIRS_WARPS * 32, pairs_smem(e), s>>>(p, e->gctl.p + 2);
             else
-                k_twobody_g<NR, true><<<grid, PAIRS_WARPS * 32, pairs_smem(e), s>>>(p);
-            k_pairs_reduce<<<gb, T, 0, s>>>(p);
+                k_twobody_g<NR, true><<<grid, PAIRS_WARPS * 32, pairs_smem(e), s>>>(p, e->gctl.p + 2);
+            k_group_reduce<<<gb, T, 0, s>>>(p, 0);
         } else if (p.precision)
             k_twobody32<NR><<<gw, T, (size_t)p.ne * p.ne * sizeof(float4), s>>>(p);
         else
@@ -2052,7 +2077,14 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
         D3_CUDA(cudaMemsetAsync(p.fc, 0, sizeof(double) * 3 * n, s));
         D3_CUDA(cudaMemsetAsync(p.vc, 0, sizeof(double) * 6 * n, s));
     }
-    if (p.precision)
+    if (p.gslices > 0 && p.shard_world <= 1) {
+        const size_t sm = 64 + PAIRS_WARPS * 32 * ((p.precision ? sizeof(float4) : sizeof(double4)) + sizeof(double));
+        if (p.precision)
+            k_chain_g<false><<<e->dev_sms * 2, PAIRS_WARPS * 32, sm, s>>>(p, Gsum, e->gctl.p + 3);
+        else
+            k_chain_g<true><<<e->dev_sms * 2, PAIRS_WARPS * 32, sm, s>>>(p, Gsum, e->gctl.p + 3);
+        k_group_reduce<<<gb, T, 0, s>>>(p, 2);
+    } else if (p.precision)
         k_chain32<<<gw, T, 0, s>>>(p, Gsum);
     else
         k_chain<<<gw, T, 0, s>>>(p, Gsum);
@@ -2074,7 +2106,7 @@ int engine_pass_times(Engine *e, float *ms, int cap, unsigned long long *counter
 }
 
 int engine_launches_per_eval(const Engine *e) {
-    const int pairs = pairs_grouped(e) ? 2 : 0; // group cut and slice reduction
+    const int pairs = pairs_grouped(e) ? 4 : 0; // group cut and three slice reductions
     if (!e->use_atm) return 12 + pairs;
     if (e->opt.atm_surrogate && e->surr.loaded) return 20 + pairs;
     return (blockpair_warps(e) > 0 ? 17 : 16) + pairs;

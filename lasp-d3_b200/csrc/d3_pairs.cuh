@@ -11,16 +11,22 @@
 // in that stencil, so a distance test per (i, j) pair is the only filter.
 //
 // Work. A work item is (group, slice of the stencil rows): one warp, lane L owns the
-// group's atom L, partners are staged 32 at a time in the warp's shared memory (position
-// and the C6 rows of the partner at every type: lanes of different types read distinct
-// banks, lanes of one type the same word) and visited by all lanes together. Items are
-// taken from a counter by persistent warps. Each item writes its lanes' sums (energy,
-// dE/dCN, force, virial) to its slice's row of a partial array; k_pairs_reduce adds the
+// group's atom L, partners are staged 32 at a time in the warp's shared memory and visited
+// by all lanes together. Items are taken from a counter by persistent warps. Each item
+// writes its lanes' sums to its slice's row of a partial array; k_group_reduce adds the
 // slices of every atom in a fixed order, so results do not depend on scheduling.
+//
+// Three passes use the same groups: coordination numbers (k_cn_g, rc_CN stencil, the
+// reference's coordination_number_kernel, src/d3_kernel.cu:544-683), the two-body term
+// (k_twobody_g, rc stencil; staged partner data: position and the partner's C6 rows at
+// every type, where lanes of different types read distinct banks and lanes of one type the
+// same word) and the dE/dCN chain rule (k_chain_g, rc_CN stencil, the reference's
+// three_body_kernel, src/d3_kernel.cu:1511-1698; staged: position and dE/dCN).
 
 constexpr int PAIRS_MAX_TYPES = 8;    // staged C6 rows per partner: ne * NR values
 constexpr int PAIRS_WARPS = 8;        // warps per CTA
-constexpr int PAIRS_NSUM = 11;        // e, g, f[3], v[6] per atom and slice
+constexpr int PAIRS_NSUM = 11;        // e, g, f[3], v[6] per atom and slice (two-body; CN
+                                      // uses 1, the chain rule 9 of the 11)
 
 // one super-row: structure, first bin row (y, z) and its row counts (ny | nz << 8)
 // one group:     super-row, bx_lo | bx_hi << 16, position of the first atom in column
@@ -150,14 +156,90 @@ __device__ __forceinline__ void pair_term(const KP &p, R r2, const R *y, const R
     e_half = (R)0.5 * (E6 + E8);
 }
 
-// shared memory of one warp: 32 partner positions and their C6 rows at every type
+// shared memory of one warp: 32 partner positions, their C6 rows at every type (two-body)
+// or their dE/dCN (chain rule)
 template <bool F64>
 __host__ __device__ constexpr size_t pairs_warp_bytes(int ne, int NR) {
-    return 32 * (F64 ? sizeof(double4) : sizeof(float4)) + (size_t)32 * ne * NR * (F64 ? sizeof(double) : sizeof(float));
+    return 32 * (F64 ? sizeof(double4) : sizeof(float4)) +
+           (size_t)32 * (ne * NR > 1 ? ne * NR : 1) * (F64 ? sizeof(double) : sizeof(float)) + 32 * sizeof(double);
+}
+
+// One work item of a grouped pass, as the lanes of a warp see it.
+struct GroupItem {
+    int i;           // this lane's atom (binned), -1 for lanes past the group's count
+    int sl;          // stencil-row slice
+    int4 sr;         // the group's super-row
+    int bx_lo, bx_hi;
+    const SG *g;
+};
+
+__device__ __forceinline__ bool next_item(const KP &p, int *work, GroupItem &it) {
+    const int lane = threadIdx.x & 31;
+    const int S = p.gslices;
+    int k = 0;
+    if (lane == 0) k = atomicAdd(work, 1);
+    k = __shfl_sync(0xffffffffu, k, 0);
+    if (k >= *p.gcount * S) return false;
+    const int gi = k / S;
+    it.sl = k - gi * S;
+    const int4 grp = p.groups[gi];
+    it.sr = p.srows[grp.x];
+    it.g = &p.sg[it.sr.x];
+    it.bx_lo = grp.y & 0xffff;
+    it.bx_hi = grp.y >> 16;
+    it.i = lane < grp.w ? group_atom(p, *it.g, it.sr, it.bx_lo, grp.z, lane) : -1;
+    return true;
+}
+
+// Every contiguous candidate range of the item's slice of a block stencil: body(base, m,
+// ox, oy, oz, px, Ty, Tz) for each chunk of m <= 32 partners starting at binned index base,
+// with this lane's origin o = x_i - T h (rounded once per range). Ranges whose image lies
+// outside the reference's image box are skipped whole unless some atom was given outside
+// the cell (box_pair: the caller tests each pair).
+template <typename R, typename R4, class Body>
+__device__ __forceinline__ void group_ranges(const KP &p, const GroupItem &it, const int4 *rows, int nrows,
+                                             bool box_pair, const R4 &xi, Body &&body) {
+    const SG &g = *it.g;
+    const int S = p.gslices;
+    const int nb0 = g.nb[0], nb1 = g.nb[1], nb2 = g.nb[2];
+    const int *bstart = p.bin_start + g.bin_base;
+    for (int r = it.sl; r < nrows; r += S) {
+        const int4 row = rows[r];
+        const int yy = it.sr.y + row.x, zz = it.sr.z + row.y;
+        const int Ty = floordiv(yy, nb1), Tz = floordiv(zz, nb2);
+        const int byy = yy - Ty * nb1, bzz = zz - Tz * nb2;
+        const int xlo = it.bx_lo + row.z, xhi = it.bx_hi + row.w;
+        const int plo = floordiv(xlo, nb0), phi = floordiv(xhi, nb0);
+        const int rowbase = nb0 * (byy + nb1 * bzz);
+        for (int px = plo; px <= phi; ++px) {
+            if (g.box_mode && !box_pair && (abs(px) > g.half[0] || abs(Ty) > g.half[1] || abs(Tz) > g.half[2]))
+                continue;
+            const int a = max(xlo, px * nb0) - px * nb0;
+            const int b = min(xhi, px * nb0 + nb0 - 1) - px * nb0;
+            const int jlo = bstart[rowbase + a], jhi = bstart[rowbase + b + 1];
+            if (jlo >= jhi) continue;
+            const double shx = px * g.h[0] + Ty * g.h[3] + Tz * g.h[6];
+            const double shy = px * g.h[1] + Ty * g.h[4] + Tz * g.h[7];
+            const double shz = px * g.h[2] + Ty * g.h[5] + Tz * g.h[8];
+            const R ox = (R)((double)xi.x - shx), oy = (R)((double)xi.y - shy), oz = (R)((double)xi.z - shz);
+            for (int base = jlo; base < jhi; base += 32) body(base, min(32, jhi - base), ox, oy, oz, px, Ty, Tz);
+        }
+    }
+}
+
+// CN term of one pair: value and (d CN / d r) / r; optional tanh^3 smooth cutoff (the
+// reference's SMOOTH_CUTOFF_CN)
+template <typename R>
+__device__ __forceinline__ R cn_pair(const KP &p, R r2, R rsum, R *dcn_over_r) {
+    if constexpr (sizeof(R) == 8) {
+        return cn_term(p, sqrt(r2), rsum, dcn_over_r);
+    } else {
+        return cn_term32(p, r2, rsum, dcn_over_r);
+    }
 }
 
 template <int NR, bool F64>
-__global__ void __launch_bounds__(PAIRS_WARPS * 32, F64 ? 1 : 2) k_twobody_g(KP p) {
+__global__ void __launch_bounds__(PAIRS_WARPS * 32, F64 ? 1 : 2) k_twobody_g(KP p, int *work) {
     using R = typename PairReal<F64>::R;
     using R4 = typename PairReal<F64>::R4;
     extern __shared__ __align__(16) unsigned char smp[];
@@ -182,20 +264,10 @@ __global__ void __launch_bounds__(PAIRS_WARPS * 32, F64 ? 1 : 2) k_twobody_g(KP 
     const R *dwsrc = F64 ? reinterpret_cast<const R *>(p.dw) : reinterpret_cast<const R *>(p.dw32);
     const int rowlen = ne * NR;
     const R rc2 = (R)p.rc2;
-    const int S = p.gslices;
-    const int items = *p.gcount * S;
     unsigned long long npair = 0;
-    for (;;) {
-        int it = 0;
-        if (lane == 0) it = atomicAdd(p.gwork, 1);
-        it = __shfl_sync(0xffffffffu, it, 0);
-        if (it >= items) break;
-        const int gi = it / S, sl = it - gi * S;
-        const int4 grp = p.groups[gi];
-        const int4 sr = p.srows[grp.x];
-        const SG &g = p.sg[sr.x];
-        const int bx_lo = grp.y & 0xffff, bx_hi = grp.y >> 16;
-        const int i = lane < grp.w ? group_atom(p, g, sr, bx_lo, grp.z, lane) : -1;
+    GroupItem it;
+    while (next_item(p, work, it)) {
+        const int i = it.i;
         const bool iv = i >= 0;
         R4 xi;
         int ti = 0;
@@ -216,85 +288,59 @@ __global__ void __launch_bounds__(PAIRS_WARPS * 32, F64 ? 1 : 2) k_twobody_g(KP 
 #pragma unroll
             for (int b = 0; b < NR; ++b) wi[b] = dwi[b] = (R)0;
         }
-        // exact image-box test per pair only when atoms were given outside the cell
-        const bool box_pair = g.box_mode && p.anyshift[sr.x];
+        const SG &g = *it.g;
+        const bool box_pair = g.box_mode && p.anyshift[it.sr.x];
         double E = 0, Gd = 0, FX = 0, FY = 0, FZ = 0, V[6] = {0, 0, 0, 0, 0, 0};
-        const int nb0 = g.nb[0], nb1 = g.nb[1], nb2 = g.nb[2];
-        const int *bstart = p.bin_start + g.bin_base;
-        const int4 *rows = p.stencils + g.st2b_off;
-        for (int r = sl; r < g.st2b_n; r += S) {
-            const int4 row = rows[r];
-            const int yy = sr.y + row.x, zz = sr.z + row.y;
-            const int Ty = floordiv(yy, nb1), Tz = floordiv(zz, nb2);
-            const int byy = yy - Ty * nb1, bzz = zz - Tz * nb2;
-            const int xlo = bx_lo + row.z, xhi = bx_hi + row.w;
-            const int plo = floordiv(xlo, nb0), phi = floordiv(xhi, nb0);
-            const int rowbase = nb0 * (byy + nb1 * bzz);
-            for (int px = plo; px <= phi; ++px) {
-                if (g.box_mode && !box_pair &&
-                    (abs(px) > g.half[0] || abs(Ty) > g.half[1] || abs(Tz) > g.half[2]))
-                    continue; // outside the reference's image box for every pair of the range
-                const int a = max(xlo, px * nb0) - px * nb0;
-                const int b = min(xhi, px * nb0 + nb0 - 1) - px * nb0;
-                const int jlo = bstart[rowbase + a], jhi = bstart[rowbase + b + 1];
-                if (jlo >= jhi) continue;
-                const double shx = px * g.h[0] + Ty * g.h[3] + Tz * g.h[6];
-                const double shy = px * g.h[1] + Ty * g.h[4] + Tz * g.h[7];
-                const double shz = px * g.h[2] + Ty * g.h[5] + Tz * g.h[8];
-                // origin of this range: x_i - T h (rounded once)
-                const R ox = (R)((double)xi.x - shx), oy = (R)((double)xi.y - shy), oz = (R)((double)xi.z - shz);
-                for (int base = jlo; base < jhi; base += 32) {
-                    const int m = min(32, jhi - base);
-                    __syncwarp();
-                    if (lane < m) sP[lane] = xsrc[base + lane];
-                    {
-                        const R *src = Ysrc + (size_t)base * rowlen;
-                        const int tot = m * rowlen;
-                        for (int k = lane; k < tot; k += 32) sY[k] = src[k];
-                    }
-                    __syncwarp();
-                    R e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
-                    for (int jj = 0; jj < m; ++jj) {
-                        const R4 xj = sP[jj];
-                        const R dx = ox - xj.x, dy = oy - xj.y, dz = oz - xj.z;
-                        const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-                        bool act = iv && r2 < rc2 && r2 > (R)0;
-                        if (box_pair && act) act = in_box(g, si, p.shift[base + jj], px, Ty, Tz);
-                        if (!act) continue;
-                        ++npair;
-                        const int tj = (int)xj.w;
-                        const R *tp = ptab + 3 * (ti * ne + tj);
-                        R eh, Gt, fs;
-                        pair_term<NR, R>(p, r2, sY + jj * rowlen + ti * NR, wi, dwi, tp[0], tp[1], tp[2], eh, Gt, fs);
-                        e += eh;
-                        Gd += (double)Gt;
-                        fx = fma(fs, dx, fx);
-                        fy = fma(fs, dy, fy);
-                        fz = fma(fs, dz, fz);
-                        const R fdx = fs * dx, fdy = fs * dy;
-                        vxx = fma(fdx, dx, vxx);
-                        vyy = fma(fdy, dy, vyy);
-                        vzz = fma(fs * dz, dz, vzz);
-                        vxy = fma(fdx, dy, vxy);
-                        vxz = fma(fdx, dz, vxz);
-                        vyz = fma(fdy, dz, vyz);
-                    }
-                    // blocked summation: 32-partner sums carried in FP64
-                    E += e;
-                    FX += fx;
-                    FY += fy;
-                    FZ += fz;
-                    V[0] += vxx;
-                    V[1] += vyy;
-                    V[2] += vzz;
-                    V[3] += vxy;
-                    V[4] += vxz;
-                    V[5] += vyz;
-                }
+        group_ranges<R, R4>(p, it, p.stencils + g.st2b_off, g.st2b_n, box_pair, xi,
+                            [&](int base, int m, R ox, R oy, R oz, int px, int Ty, int Tz) {
+            __syncwarp();
+            if (lane < m) sP[lane] = xsrc[base + lane];
+            {
+                const R *src = Ysrc + (size_t)base * rowlen;
+                const int tot = m * rowlen;
+                for (int k = lane; k < tot; k += 32) sY[k] = src[k];
             }
-        }
+            __syncwarp();
+            R e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+            for (int jj = 0; jj < m; ++jj) {
+                const R4 xj = sP[jj];
+                const R dx = ox - xj.x, dy = oy - xj.y, dz = oz - xj.z;
+                const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                bool act = iv && r2 < rc2 && r2 > (R)0;
+                if (box_pair && act) act = in_box(g, si, p.shift[base + jj], px, Ty, Tz);
+                if (!act) continue;
+                ++npair;
+                const int tj = (int)xj.w;
+                const R *tp = ptab + 3 * (ti * ne + tj);
+                R eh, Gt, fs;
+                pair_term<NR, R>(p, r2, sY + jj * rowlen + ti * NR, wi, dwi, tp[0], tp[1], tp[2], eh, Gt, fs);
+                e += eh;
+                Gd += (double)Gt;
+                fx = fma(fs, dx, fx);
+                fy = fma(fs, dy, fy);
+                fz = fma(fs, dz, fz);
+                const R fdx = fs * dx, fdy = fs * dy;
+                vxx = fma(fdx, dx, vxx);
+                vyy = fma(fdy, dy, vyy);
+                vzz = fma(fs * dz, dz, vzz);
+                vxy = fma(fdx, dy, vxy);
+                vxz = fma(fdx, dz, vxz);
+                vyz = fma(fdy, dz, vyz);
+            }
+            // blocked summation: 32-partner sums carried in FP64
+            E += e;
+            FX += fx;
+            FY += fy;
+            FZ += fz;
+            V[0] += vxx;
+            V[1] += vyy;
+            V[2] += vzz;
+            V[3] += vxy;
+            V[4] += vxz;
+            V[5] += vyz;
+        });
         if (iv) {
-            double *o = p.gpart + ((size_t)sl * p.n + i) * PAIRS_NSUM;
+            double *o = p.gpart + ((size_t)it.sl * p.n + i) * PAIRS_NSUM;
             o[0] = E;
             o[1] = Gd;
             o[2] = FX;
@@ -308,25 +354,177 @@ __global__ void __launch_bounds__(PAIRS_WARPS * 32, F64 ? 1 : 2) k_twobody_g(KP 
     if (lane == 0 && npair) atomicAdd(&p.counters[1], npair);
 }
 
-// per atom: the slices' sums in a fixed order -> two-body energy, dE/dCN, force, virial
-__global__ void k_pairs_reduce(KP p) {
+// coordination numbers on atom groups (rc_CN stencil): 0 < r^2 <= rc_CN^2
+template <bool F64>
+__global__ void __launch_bounds__(PAIRS_WARPS * 32, 2) k_cn_g(KP p, int *work) {
+    using R = typename PairReal<F64>::R;
+    using R4 = typename PairReal<F64>::R4;
+    extern __shared__ __align__(16) unsigned char smp[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    R *rcov = reinterpret_cast<R *>(smp);
+    for (int k = threadIdx.x; k < p.ne; k += blockDim.x) rcov[k] = (R)p.rcov[k];
+    __syncthreads();
+    const size_t tab_bytes = ((size_t)PAIRS_MAX_TYPES * sizeof(double) + 15) & ~(size_t)15;
+    R4 *sP = reinterpret_cast<R4 *>(smp + tab_bytes + (size_t)warp * 32 * sizeof(R4));
+    const R4 *xsrc = F64 ? reinterpret_cast<const R4 *>(p.xs) : reinterpret_cast<const R4 *>(p.xs32);
+    const R rcn2 = (R)p.rcn2;
+    unsigned long long npair = 0;
+    GroupItem it;
+    while (next_item(p, work, it)) {
+        const int i = it.i;
+        const bool iv = i >= 0;
+        R4 xi;
+        xi.x = xi.y = xi.z = xi.w = (R)0;
+        int4 si = make_int4(0, 0, 0, 0);
+        if (iv) {
+            xi = xsrc[i];
+            si = p.shift[i];
+        }
+        const R ri = rcov[(int)xi.w];
+        const SG &g = *it.g;
+        const bool box_pair = g.box_mode && p.anyshift[it.sr.x];
+        double CN = 0;
+        group_ranges<R, R4>(p, it, p.stencils + g.stcb_off, g.stcb_n, box_pair, xi,
+                            [&](int base, int m, R ox, R oy, R oz, int px, int Ty, int Tz) {
+            __syncwarp();
+            if (lane < m) sP[lane] = xsrc[base + lane];
+            __syncwarp();
+            R c = 0;
+            for (int jj = 0; jj < m; ++jj) {
+                const R4 xj = sP[jj];
+                const R dx = ox - xj.x, dy = oy - xj.y, dz = oz - xj.z;
+                const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                bool act = iv && r2 <= rcn2 && r2 > (R)0;
+                if (box_pair && act) act = in_box(g, si, p.shift[base + jj], px, Ty, Tz);
+                if (!act) continue;
+                ++npair;
+                R d;
+                c += cn_pair<R>(p, r2, ri + rcov[(int)xj.w], &d);
+            }
+            CN += c;
+        });
+        if (iv) p.gpart[((size_t)it.sl * p.n + i) * PAIRS_NSUM] = CN;
+    }
+    for (int o = 16; o > 0; o >>= 1) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+    if (lane == 0 && npair) atomicAdd(&p.counters[2], npair);
+}
+
+// dE/dCN chain rule on atom groups (rc_CN stencil): F_i += (dE/dCN_i + dE/dCN_j) dCN_ij/dr r_ij / r
+template <bool F64>
+__global__ void __launch_bounds__(PAIRS_WARPS * 32, 2) k_chain_g(KP p, const double *Gd, int *work) {
+    using R = typename PairReal<F64>::R;
+    using R4 = typename PairReal<F64>::R4;
+    extern __shared__ __align__(16) unsigned char smp[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    R *rcov = reinterpret_cast<R *>(smp);
+    for (int k = threadIdx.x; k < p.ne; k += blockDim.x) rcov[k] = (R)p.rcov[k];
+    __syncthreads();
+    const size_t tab_bytes = ((size_t)PAIRS_MAX_TYPES * sizeof(double) + 15) & ~(size_t)15;
+    unsigned char *wb = smp + tab_bytes + (size_t)warp * 32 * (sizeof(R4) + sizeof(double));
+    R4 *sP = reinterpret_cast<R4 *>(wb);
+    double *sG = reinterpret_cast<double *>(wb + 32 * sizeof(R4));
+    const R4 *xsrc = F64 ? reinterpret_cast<const R4 *>(p.xs) : reinterpret_cast<const R4 *>(p.xs32);
+    const R rcn2 = (R)p.rcn2;
+    GroupItem it;
+    while (next_item(p, work, it)) {
+        const int i = it.i;
+        const bool iv = i >= 0;
+        R4 xi;
+        xi.x = xi.y = xi.z = xi.w = (R)0;
+        int4 si = make_int4(0, 0, 0, 0);
+        double gi = 0;
+        if (iv) {
+            xi = xsrc[i];
+            si = p.shift[i];
+            gi = Gd[i];
+        }
+        const R ri = rcov[(int)xi.w];
+        const SG &g = *it.g;
+        const bool box_pair = g.box_mode && p.anyshift[it.sr.x];
+        double F[3] = {0, 0, 0}, V[6] = {0, 0, 0, 0, 0, 0};
+        group_ranges<R, R4>(p, it, p.stencils + g.stcb_off, g.stcb_n, box_pair, xi,
+                            [&](int base, int m, R ox, R oy, R oz, int px, int Ty, int Tz) {
+            __syncwarp();
+            if (lane < m) {
+                sP[lane] = xsrc[base + lane];
+                sG[lane] = Gd[base + lane];
+            }
+            __syncwarp();
+            R fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
+            for (int jj = 0; jj < m; ++jj) {
+                const R4 xj = sP[jj];
+                const R dx = ox - xj.x, dy = oy - xj.y, dz = oz - xj.z;
+                const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                bool act = iv && r2 <= rcn2 && r2 > (R)0;
+                if (box_pair && act) act = in_box(g, si, p.shift[base + jj], px, Ty, Tz);
+                if (!act) continue;
+                R dcn;
+                cn_pair<R>(p, r2, ri + rcov[(int)xj.w], &dcn);
+                const R dE = (R)(gi + sG[jj]) * dcn;
+                const R fdx = dE * dx, fdy = dE * dy;
+                fx += fdx;
+                fy += fdy;
+                fz = fma(dE, dz, fz);
+                vxx = fma(fdx, dx, vxx);
+                vyy = fma(fdy, dy, vyy);
+                vzz = fma(dE * dz, dz, vzz);
+                vxy = fma(fdx, dy, vxy);
+                vxz = fma(fdx, dz, vxz);
+                vyz = fma(fdy, dz, vyz);
+            }
+            F[0] += fx;
+            F[1] += fy;
+            F[2] += fz;
+            V[0] += vxx;
+            V[1] += vyy;
+            V[2] += vzz;
+            V[3] += vxy;
+            V[4] += vxz;
+            V[5] += vyz;
+        });
+        if (iv) {
+            double *o = p.gpart + ((size_t)it.sl * p.n + i) * PAIRS_NSUM;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) o[k] = F[k];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) o[3 + k] = V[k];
+        }
+    }
+}
+
+// per atom: the slices' sums in a fixed order. what: 0 two-body (energy, dE/dCN, force,
+// virial), 1 CN, 2 chain rule (force, virial)
+__global__ void k_group_reduce(KP p, int what) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.n) return;
+    const int nsum = what == 0 ? PAIRS_NSUM : (what == 1 ? 1 : 9);
     double acc[PAIRS_NSUM];
 #pragma unroll
     for (int k = 0; k < PAIRS_NSUM; ++k) acc[k] = 0.0;
     for (int s = 0; s < p.gslices; ++s) {
         const double *o = p.gpart + ((size_t)s * p.n + i) * PAIRS_NSUM;
 #pragma unroll
-        for (int k = 0; k < PAIRS_NSUM; ++k) acc[k] += o[k];
+        for (int k = 0; k < PAIRS_NSUM; ++k)
+            if (k < nsum) acc[k] += o[k];
     }
-    p.e2[i] = acc[0];
-    p.g2[i] = acc[1];
-    p.f2[3 * i] = acc[2];
-    p.f2[3 * i + 1] = acc[3];
-    p.f2[3 * i + 2] = acc[4];
     const double sc = -1.0 / (2.0 * p.sg[p.sid[i]].vol);
-    double *v = p.v2 + 6 * (size_t)i;
+    if (what == 1) {
+        p.cn[i] = acc[0];
+    } else if (what == 0) {
+        p.e2[i] = acc[0];
+        p.g2[i] = acc[1];
+        p.f2[3 * i] = acc[2];
+        p.f2[3 * i + 1] = acc[3];
+        p.f2[3 * i + 2] = acc[4];
+        double *v = p.v2 + 6 * (size_t)i;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) v[k] = acc[5 + k] * sc;
+        for (int k = 0; k < 6; ++k) v[k] = acc[5 + k] * sc;
+    } else {
+        p.fc[3 * i] = acc[0];
+        p.fc[3 * i + 1] = acc[1];
+        p.fc[3 * i + 2] = acc[2];
+        double *v = p.vc + 6 * (size_t)i;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) v[k] = acc[3 + k] * sc;
+    }
 }
