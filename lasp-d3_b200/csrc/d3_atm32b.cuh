@@ -479,7 +479,36 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             }
         }
         __syncthreads();
+        // scatter the entry numbers, then order each cell's entries by entry number: the
+        // sorted order (and so the blocks) is then the same in every CTA that sorts this
+        // apex, which the apex split relies on (each split walks its own share of block rows)
         for (int k = tid; k < m; k += blockDim.x) {
+            const int2 ent = p.atm_ent[e0 + k];
+            const double4 xj = p.xs[ent.x];
+            double sx, sy, sz;
+            image_vec(g, sext8(ent.y & 0xff), sext8((ent.y >> 8) & 0xff), sext8((ent.y >> 16) & 0xff), sx, sy, sz);
+            const int cx = min(ATMB_GRID - 1, max(0, (int)((xj.x + sx - xa.x + rc) * cinv)));
+            const int cy = min(ATMB_GRID - 1, max(0, (int)((xj.y + sy - xa.y + rc) * cinv)));
+            const int cz = min(ATMB_GRID - 1, max(0, (int)((xj.z + sz - xa.z + rc) * cinv)));
+            sjy[atomicAdd(&cellpos[atmb_hilbert(cx, cy, cz)], 1)] = k;
+        }
+        __syncthreads();
+        // cell c now spans [end of cell c - 1, cellpos[c]); cells hold a few entries each
+        for (int c = tid; c < ATMB_CELLS; c += blockDim.x) {
+            const int lo = c ? cellpos[c - 1] : 0, hi = cellpos[c];
+            for (int q = lo + 1; q < hi; ++q) {
+                const int v = sjy[q];
+                int r = q - 1;
+                while (r >= lo && sjy[r] > v) {
+                    sjy[r + 1] = sjy[r];
+                    --r;
+                }
+                sjy[r + 1] = v;
+            }
+        }
+        __syncthreads();
+        for (int pos = tid; pos < m; pos += blockDim.x) {
+            const int k = sjy[pos];
             const int2 ent = p.atm_ent[e0 + k];
             const int jp = ent.x;
             const double4 xj = p.xs[jp];
@@ -487,10 +516,6 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             double sx, sy, sz;
             image_vec(g, sext8(ent.y & 0xff), sext8((ent.y >> 8) & 0xff), sext8((ent.y >> 16) & 0xff), sx, sy, sz);
             const double vx = xj.x + sx - xa.x, vy = xj.y + sy - xa.y, vz = xj.z + sz - xa.z;
-            const int cx = min(ATMB_GRID - 1, max(0, (int)((vx + rc) * cinv)));
-            const int cy = min(ATMB_GRID - 1, max(0, (int)((vy + rc) * cinv)));
-            const int cz = min(ATMB_GRID - 1, max(0, (int)((vz + rc) * cinv)));
-            const int pos = atomicAdd(&cellpos[atmb_hilbert(cx, cy, cz)], 1);
             const double d2 = vx * vx + vy * vy + vz * vz;
             const double *ya = yapex + tp * NR;                   // C6_ae = y_{a,tp} . w_e
             const double *yq = p.Y + ((size_t)jp * ne + ta) * NR; // dC6_ae/dCN_a = y_{e,ta} . dw_a
@@ -506,7 +531,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             sB[pos] = make_float4((float)(1.0 / sqrt(d2)), (float)(1.0 / d2), (float)sqrt(c6),
                                   (float)pow((double)r0sq[ta * ne + tp] / d2, 8.0 / 3.0));
             sJ[pos] = make_float4(__int_as_float(jp), __int_as_float(tp), (float)(dcq / c6), (float)(dca / c6));
-            sjy[pos] = jp;
+            sjy[pos] = jp; // this thread's own slot: the entry number it replaces was read above
         }
         __syncthreads();
         // ---- block bounding boxes

@@ -1705,6 +1705,15 @@ static AtmbShape blockpair_shape(const Engine *e) {
         // the entry sort's cell counters live in the warps' staging area
         if (w >= 2 && mcap >= ATMB_MCAP_MIN && w * per >= ATMB_CELLS * sizeof(int)) return {w, ctas, mcap, nbuf};
     }
+    // default: up to 12 warps with one y buffer each (three warps per scheduler hide each
+    // other's copies; measured 266 ms against 288 ms with 8 double-buffered warps on the
+    // 20,000-atom box), as long as the shared memory leaves a list capacity of 4,096
+    for (int w = ATMB_MAXW1; w > ATMB_MAXW; --w) {
+        const size_t per1 = atmb_smem_warp(e->ne, e->nref, 1);
+        int mcap = ATMB_MCAP_MAX;
+        while (mcap >= ATMB_MCAP_MIN && atmb_smem_fixed(e->ne, e->nref, mcap) + w * per1 > limit) mcap -= 512;
+        if (mcap >= ATMB_MCAP_MIN && w * per1 >= ATMB_CELLS * sizeof(int)) return {w, 1, mcap, 1};
+    }
     const size_t per = atmb_smem_warp(e->ne, e->nref);
     // two CTAs of four warps per SM, so that one CTA's per-apex sort and set-up overlap the
     // other's block pairs, when both fit the SM's 228 KB (each with 2 KB for the static

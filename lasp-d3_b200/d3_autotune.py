@@ -4,8 +4,8 @@ Tunables (engine options):
   D3_OPT_BIN_DIVISOR        cell-list bin width = smallest cutoff / divisor   (pair passes)
   D3_OPT_PAIR_KERNEL        two-body threads per atom: 1 (groups of 32 atoms,  (two-body)
                             one lane each) or 32 (one warp per atom)
-  D3_OPT_ATMB_WARPS         block-pair ATM kernel: warps per CTA (8 with two   (ATM pass,
-                            y buffers per warp, 12 with one)                     precision)
+  D3_OPT_ATMB_WARPS         block-pair ATM kernel: warps per CTA (up to 8 with (ATM pass,
+                            two y buffers per warp, 9-12 with one)               precision)
   D3_OPT_ATM_CTAS_PER_SM    CTAs per SM (block-pair: 2 CTAs of 4 warps when they fit;
                             mirror / FP64 kernels: persistent CTAs per SM)
   D3_OPT_ATMB_LIST_CAPACITY longest list of the block-pair kernel (the rest go to the
@@ -33,7 +33,7 @@ PAIR_KERNELS = (0, 1)
 ATM_TILES = (64, 128, 256)
 ATM_CTAS = (0, 2, 3)
 # block-pair shapes: (warps per CTA, CTAs per SM, list capacity; 0 = automatic)
-ATMB_SHAPES = ((0, 0, 0), (12, 0, 0), (6, 0, 0), (4, 2, 0), (8, 0, 4096))
+ATMB_SHAPES = ((0, 0, 0), (8, 0, 0), (10, 0, 0), (4, 2, 0), (12, 0, 4096))
 
 
 def cache_path():

@@ -22,8 +22,8 @@ class FakeHandle:
     def pass_times(self):
         o = self.opt.get
         pair = 10.0 + abs(o(OPT_BIN_DIVISOR, 6) - 4) + (3.0 if o(OPT_PAIR_KERNEL, 0) == 1 else 0.0)
-        # precision optimum: 12 warps; FP64 optimum: tile 128, 2 CTAs per SM
-        atm = 100.0 - (20.0 if o(OPT_ATMB_WARPS, 0) == 12 else 0.0) + (5.0 if o(OPT_ATMB_LIST_CAPACITY, 0) else 0.0)
+        # precision optimum: 10 warps; FP64 optimum: tile 128, 2 CTAs per SM
+        atm = 100.0 - (20.0 if o(OPT_ATMB_WARPS, 0) == 10 else 0.0) + (5.0 if o(OPT_ATMB_LIST_CAPACITY, 0) else 0.0)
         atm += abs(o(OPT_ATM_TILE, 0) - 128) / 64.0 + (0.0 if o(OPT_ATM_CTAS_PER_SM, 0) == 2 else 1.0)
         return {"bin": 0.0, "cn": 0.0, "twobody": pair, "atm_list": 0.0, "atm": atm, "chain": 0.0, "finalize": 0.0}, None
 
@@ -36,7 +36,7 @@ def test_tuner_keeps_the_fastest_candidates(tmp_path, monkeypatch, precision):
     res = d3_autotune.tune(h, key, repeats=1)
     assert res["bin_divisor"] == 4 and res["pair_kernel"] == 0
     if precision:
-        assert res["atmb_warps"] == 12 and res["atmb_mcap"] == 0
+        assert res["atmb_warps"] == 10 and res["atmb_mcap"] == 0
         assert len([t for t in res["trials"] if "atmb_warps" in t]) == len(d3_autotune.ATMB_SHAPES)
     else:
         assert res["atm_tile"] == 128 and res["atm_ctas_per_sm"] == 2

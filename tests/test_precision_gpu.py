@@ -112,13 +112,13 @@ def test_atm_schedules_agree(case):
     assert np.abs(a0 - a1).max() <= 1e-6 * np.abs(a1).max()
 
 
-@pytest.mark.parametrize("shape", [(12, 0, 0, 0), (4, 2, 0, 0), (6, 0, 4096, 0), (12, 0, 4096, 0), (0, 0, 0, 3),
-                                   (12, 0, 0, 5)])
+@pytest.mark.parametrize("shape", [(8, 0, 0, 0), (4, 2, 0, 0), (6, 0, 4096, 0), (12, 0, 4096, 0), (0, 0, 0, 3),
+                                   (8, 0, 0, 5)])
 @pytest.mark.parametrize("case", ["tric", "fe"])
 def test_block_pair_shapes_agree(case, shape):
     """Launch shapes of the block-pair ATM kernel (warps per CTA, CTAs per SM, list
-    capacity, CTAs sharing an apex; 12 warps stage one y block at a time) against the
-    default shape: the same in-range triplets and the same results to FP32 level. A
+    capacity, CTAs sharing an apex; above 8 warps each stages one y block at a time, 8
+    and fewer two) against the default shape (12 warps where they fit): the same in-range triplets and the same results to FP32 level. A
     4,096-entry capacity sends the longest lists of the 3,000-atom box (up to about 4,100
     entries at rc_ATM 40) to the mirror kernel; a split of 3 or 5 makes several CTAs add
     their shares of each apex."""
