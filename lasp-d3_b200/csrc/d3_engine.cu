@@ -607,9 +607,14 @@ __global__ void k_atm_list(KP p) {
         return;
     }
     const bool full = p.atm_center != 0;
+    // the image box needs each partner's wrap shift only when some atom was given outside
+    // the cell; otherwise the test is on the image alone
+    const bool box_pair = g.box_mode && p.anyshift[p.sid[a]];
     traverse(p, g, p.bin_s[a], p.stencils + g.sta_off, g.sta_n, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         bool keep = false;
-        if (act && (full || p.orig[j] <= oa) && in_box(g, sa, p.shift[j], Tx, Ty, Tz)) {
+        const bool inbox = box_pair ? in_box(g, sa, p.shift[j], Tx, Ty, Tz)
+                                    : !(g.box_mode && (abs(Tx) > g.half[0] || abs(Ty) > g.half[1] || abs(Tz) > g.half[2]));
+        if (act && (full || p.orig[j] <= oa) && inbox) {
             const double4 xj = p.xs[j];
             const double dx = xa.x - (xj.x + sh.x), dy = xa.y - (xj.y + sh.y), dz = xa.z - (xj.z + sh.z);
             const double d2 = dx * dx + dy * dy + dz * dz;
