@@ -612,9 +612,10 @@ __global__ void k_atm_list(KP p) {
     const bool box_pair = g.box_mode && p.anyshift[p.sid[a]];
     traverse(p, g, p.bin_s[a], p.stencils + g.sta_off, g.sta_n, [&](int j, int Tx, int Ty, int Tz, const double3 &sh, bool act) {
         bool keep = false;
-        const bool inbox = box_pair ? in_box(g, sa, p.shift[j], Tx, Ty, Tz)
-                                    : !(g.box_mode && (abs(Tx) > g.half[0] || abs(Ty) > g.half[1] || abs(Tz) > g.half[2]));
-        if (act && (full || p.orig[j] <= oa) && inbox) {
+        // (act first: j is a valid index only for active lanes)
+        if (act && (full || p.orig[j] <= oa) &&
+            (box_pair ? in_box(g, sa, p.shift[j], Tx, Ty, Tz)
+                      : !(g.box_mode && (abs(Tx) > g.half[0] || abs(Ty) > g.half[1] || abs(Tz) > g.half[2])))) {
             const double4 xj = p.xs[j];
             const double dx = xa.x - (xj.x + sh.x), dy = xa.y - (xj.y + sh.y), dz = xa.z - (xj.z + sh.z);
             const double d2 = dx * dx + dy * dy + dz * dz;
