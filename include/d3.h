@@ -134,10 +134,13 @@ enum {
     D3_OPT_ATMB_LIST_CAPACITY = 12, /* longest half list (entries) the block-pair kernel takes,
                                     0 = as many as the shared memory allows (4,096..8,192);
                                     longer lists go to the mirror-symmetric kernel */
-    D3_OPT_ATMB_SPLIT = 13       /* CTAs of the block-pair kernel sharing one apex, each taking
+    D3_OPT_ATMB_SPLIT = 13,      /* CTAs of the block-pair kernel sharing one apex, each taking
                                     every S-th block row (0 = automatic: more than one only
                                     when the apexes are fewer than about 4 per CTA, e.g. the
                                     96-atom water box; 1..64) */
+    D3_OPT_ATMB_FINE_SKIP = 14   /* block-pair kernel: 1 skips out-of-range visits per two
+                                    steps, 0 (default) per four steps (more overlap of the
+                                    packed pairs) */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);
 

@@ -266,6 +266,7 @@ int d3_set_option(d3_handle_t *handle, int option, int value) {
         break;
     case D3_OPT_ATMB_LIST_CAPACITY: o.atmb_mcap = value < 0 ? 0 : value; break;
     case D3_OPT_ATMB_SPLIT: o.atmb_split = value < 0 ? 0 : value; break;
+    case D3_OPT_ATMB_FINE_SKIP: o.atmb_fine_skip = value != 0; break;
     case D3_OPT_PAIR_KERNEL:
         if (value != 0 && value != 1) {
             set_error("D3_OPT_PAIR_KERNEL takes 0 (atom groups) or 1 (one warp per atom)");

@@ -388,7 +388,13 @@ __device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 
 // NBUF = 2: the next y block is copied while the current one is visited (up to 8 warps
 // per CTA fit the shared memory); NBUF = 1: copy, wait, visit, which leaves room for 12
 // warps (three per scheduler) whose visits hide each other's copies
-template <int NR, int NBUF>
+// SIMPLE: this launch takes only the apexes of weight-free structures (no atom twice in a
+// list), whose visits skip the repeated-index weights; the other launch takes the rest.
+// Each instance then carries only the live values of its own visit form.
+// FINE: a packed pair of steps is skipped when no lane has an in-range visit in it (else a
+// group of four steps is skipped only when all four are out of range): fewer visit slots,
+// less overlap between the two packed pairs of an iteration
+template <int NR, int NBUF, bool SIMPLE, bool FINE>
 __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) k_atm32b(KP p, float4 *scratch) {
     extern __shared__ __align__(16) unsigned char smb[];
     const int ne = p.ne;
@@ -441,7 +447,8 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         const double4 xa = p.xs[a];
         const int ta = (int)xa.w;
         const SG &g = p.sg[p.sid[a]];
-        const bool simple = g.atm_simple != 0;
+        if ((g.atm_simple != 0) != SIMPLE) continue; // the other instance takes this apex
+        constexpr bool simple = SIMPLE;
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
         for (int k = tid; k < ATMB_CELLS; k += blockDim.x) cellpos[k] = 0;
         if (tid == 0) s_row = 0;
@@ -722,18 +729,17 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                         any |= a0q[pq] | a1q[pq];
                         nv += (a0q[pq] ? 2 : 0) + (a1q[pq] ? 2 : 0);
                     }
-                    if (__any_sync(0xffffffffu, any)) {
-                        if (simple) {
+                    if constexpr (FINE) {
 #pragma unroll
-                            for (int pq = 0; pq < 2; ++pq)
-                                atmb_visit2<NR, true>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0, yQ1,
-                                                      yrow_x, a, third, force_scaled, xt, ys[pq], apx);
-                        } else {
+                        for (int pq = 0; pq < 2; ++pq)
+                            if (__any_sync(0xffffffffu, a0q[pq] | a1q[pq]))
+                                atmb_visit2<NR, simple>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0,
+                                                        yQ1, yrow_x, a, third, force_scaled, xt, ys[pq], apx);
+                    } else if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
-                            for (int pq = 0; pq < 2; ++pq)
-                                atmb_visit2<NR, false>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0, yQ1,
-                                                       yrow_x, a, third, force_scaled, xt, ys[pq], apx);
-                        }
+                        for (int pq = 0; pq < 2; ++pq)
+                            atmb_visit2<NR, simple>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0, yQ1,
+                                                    yrow_x, a, third, force_scaled, xt, ys[pq], apx);
                     }
                     const int src = (lane + 4) & 31;
                     ys[0].shift(src);
@@ -765,7 +771,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                 xs[4] += tWy;
                 xs[5] += tWz;
                 xs[6] += tSA;
-                if (simple) { // U = W
+                if constexpr (simple) { // U = W
                     xs[7] += tWx;
                     xs[8] += tWy;
                     xs[9] += tWz;

@@ -30,6 +30,7 @@
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
+#include <type_traits>
 
 #include "d3_mlp.h"
 #include "d3_synth_params.h"
@@ -1194,7 +1195,7 @@ struct Engine {
         const void *fn = nullptr;
         size_t sm = 0;
         int blocks = 1;
-    } atm_occ_cache[8];
+    } atm_occ_cache[12]; // 0-3 mirror / FP64 ATM, 5 grouped two-body, 8-11 block-pair ATM
     SurrState surr;
     int shard_rank = 0, shard_world = 0; // set by engine_shard_begin
 
@@ -1888,6 +1889,12 @@ static KP make_kp(Engine *e) {
     return p;
 }
 
+// the block-pair ATM kernel instance of a buffering, apex kind and skip granularity
+template <int NR, int NBUF, bool SIMPLE>
+static const void *blockpair_fn(bool fine) {
+    return fine ? (const void *)k_atm32b<NR, NBUF, SIMPLE, true> : (const void *)k_atm32b<NR, NBUF, SIMPLE, false>;
+}
+
 // dynamic shared memory attribute and occupancy of an ATM kernel, cached per kernel and
 // size so that evaluations inside a CUDA-graph capture make no such host calls
 static int atm_occupancy(Engine *e, int which, size_t sm, const void *fn) {
@@ -1900,6 +1907,18 @@ static int atm_occupancy(Engine *e, int which, size_t sm, const void *fn) {
     c.sm = sm;
     c.blocks = std::max(1, blocks);
     return c.blocks;
+}
+
+// one launch of the block-pair ATM kernel for the apexes of one kind (weight-free or not)
+template <int NR>
+static void launch_blockpair(Engine *e, const KP &p, cudaStream_t s, const AtmbShape &shb, bool simple, int grid,
+                             size_t smb) {
+    const bool fine = e->opt.atmb_fine_skip != 0;
+    const void *fn = shb.nbuf == 2 ? (simple ? blockpair_fn<NR, 2, true>(fine) : blockpair_fn<NR, 2, false>(fine))
+                                   : (simple ? blockpair_fn<NR, 1, true>(fine) : blockpair_fn<NR, 1, false>(fine));
+    atm_occupancy(e, 8 + (shb.nbuf == 2 ? 0 : 2) + (simple ? 1 : 0), smb, fn);
+    void *args[] = {(void *)&p, (void *)&e->atmb_scratch.p};
+    D3_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(32 * shb.warps), args, smb, s));
 }
 
 static SurrDesc surr_desc(const int *chan, int nch, float *G, const float *dEdG, int *center) {
@@ -2044,12 +2063,15 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
                     // lists up to shb.mcap entries: block-pair schedule; longer ones below
                     const size_t smb =
                         atmb_smem_fixed(p.ne, NR, shb.mcap) + (size_t)nwb * atmb_smem_warp(p.ne, NR, shb.nbuf);
-                    if (shb.nbuf == 2) {
-                        atm_occupancy(e, 4, smb, (const void *)k_atm32b<NR, 2>);
-                        k_atm32b<NR, 2><<<e->dev_sms * shb.ctas, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
-                    } else {
-                        atm_occupancy(e, 6, smb, (const void *)k_atm32b<NR, 1>);
-                        k_atm32b<NR, 1><<<e->dev_sms * shb.ctas, 32 * nwb, smb, s>>>(p, e->atmb_scratch.p);
+                    // one launch per apex kind present: weight-free structures (every cell
+                    // height above 2 rc_ATM) and the others
+                    bool kind[2] = {false, false};
+                    for (const SG &q : e->sg) kind[q.atm_simple ? 1 : 0] = true;
+                    const int grid = e->dev_sms * shb.ctas;
+                    for (int k = 1; k >= 0; --k) {
+                        if (!kind[k]) continue;
+                        if (k == 0 && kind[1]) D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
+                        launch_blockpair<NR>(e, p, s, shb, k == 1, grid, smb);
                     }
                     D3_CUDA(cudaMemsetAsync(p.work, 0, sizeof(int), s));
                     pc.atm_min_m = shb.mcap;

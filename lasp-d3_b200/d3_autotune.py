@@ -10,6 +10,7 @@ Tunables (engine options):
                             mirror / FP64 kernels: persistent CTAs per SM)
   D3_OPT_ATMB_LIST_CAPACITY longest list of the block-pair kernel (the rest go to the
                             mirror kernel)
+  D3_OPT_ATMB_FINE_SKIP     block-pair kernel: skip out-of-range visits per two steps
   D3_OPT_ATM_TILE           partner-tile entries of the mirror and FP64 ATM kernels
 
 `tune(handle, key)` times each candidate with the engine's per-pass CUDA-event timers
@@ -25,15 +26,16 @@ import json
 import math
 import os
 
-from d3_b200 import (OPT_ATM_CTAS_PER_SM, OPT_ATM_TILE, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_WARPS, OPT_BIN_DIVISOR,
-                     OPT_PAIR_KERNEL)
+from d3_b200 import (OPT_ATM_CTAS_PER_SM, OPT_ATM_TILE, OPT_ATMB_FINE_SKIP, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_WARPS,
+                     OPT_BIN_DIVISOR, OPT_PAIR_KERNEL)
 
 BIN_DIVISORS = (3, 4, 6, 8)
 PAIR_KERNELS = (0, 1)
 ATM_TILES = (64, 128, 256)
 ATM_CTAS = (0, 2, 3)
-# block-pair shapes: (warps per CTA, CTAs per SM, list capacity; 0 = automatic)
-ATMB_SHAPES = ((0, 0, 0), (8, 0, 0), (10, 0, 0), (4, 2, 0), (12, 0, 4096))
+# block-pair shapes: (warps per CTA, CTAs per SM, list capacity; 0 = automatic; skip
+# out-of-range visits per two steps)
+ATMB_SHAPES = ((0, 0, 0, 0), (0, 0, 0, 1), (8, 0, 0, 0), (10, 0, 0, 0), (4, 2, 0, 0), (12, 0, 4096, 0))
 
 
 def cache_path():
@@ -80,6 +82,7 @@ def apply(handle, params):
     handle.set_option(OPT_ATM_CTAS_PER_SM, params["atm_ctas_per_sm"])
     handle.set_option(OPT_ATMB_WARPS, params.get("atmb_warps", 0))
     handle.set_option(OPT_ATMB_LIST_CAPACITY, params.get("atmb_mcap", 0))
+    handle.set_option(OPT_ATMB_FINE_SKIP, params.get("atmb_fine_skip", 0))
 
 
 def _time(handle, repeats):
@@ -102,7 +105,7 @@ def tune(handle, key, repeats=2, use_cache=True, atm=True, precision=None):
     if precision is None:
         precision = key.endswith("|p1")
     params = {"bin_divisor": 6, "pair_kernel": 0, "atm_tile": 0, "atm_ctas_per_sm": 0, "atmb_warps": 0,
-              "atmb_mcap": 0}
+              "atmb_mcap": 0, "atmb_fine_skip": 0}
     apply(handle, params)
     pair_passes = ("bin", "cn", "twobody", "atm_list", "chain")
     best = None
@@ -123,15 +126,17 @@ def tune(handle, key, repeats=2, use_cache=True, atm=True, precision=None):
         if precision:
             # the block-pair kernel takes the lists up to its capacity, the mirror kernel
             # (tile, CTAs per SM at their defaults) the longer ones
-            for w, c, m in ATMB_SHAPES:
+            for w, c, m, f in ATMB_SHAPES:
                 handle.set_option(OPT_ATMB_WARPS, w)
                 handle.set_option(OPT_ATM_CTAS_PER_SM, c)
                 handle.set_option(OPT_ATMB_LIST_CAPACITY, m)
+                handle.set_option(OPT_ATMB_FINE_SKIP, f)
                 t = _time(handle, repeats)["atm"]
-                trials.append({"atmb_warps": w, "atm_ctas_per_sm": c, "atmb_mcap": m, "atm_ms": t})
+                trials.append({"atmb_warps": w, "atm_ctas_per_sm": c, "atmb_mcap": m, "atmb_fine_skip": f, "atm_ms": t})
                 if best is None or t < best[0]:
-                    best = (t, w, c, m)
-            params["atmb_warps"], params["atm_ctas_per_sm"], params["atmb_mcap"] = best[1], best[2], best[3]
+                    best = (t, w, c, m, f)
+            (params["atmb_warps"], params["atm_ctas_per_sm"], params["atmb_mcap"],
+             params["atmb_fine_skip"]) = best[1:]
         else:
             for tile in ATM_TILES:
                 for ctas in ATM_CTAS:

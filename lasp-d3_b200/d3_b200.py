@@ -27,7 +27,7 @@ OPT_ATM_SURROGATE = 7
 OPT_ATM_SCHEDULE = 8
 OPT_ATM_LIST_CAPACITY = 9
 OPT_PAIR_KERNEL = 10
-OPT_ATMB_WARPS, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_SPLIT = 11, 12, 13
+OPT_ATMB_WARPS, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_SPLIT, OPT_ATMB_FINE_SKIP = 11, 12, 13, 14
 TABLE_5REF, TABLE_7REF = 0, 1
 
 _lib = None

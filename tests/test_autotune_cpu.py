@@ -38,6 +38,7 @@ def test_tuner_keeps_the_fastest_candidates(tmp_path, monkeypatch, precision):
     if precision:
         assert res["atmb_warps"] == 10 and res["atmb_mcap"] == 0
         assert len([t for t in res["trials"] if "atmb_warps" in t]) == len(d3_autotune.ATMB_SHAPES)
+        assert res["atmb_fine_skip"] == 0
     else:
         assert res["atm_tile"] == 128 and res["atm_ctas_per_sm"] == 2
     # applied to the handle, and reused from the cache without timing

@@ -112,8 +112,8 @@ def test_atm_schedules_agree(case):
     assert np.abs(a0 - a1).max() <= 1e-6 * np.abs(a1).max()
 
 
-@pytest.mark.parametrize("shape", [(8, 0, 0, 0), (4, 2, 0, 0), (6, 0, 4096, 0), (12, 0, 4096, 0), (0, 0, 0, 3),
-                                   (8, 0, 0, 5)])
+@pytest.mark.parametrize("shape", [(8, 0, 0, 0, 0), (4, 2, 0, 0, 0), (6, 0, 4096, 0, 0), (12, 0, 4096, 0, 0),
+                                   (0, 0, 0, 3, 0), (8, 0, 0, 5, 0), (0, 0, 0, 0, 1), (8, 0, 0, 0, 1)])
 @pytest.mark.parametrize("case", ["tric", "fe"])
 def test_block_pair_shapes_agree(case, shape):
     """Launch shapes of the block-pair ATM kernel (warps per CTA, CTAs per SM, list
@@ -121,8 +121,8 @@ def test_block_pair_shapes_agree(case, shape):
     and fewer two) against the default shape (12 warps where they fit): the same in-range triplets and the same results to FP32 level. A
     4,096-entry capacity sends the longest lists of the 3,000-atom box (up to about 4,100
     entries at rc_ATM 40) to the mirror kernel; a split of 3 or 5 makes several CTAs add
-    their shares of each apex."""
-    from d3_b200 import OPT_ATM_CTAS_PER_SM, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_SPLIT, OPT_ATMB_WARPS
+    their shares of each apex; the last two skip out-of-range visits per two steps."""
+    from d3_b200 import OPT_ATM_CTAS_PER_SM, OPT_ATMB_FINE_SKIP, OPT_ATMB_LIST_CAPACITY, OPT_ATMB_SPLIT, OPT_ATMB_WARPS
 
     if case == "tric":
         sys_, kw = S.triclinic_box(3000, seed=5), dict(rc=95.0, rc_cn=40.0, rc_atm=40.0)
@@ -132,7 +132,7 @@ def test_block_pair_shapes_agree(case, shape):
         kw = dict(rc=30.0, rc_cn=30.0, rc_atm=30.0)
     out = []
     for opts in ((), ((OPT_ATMB_WARPS, shape[0]), (OPT_ATM_CTAS_PER_SM, shape[1]), (OPT_ATMB_LIST_CAPACITY, shape[2]),
-                      (OPT_ATMB_SPLIT, shape[3]))):
+                      (OPT_ATMB_SPLIT, shape[3]), (OPT_ATMB_FINE_SKIP, shape[4]))):
         d = D3(sys_["Z"], len(sys_["Z"]), damping=1, functional=0, **kw)
         d.set_option(OPT_PRECISION, 1)
         for o, v in opts:
