@@ -302,30 +302,43 @@ __global__ void __launch_bounds__(PAIRS_WARPS * 32, F64 ? 1 : 2) k_twobody_g(KP 
             }
             __syncwarp();
             R e = 0, fx = 0, fy = 0, fz = 0, vxx = 0, vyy = 0, vzz = 0, vxy = 0, vxz = 0, vyz = 0;
-            for (int jj = 0; jj < m; ++jj) {
-                const R4 xj = sP[jj];
-                const R dx = ox - xj.x, dy = oy - xj.y, dz = oz - xj.z;
-                const R r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-                bool act = iv && r2 < rc2 && r2 > (R)0;
-                if (box_pair && act) act = in_box(g, si, p.shift[base + jj], px, Ty, Tz);
-                if (!act) continue;
-                ++npair;
-                const int tj = (int)xj.w;
-                const R *tp = ptab + 3 * (ti * ne + tj);
-                R eh, Gt, fs;
-                pair_term<NR, R>(p, r2, sY + jj * rowlen + ti * NR, wi, dwi, tp[0], tp[1], tp[2], eh, Gt, fs);
-                e += eh;
-                Gd += (double)Gt;
-                fx = fma(fs, dx, fx);
-                fy = fma(fs, dy, fy);
-                fz = fma(fs, dz, fz);
-                const R fdx = fs * dx, fdy = fs * dy;
-                vxx = fma(fdx, dx, vxx);
-                vyy = fma(fdy, dy, vyy);
-                vzz = fma(fs * dz, dz, vzz);
-                vxy = fma(fdx, dy, vxy);
-                vxz = fma(fdx, dz, vxz);
-                vyz = fma(fdy, dz, vyz);
+            // two partners per iteration (independent dependency chains); an inactive one
+            // runs on a stand-in distance (rc^2, finite terms) and its sums are dropped
+            for (int jj = 0; jj < m; jj += 2) {
+                const int j1 = jj + 1 < m ? jj + 1 : jj;
+                const R4 x0 = sP[jj], x1 = sP[j1];
+                const R dx0 = ox - x0.x, dy0 = oy - x0.y, dz0 = oz - x0.z;
+                const R dx1 = ox - x1.x, dy1 = oy - x1.y, dz1 = oz - x1.z;
+                const R r20 = fma(dx0, dx0, fma(dy0, dy0, dz0 * dz0));
+                const R r21 = fma(dx1, dx1, fma(dy1, dy1, dz1 * dz1));
+                bool act0 = iv && r20 < rc2 && r20 > (R)0;
+                bool act1 = iv && j1 != jj && r21 < rc2 && r21 > (R)0;
+                if (box_pair) {
+                    if (act0) act0 = in_box(g, si, p.shift[base + jj], px, Ty, Tz);
+                    if (act1) act1 = in_box(g, si, p.shift[base + j1], px, Ty, Tz);
+                }
+                if (!(act0 || act1)) continue;
+                npair += (act0 ? 1 : 0) + (act1 ? 1 : 0);
+                const R *tp0 = ptab + 3 * (ti * ne + (int)x0.w), *tp1 = ptab + 3 * (ti * ne + (int)x1.w);
+                R eh0, Gt0, fs0, eh1, Gt1, fs1;
+                pair_term<NR, R>(p, act0 ? r20 : rc2, sY + jj * rowlen + ti * NR, wi, dwi, tp0[0], tp0[1], tp0[2], eh0,
+                                 Gt0, fs0);
+                pair_term<NR, R>(p, act1 ? r21 : rc2, sY + j1 * rowlen + ti * NR, wi, dwi, tp1[0], tp1[1], tp1[2], eh1,
+                                 Gt1, fs1);
+                if (!act0) eh0 = Gt0 = fs0 = (R)0;
+                if (!act1) eh1 = Gt1 = fs1 = (R)0;
+                e += eh0 + eh1;
+                Gd += (double)Gt0 + (double)Gt1;
+                fx = fma(fs0, dx0, fma(fs1, dx1, fx));
+                fy = fma(fs0, dy0, fma(fs1, dy1, fy));
+                fz = fma(fs0, dz0, fma(fs1, dz1, fz));
+                const R fdx0 = fs0 * dx0, fdy0 = fs0 * dy0, fdx1 = fs1 * dx1, fdy1 = fs1 * dy1;
+                vxx = fma(fdx0, dx0, fma(fdx1, dx1, vxx));
+                vyy = fma(fdy0, dy0, fma(fdy1, dy1, vyy));
+                vzz = fma(fs0 * dz0, dz0, fma(fs1 * dz1, dz1, vzz));
+                vxy = fma(fdx0, dy0, fma(fdx1, dy1, vxy));
+                vxz = fma(fdx0, dz0, fma(fdx1, dz1, vxz));
+                vyz = fma(fdy0, dz0, fma(fdy1, dz1, vyz));
             }
             // blocked summation: 32-partner sums carried in FP64
             E += e;
