@@ -51,8 +51,8 @@ constexpr int ATMB_MAXW1 = 12;    // warps per CTA at most with one y buffer per
 constexpr int ATMB_CTAS_PER_SM = 2; // preferred CTAs per SM (of four warps each)
 
 // global scratch per CTA (float4 units): per-entry records sA, sB, sJ and the per-entry
-// accumulators [6][mcap] floats
-__host__ __device__ inline size_t atmb_scratch_per_cta(int mcap) { return 3 * (size_t)mcap + (6 * (size_t)mcap + 3) / 4; }
+// accumulators [7][mcap] floats
+__host__ __device__ inline size_t atmb_scratch_per_cta(int mcap) { return 3 * (size_t)mcap + (7 * (size_t)mcap + 3) / 4; }
 
 // shared memory: fixed part + per-warp staging
 __host__ __device__ inline size_t atmb_smem_fixed(int ne, int NR, int mcap) {
@@ -213,8 +213,11 @@ struct AtmbX2 {
 
 // y sums of one entry over a block pair: SE = sum w E, SD = sum w E lam, SA = sum wf
 // f_apex-side, S3 = sum wf f3, W = sum wf f3 v_other (force scalar of the entry SF = SA + S3)
+// (weighted form also SC = sum (w - wf)(f_apex-side + f3): where the energy weight w of a
+// visit differs from its force weight wf, the apex virial gets SC v (x) v per entry)
+template <bool SIMPLE>
 struct AtmbSide {
-    float SE, SD, SA, S3, Wx, Wy, Wz;
+    float SE, SD, SA, S3, Wx, Wy, Wz, SC;
     // add the y sums that lane src holds
     __device__ __forceinline__ void add_from(const AtmbSide &o, int src) {
         SE += __shfl_sync(0xffffffffu, o.SE, src);
@@ -224,6 +227,7 @@ struct AtmbSide {
         Wx += __shfl_sync(0xffffffffu, o.Wx, src);
         Wy += __shfl_sync(0xffffffffu, o.Wy, src);
         Wz += __shfl_sync(0xffffffffu, o.Wz, src);
+        if (!SIMPLE) SC += __shfl_sync(0xffffffffu, o.SC, src);
     }
     __device__ __forceinline__ void flush(float *acc, int mcap, int e, int m) {
         if (e < m && (SE != 0.f || SA != 0.f || S3 != 0.f || SD != 0.f)) {
@@ -233,25 +237,27 @@ struct AtmbSide {
             atomicAdd(&acc[3 * mcap + e], Wx);
             atomicAdd(&acc[4 * mcap + e], Wy);
             atomicAdd(&acc[5 * mcap + e], Wz);
+            if (!SIMPLE && SC != 0.f) atomicAdd(&acc[6 * mcap + e], SC);
         }
     }
 };
 
 // packed sums of one block pair: component x for one visit of a pair, y for the other
+template <bool SIMPLE>
 struct AtmbSide2 {
-    float2 SE, SD, SA, S3, Wx, Wy, Wz, Ux, Uy, Uz;
+    float2 SE, SD, SA, S3, Wx, Wy, Wz, Ux, Uy, Uz, SC;
     // the y sums move with their y: take those of lane src
     __device__ __forceinline__ void shift(int src) {
-        float2 *v[7] = {&SE, &SD, &SA, &S3, &Wx, &Wy, &Wz};
+        float2 *v[8] = {&SE, &SD, &SA, &S3, &Wx, &Wy, &Wz, &SC};
 #pragma unroll
-        for (int q = 0; q < 7; ++q) {
+        for (int q = 0; q < (SIMPLE ? 7 : 8); ++q) {
             v[q]->x = __shfl_sync(0xffffffffu, v[q]->x, src);
             v[q]->y = __shfl_sync(0xffffffffu, v[q]->y, src);
         }
     }
     // one component as a scalar side (y sums only)
-    __device__ __forceinline__ AtmbSide part(int c) const {
-        AtmbSide o{};
+    __device__ __forceinline__ AtmbSide<SIMPLE> part(int c) const {
+        AtmbSide<SIMPLE> o{};
         o.SE = c ? SE.y : SE.x;
         o.SD = c ? SD.y : SD.x;
         o.SA = c ? SA.y : SA.x;
@@ -259,6 +265,7 @@ struct AtmbSide2 {
         o.Wx = c ? Wx.y : Wx.x;
         o.Wy = c ? Wy.y : Wy.x;
         o.Wz = c ? Wz.y : Wz.x;
+        o.SC = c ? SC.y : SC.x;
         return o;
     }
 };
@@ -278,7 +285,7 @@ template <int NR, bool SIMPLE>
 __device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 d3in, bool act0, bool act1,
                                             const float4 P0, const float4 P1, const float4 *yQ0, const float4 *yQ1,
                                             const float4 *yrow, int a, float third, bool force_scaled,
-                                            AtmbSide2 &xt, AtmbSide2 &ys, const AtmbCarry &apx) {
+                                            AtmbSide2<SIMPLE> &xt, AtmbSide2<SIMPLE> &ys) {
     const int k1 = (k0 + 1) & 31;
     const float2 ONE = make_float2(1.0f, 1.0f), M1 = make_float2(-1.0f, -1.0f), M2 = make_float2(-2.0f, -2.0f);
     const float2 d3 = make_float2(act0 ? d3in.x : X.d1.x, act1 ? d3in.y : X.d1.x);
@@ -365,23 +372,12 @@ __device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 
     ys.Wy = __ffma2_rn(wf3, X.vy, ys.Wy);
     ys.Wz = __ffma2_rn(wf3, X.vz, ys.Wz);
     if (!SIMPLE) {
-        // virial weights w where the force weights differ (repeated indices)
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const float w = c ? -nw.y : -nw.x, f = c ? wf.y : wf.x;
-            if (w != f) {
-                const float F1 = c ? f1.y : f1.x, F2 = c ? f2.y : f2.x, F3 = c ? f3.y : f3.x;
-                const float py = c ? P0.y : P0.x, pyy = c ? P0.w : P0.z, pz = c ? P1.y : P1.x;
-                const float vx = X.vx.x, vy = X.vy.x, vz = X.vz.x;
-                const double c1 = (double)(w - f) * (double)(F1 + F3), c2 = (double)(w - f) * (double)(F2 + F3);
-                apx[3] += c1 * vx * vx + c2 * py * py;
-                apx[4] += c1 * vy * vy + c2 * pyy * pyy;
-                apx[5] += c1 * vz * vz + c2 * pz * pz;
-                apx[6] += c1 * vx * vy + c2 * py * pyy;
-                apx[7] += c1 * vx * vz + c2 * py * pz;
-                apx[8] += c1 * vy * vz + c2 * pyy * pz;
-            }
-        }
+        // where the energy / virial weight w of a visit differs from its force weight wf
+        // (repeated indices) the apex virial needs (w - wf)(f_apex-side + f3) v (x) v for
+        // both entries: per entry coefficients, applied once per entry at the end
+        const float2 dwf = __ffma2_rn(nw, M1, __fmul2_rn(wf, M1)); // -nw - wf = w - wf
+        xt.SC = __ffma2_rn(dwf, __fadd2_rn(f1, f3), xt.SC);
+        ys.SC = __ffma2_rn(dwf, __fadd2_rn(f2, f3), ys.SC);
     }
 }
 
@@ -452,7 +448,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
         for (int k = tid; k < ATMB_CELLS; k += blockDim.x) cellpos[k] = 0;
         if (tid == 0) s_row = 0;
-        for (int q = 0; q < 6; ++q)
+        for (int q = 0; q < (SIMPLE ? 6 : 7); ++q)
             for (int e = tid; e < m; e += blockDim.x) __stcg(&acc[q * mcap + e], 0.f);
         double dwa[NR];
 #pragma unroll
@@ -632,6 +628,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             X.qa = qa;
 #pragma unroll
             for (int q = 0; q < 10; ++q) xs[q] = 0.0;
+            float xsc = 0.f; // weighted form: the x entry's virial coefficient over this row
             // block pairs (A, B) whose boxes are within rc_ATM, visited in order of B; the
             // y block of the next one is copied (cp.async) while the current one is visited
             auto near = [&](int B) {
@@ -700,8 +697,8 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                     yQ1[lane] = make_float4(b0.z, b1z, b0.w, b1w);
                 }
                 __syncwarp();
-                AtmbSide2 xt{};    // x side of this block pair (two partial sums)
-                AtmbSide2 ys[2]{}; // y sides of steps s + 2p (x) and s + 2p + 1 (y), travelling with their y
+                AtmbSide2<simple> xt{};    // x side of this block pair (two partial sums)
+                AtmbSide2<simple> ys[2]{}; // y sides of steps s + 2p (x) and s + 2p + 1 (y), travelling with their y
                 const bool diag = (A == B);
                 const int s0 = diag ? 1 : 0, s1 = diag ? 17 : 32;
                 const float4 *yrow_x = yrow + tx * RQ * 32; // rows at the x entry's type
@@ -734,12 +731,12 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                         for (int pq = 0; pq < 2; ++pq)
                             if (__any_sync(0xffffffffu, a0q[pq] | a1q[pq]))
                                 atmb_visit2<NR, simple>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0,
-                                                        yQ1, yrow_x, a, third, force_scaled, xt, ys[pq], apx);
+                                                        yQ1, yrow_x, a, third, force_scaled, xt, ys[pq]);
                     } else if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
                         for (int pq = 0; pq < 2; ++pq)
                             atmb_visit2<NR, simple>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0, yQ1,
-                                                    yrow_x, a, third, force_scaled, xt, ys[pq], apx);
+                                                    yrow_x, a, third, force_scaled, xt, ys[pq]);
                     }
                     const int src = (lane + 4) & 31;
                     ys[0].shift(src);
@@ -749,7 +746,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                 // lane L now holds the complete sums of y entry B[(L + s1 + q) mod 32] from the
                 // visits of steps = q (mod 4) (q = 0, 1 in ys[0].x, .y; 2, 3 in ys[1].x, .y):
                 // gather the entry B[(L + s1) mod 32]
-                AtmbSide yg = ys[0].part(0);
+                AtmbSide<simple> yg = ys[0].part(0);
                 yg.add_from(ys[0].part(1), (lane - 1) & 31);
                 yg.add_from(ys[1].part(0), (lane - 2) & 31);
                 yg.add_from(ys[1].part(1), (lane - 3) & 31);
@@ -779,6 +776,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                     xs[7] -= xt.Ux.x + xt.Ux.y;
                     xs[8] -= xt.Uy.x + xt.Uy.y;
                     xs[9] -= xt.Uz.x + xt.Uz.y;
+                    xsc += xt.SC.x + xt.SC.y;
                 }
                 B = Bn;
                 if (NBUF == 2) cur ^= 1;
@@ -791,6 +789,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                 atomicAdd(&acc[3 * mcap + xe], (float)xs[3]);
                 atomicAdd(&acc[4 * mcap + xe], (float)xs[4]);
                 atomicAdd(&acc[5 * mcap + xe], (float)xs[5]);
+                if (!simple && xsc != 0.f) atomicAdd(&acc[6 * mcap + xe], xsc);
                 // apex force of the a-x sides and the x-y cross terms of the virial
                 apx[0] -= xs[6] * vx;
                 apx[1] -= xs[6] * vy;
@@ -823,12 +822,15 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             atomicAdd(&p.fb[3 * j + 2], SF * vz - Wz);
             ea += SE * (1.0 / 6.0);
             ga += 0.5 * lam_ae * SE;
-            apx[3] += SF * vx * vx;
-            apx[4] += SF * vy * vy;
-            apx[5] += SF * vz * vz;
-            apx[6] += SF * vx * vy;
-            apx[7] += SF * vx * vz;
-            apx[8] += SF * vy * vz;
+            // virial: the force scalar, plus in the weighted form the coefficient of the
+            // visits whose energy and force weights differ
+            const double SV = SIMPLE ? SF : SF + (double)__ldcg(&acc[6 * mcap + e]);
+            apx[3] += SV * vx * vx;
+            apx[4] += SV * vy * vy;
+            apx[5] += SV * vz * vz;
+            apx[6] += SV * vx * vy;
+            apx[7] += SV * vx * vz;
+            apx[8] += SV * vy * vz;
         }
         const double vals[11] = {ea, ga, apx[0], apx[1], apx[2], apx[3], apx[4], apx[5], apx[6], apx[7], apx[8]};
 #pragma unroll
