@@ -64,6 +64,7 @@ struct SG {
     int st2_off, st2_n, stc_off, stc_n, sta_off, sta_n; // stencil rows (two-body, CN, ATM)
     int st2b_off, st2b_n;     // two-body stencil of a block of gy x gz bin rows (atom groups)
     int stcb_off, stcb_n;     // CN / chain-rule stencil of the same blocks
+    int stab_off, stab_n;     // rc_ATM stencil of the same blocks (ATM half lists)
     int atm_simple;           // every cell height > 2 rc_ATM: no atom twice in an ATM list
 };
 
@@ -1556,6 +1557,15 @@ static void build_structures(Engine *e, int nstruct, const uint64_t *counts, con
             r.stcb_off = (int)rows.size();
             r.stcb_n = (int)blkc.size();
             for (auto &x : blkc) rows.push_back(make_int4(x.dy, x.dz, x.dxlo, x.dxhi));
+            if (e->use_atm) {
+                std::vector<StencilRow> sa;
+                for (int q = r.sta_off; q < r.sta_off + r.sta_n; ++q)
+                    sa.push_back({rows[q].x, rows[q].y, rows[q].z, rows[q].w});
+                const auto blka = merge_block_stencil(sa, gy, gz);
+                r.stab_off = (int)rows.size();
+                r.stab_n = (int)blka.size();
+                for (auto &x : blka) rows.push_back(make_int4(x.dy, x.dz, x.dxlo, x.dxhi));
+            }
             for (int bz = 0; bz < r.nb[2]; bz += gz)
                 for (int by = 0; by < r.nb[1]; by += gy)
                     srow.push_back(make_int4(k, by, bz, std::min(gy, r.nb[1] - by) | (std::min(gz, r.nb[2] - bz) << 8)));
@@ -1577,7 +1587,7 @@ static void build_structures(Engine *e, int nstruct, const uint64_t *counts, con
     if (!srow.empty())
         D3_CUDA(cudaMemcpy(e->srows.p, srow.data(), sizeof(int4) * srow.size(), cudaMemcpyHostToDevice));
     e->groups.ensure(e->group_bound);
-    e->gctl.ensure(4); // [0] groups, [1..3] work counters of the CN, two-body and chain passes
+    e->gctl.ensure(6); // [0] groups, [1..5] work counters: CN, two-body, chain, ATM list count, fill
     e->anyshift.ensure(std::max(1, nstruct));
     e->nstruct = nstruct;
     e->nbins_total = bin_base;
@@ -1970,7 +1980,7 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
         k_binsort<<<(p.nbins_total + T - 1) / T, T, 0, s>>>(p);
         k_gather<<<gb, T, 0, s>>>(p);
         if (p.gslices > 0) {
-            D3_CUDA(cudaMemsetAsync(e->gctl.p, 0, 4 * sizeof(int), s));
+            D3_CUDA(cudaMemsetAsync(e->gctl.p, 0, 6 * sizeof(int), s));
             k_groups<<<(p.nsrow + 127) / 128, 128, 0, s>>>(p);
         }
         D3_CUDA(cudaEventRecord(ev[1], s));
@@ -2042,7 +2052,13 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
             pc.atm_napex = S.napex.p;
             pc.surr_flag = S.flag.p;
         }
-        if (e->use_atm) {
+        if (e->use_atm && p.gslices > 0) {
+            const size_t sm = PAIRS_WARPS * 32 * (sizeof(double4) + sizeof(int));
+            k_atm_list_g<false><<<e->dev_sms * 2, PAIRS_WARPS * 32, sm, s>>>(pc, e->gctl.p + 4);
+            k_atm_list_prefix<<<gb, T, 0, s>>>(pc);
+            k_scan<long long, int><<<1, 1024, 0, s>>>(p.atm_cnt, p.atm_off, n);
+            k_atm_list_g<true><<<e->dev_sms * 2, PAIRS_WARPS * 32, sm, s>>>(pc, e->gctl.p + 5);
+        } else if (e->use_atm) {
             k_atm_list<false><<<gw, T, 0, s>>>(pc);
             k_scan<long long, int><<<1, 1024, 0, s>>>(p.atm_cnt, p.atm_off, n);
             k_atm_list<true><<<gw, T, 0, s>>>(pc);
@@ -2143,7 +2159,8 @@ int engine_pass_times(Engine *e, float *ms, int cap, unsigned long long *counter
 }
 
 int engine_launches_per_eval(const Engine *e) {
-    const int pairs = pairs_grouped(e) ? 4 : 0; // group cut and three slice reductions
+    // grouped passes: group cut, three slice reductions and the ATM lists' prefix pass
+    const int pairs = pairs_grouped(e) ? (e->use_atm ? 5 : 4) : 0;
     if (!e->use_atm) return 12 + pairs;
     if (e->opt.atm_surrogate && e->surr.loaded) return 20 + pairs;
     return (blockpair_warps(e) > 0 ? 17 : 16) + pairs;

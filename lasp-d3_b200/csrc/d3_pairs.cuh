@@ -541,3 +541,90 @@ __global__ void k_group_reduce(KP p, int what) {
         for (int k = 0; k < 6; ++k) v[k] = acc[3 + k] * sc;
     }
 }
+
+// ATM half lists on atom groups (rc_ATM stencil): for apex a the entries (j, T) with j <= a in
+// caller order (all of them in centre mode) and 1e-12 <= r^2 <= rc_ATM^2, the distance
+// evaluated as the per-apex kernel does (x_a - (x_j + T h)). Count pass: counts per
+// (stencil slice, apex) into the partial array; k_atm_list_prefix turns them into offsets
+// within the apex and the apex totals; fill pass: every lane writes its apex's entries of
+// its slice at atm_off[a] + that offset, so each list is contiguous and its order fixed.
+template <bool FILL>
+__global__ void __launch_bounds__(PAIRS_WARPS * 32, 2) k_atm_list_g(KP p, int *work) {
+    extern __shared__ __align__(16) unsigned char smp[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double4 *sP = reinterpret_cast<double4 *>(smp + (size_t)warp * 32 * (sizeof(double4) + sizeof(int)));
+    int *sO = reinterpret_cast<int *>(sP + 32);
+    int *gcnt = reinterpret_cast<int *>(p.gpart); // [slice][n]
+    const bool full = p.atm_center != 0;
+    bool range_err = false, overflow = false;
+    GroupItem it;
+    while (next_item(p, work, it)) {
+        const int a = it.i;
+        const SG &g = *it.g;
+        double4 xa = make_double4(0, 0, 0, 0);
+        int4 sa = make_int4(0, 0, 0, 0);
+        int oa = -1;
+        bool take = a >= 0;
+        if (take) {
+            xa = p.xs[a];
+            sa = p.shift[a];
+            oa = p.orig[a];
+            if ((p.atm_center && !p.surr_flag[a]) ||
+                (p.shard_world > 1 && (p.n - 1 - oa) % p.shard_world != p.shard_rank))
+                take = false;
+        }
+        const bool box_pair = g.box_mode && p.anyshift[it.sr.x];
+        long long pos = 0;
+        int count = 0;
+        if (FILL && take) pos = p.atm_off[a] + gcnt[(size_t)it.sl * p.n + a];
+        group_ranges<double, double4>(p, it, p.stencils + g.stab_off, g.stab_n, box_pair, xa,
+                                      [&](int base, int m, double, double, double, int px, int Ty, int Tz) {
+            __syncwarp();
+            if (lane < m) {
+                sP[lane] = p.xs[base + lane];
+                sO[lane] = p.orig[base + lane];
+            }
+            __syncwarp();
+            if (!take) return;
+            const double shx = px * g.h[0] + Ty * g.h[3] + Tz * g.h[6];
+            const double shy = px * g.h[1] + Ty * g.h[4] + Tz * g.h[7];
+            const double shz = px * g.h[2] + Ty * g.h[5] + Tz * g.h[8];
+            for (int jj = 0; jj < m; ++jj) {
+                if (!full && sO[jj] > oa) continue;
+                if (box_pair && !in_box(g, sa, p.shift[base + jj], px, Ty, Tz)) continue;
+                const double4 xj = sP[jj];
+                const double dx = xa.x - (xj.x + shx), dy = xa.y - (xj.y + shy), dz = xa.z - (xj.z + shz);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 > p.ratm2 || d2 < 1e-12) continue;
+                if (FILL) {
+                    if (abs(px) > 127 || abs(Ty) > 127 || abs(Tz) > 127) range_err = true;
+                    if (pos < p.atm_cap)
+                        p.atm_ent[pos] = make_int2(base + jj, (px & 0xff) | ((Ty & 0xff) << 8) | ((Tz & 0xff) << 16));
+                    ++pos;
+                } else {
+                    ++count;
+                }
+            }
+        });
+        if (!FILL && a >= 0) gcnt[(size_t)it.sl * p.n + a] = take ? count : 0;
+        if (FILL && take && pos > p.atm_cap) overflow = true;
+    }
+    if (FILL) {
+        if (__any_sync(0xffffffffu, range_err) && lane == 0) atomicOr(p.status, ST_SHIFT_RANGE);
+        if (__any_sync(0xffffffffu, overflow) && lane == 0) atomicOr(p.status, ST_LIST_OVERFLOW);
+    }
+}
+
+// per apex: the slices' counts -> offsets within the apex's list, and its length
+__global__ void k_atm_list_prefix(KP p) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= p.n) return;
+    int *gcnt = reinterpret_cast<int *>(p.gpart);
+    int run = 0;
+    for (int s = 0; s < p.gslices; ++s) {
+        const int c = gcnt[(size_t)s * p.n + a];
+        gcnt[(size_t)s * p.n + a] = run;
+        run += c;
+    }
+    p.atm_cnt[a] = run;
+}
