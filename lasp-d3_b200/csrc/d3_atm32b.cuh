@@ -22,14 +22,16 @@
 //     the last step the four sets in lane L belong to four consecutive y's and are gathered
 //     by three shuffles into one entry's sums, added to that entry's accumulators (L2
 //     atomics on this CTA's global slot, one per quantity per block pair).
-//  4. Per entry e at the end: energy share SE/3, dE/dCN 0.5 (lam_ea SE + SD), force
-//     SF v_e - W (FP64 atomics to the entry atom, as k_atm32); the apex gets SE/6,
-//     0.5 lam_ae SE, the force -sum SA_e v_e and the virial sum SF v_e (x) v_e minus the
-//     cross terms (accumulated by the x lanes) plus the w != wf corrections.
+//  4. Per entry e at the end: energy share SE/3, dE/dCN 0.5 (lam_ea SE + SD) and its force
+//     F_e (FP64 atomics to the entry atom, as k_atm32); the apex gets SE/6, 0.5 lam_ae SE,
+//     the force -sum F_e (each triplet term depends on relative positions only) and the
+//     virial sum v_e (x) F_e, plus in the weighted form the corrections for the visits
+//     whose energy weight w differs from the force weight wf.
 // With f1, f2, f3 the force scalars of sides a-x, a-y, x-y of a triplet (mirror symmetry of
 // k_atm: f2 of visit (x, y) is f1 of the mirrored visit), the quantities per entry are
-//   SE = sum w E, SD = sum w E lam_{e,other}, SA = sum wf f_apex-side, S3 = sum wf f3,
-//   SF = SA + S3, W = sum wf f3 v_other.
+//   SE = sum w E, SD = sum w E lam_{e,other}, F = sum wf ((f_apex-side + f3) v_e - f3 v_other);
+// x lanes keep F as SF = sum wf (f_apex-side + f3) and W = sum wf f3 v_other (v_x is fixed
+// along the row), y sums carry -F itself (five travelling quantities).
 // C6_xy = Y_y[t_x] . w_x, dC6_xy/dCN_x = Y_y[t_x] . dw_x, dC6_xy/dCN_y = D_y[t_x] . w_x
 // with the x entry's own weights in registers and the y entry's rows at the x type read
 // from the staged block (the reverse factorisation halves the shared-memory bytes per
@@ -51,8 +53,8 @@ constexpr int ATMB_MAXW1 = 12;    // warps per CTA at most with one y buffer per
 constexpr int ATMB_CTAS_PER_SM = 2; // preferred CTAs per SM (of four warps each)
 
 // global scratch per CTA (float4 units): per-entry records sA, sB, sJ and the per-entry
-// accumulators [7][mcap] floats
-__host__ __device__ inline size_t atmb_scratch_per_cta(int mcap) { return 3 * (size_t)mcap + (7 * (size_t)mcap + 3) / 4; }
+// accumulators [6][mcap] floats
+__host__ __device__ inline size_t atmb_scratch_per_cta(int mcap) { return 3 * (size_t)mcap + (6 * (size_t)mcap + 3) / 4; }
 
 // shared memory: fixed part + per-warp staging
 __host__ __device__ inline size_t atmb_smem_fixed(int ne, int NR, int mcap) {
@@ -211,68 +213,73 @@ struct AtmbX2 {
     bool qa;
 };
 
-// y sums of one entry over a block pair: SE = sum w E, SD = sum w E lam, SA = sum wf
-// f_apex-side, S3 = sum wf f3, W = sum wf f3 v_other (force scalar of the entry SF = SA + S3)
+// y sums of one entry over a block pair: SE = sum w E, SD = sum w E lam, and minus the
+// entry's force from these visits, NF = -sum wf ((f_apex-side + f3) v_e - f3 v_other)
 // (weighted form also SC = sum (w - wf)(f_apex-side + f3): where the energy weight w of a
 // visit differs from its force weight wf, the apex virial gets SC v (x) v per entry)
 template <bool SIMPLE>
 struct AtmbSide {
-    float SE, SD, SA, S3, Wx, Wy, Wz, SC;
+    float SE, SD, NFx, NFy, NFz, SC;
     // add the y sums that lane src holds
     __device__ __forceinline__ void add_from(const AtmbSide &o, int src) {
         SE += __shfl_sync(0xffffffffu, o.SE, src);
         SD += __shfl_sync(0xffffffffu, o.SD, src);
-        SA += __shfl_sync(0xffffffffu, o.SA, src);
-        S3 += __shfl_sync(0xffffffffu, o.S3, src);
-        Wx += __shfl_sync(0xffffffffu, o.Wx, src);
-        Wy += __shfl_sync(0xffffffffu, o.Wy, src);
-        Wz += __shfl_sync(0xffffffffu, o.Wz, src);
+        NFx += __shfl_sync(0xffffffffu, o.NFx, src);
+        NFy += __shfl_sync(0xffffffffu, o.NFy, src);
+        NFz += __shfl_sync(0xffffffffu, o.NFz, src);
         if (!SIMPLE) SC += __shfl_sync(0xffffffffu, o.SC, src);
     }
     __device__ __forceinline__ void flush(float *acc, int mcap, int e, int m) {
-        if (e < m && (SE != 0.f || SA != 0.f || S3 != 0.f || SD != 0.f)) {
+        if (e < m && (SE != 0.f || SD != 0.f || NFx != 0.f || NFy != 0.f || NFz != 0.f)) {
             atomicAdd(&acc[0 * mcap + e], SE);
             atomicAdd(&acc[1 * mcap + e], SD);
-            atomicAdd(&acc[2 * mcap + e], SA + S3);
-            atomicAdd(&acc[3 * mcap + e], Wx);
-            atomicAdd(&acc[4 * mcap + e], Wy);
-            atomicAdd(&acc[5 * mcap + e], Wz);
-            if (!SIMPLE && SC != 0.f) atomicAdd(&acc[6 * mcap + e], SC);
+            atomicAdd(&acc[2 * mcap + e], -NFx);
+            atomicAdd(&acc[3 * mcap + e], -NFy);
+            atomicAdd(&acc[4 * mcap + e], -NFz);
+            if (!SIMPLE && SC != 0.f) atomicAdd(&acc[5 * mcap + e], SC);
         }
     }
 };
 
-// packed sums of one block pair: component x for one visit of a pair, y for the other
+// packed y sums of one block pair (component x for one visit of a pair, y for the other),
+// travelling with their y
 template <bool SIMPLE>
-struct AtmbSide2 {
-    float2 SE, SD, SA, S3, Wx, Wy, Wz, Ux, Uy, Uz, SC;
-    // the y sums move with their y: take those of lane src
+struct AtmbYSums2 {
+    float2 SE, SD, NFx, NFy, NFz, SC;
+    // take those of lane src
     __device__ __forceinline__ void shift(int src) {
-        float2 *v[8] = {&SE, &SD, &SA, &S3, &Wx, &Wy, &Wz, &SC};
+        float2 *v[6] = {&SE, &SD, &NFx, &NFy, &NFz, &SC};
 #pragma unroll
-        for (int q = 0; q < (SIMPLE ? 7 : 8); ++q) {
+        for (int q = 0; q < (SIMPLE ? 5 : 6); ++q) {
             v[q]->x = __shfl_sync(0xffffffffu, v[q]->x, src);
             v[q]->y = __shfl_sync(0xffffffffu, v[q]->y, src);
         }
     }
-    // one component as a scalar side (y sums only)
+    // one component as a scalar side
     __device__ __forceinline__ AtmbSide<SIMPLE> part(int c) const {
         AtmbSide<SIMPLE> o{};
         o.SE = c ? SE.y : SE.x;
         o.SD = c ? SD.y : SD.x;
-        o.SA = c ? SA.y : SA.x;
-        o.S3 = c ? S3.y : S3.x;
-        o.Wx = c ? Wx.y : Wx.x;
-        o.Wy = c ? Wy.y : Wy.x;
-        o.Wz = c ? Wz.y : Wz.x;
+        o.NFx = c ? NFx.y : NFx.x;
+        o.NFy = c ? NFy.y : NFy.x;
+        o.NFz = c ? NFz.y : NFz.x;
         o.SC = c ? SC.y : SC.x;
         return o;
     }
 };
 
+// packed x sums of one block pair: SE, SD as above, SF = sum wf (f_apex-side + f3),
+// W = sum wf f3 v_other (the entry's force is SF v_x - W); weighted form: SC as above and
+// U = sum (w - wf) f3 v_other (the cross terms of the apex virial that the force weights
+// miss)
+template <bool SIMPLE>
+struct AtmbXSums2 {
+    float2 SE, SD, SF, Wx, Wy, Wz, Ux, Uy, Uz, SC;
+};
+
 // Two (possible) visits of entry x, with the staged partners k0 and k1 = k0 + 1 (mod 32)
 // of two consecutive steps, in packed f32x2 arithmetic (component x: k0, y: k1): triplet
-// terms, x-side sums into xt, y-side sums into ys, virial corrections where the virial and
+// terms, x-side sums into xt, y-side sums into ys, virial corrections where the energy and
 // force weights differ. P0 = (x, x', y, y'), P1 = (z, z', d2, d2') of the two partners.
 // Branch-free: an out-of-range pair (act false) runs on finite stand-in values (lanes
 // without entry and padding partners sit at far, distinct points with positive C6 rows)
@@ -285,7 +292,7 @@ template <int NR, bool SIMPLE>
 __device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 d3in, bool act0, bool act1,
                                             const float4 P0, const float4 P1, const float4 *yQ0, const float4 *yQ1,
                                             const float4 *yrow, int a, float third, bool force_scaled,
-                                            AtmbSide2<SIMPLE> &xt, AtmbSide2<SIMPLE> &ys) {
+                                            AtmbXSums2<SIMPLE> &xt, AtmbYSums2<SIMPLE> &ys) {
     const int k1 = (k0 + 1) & 31;
     const float2 ONE = make_float2(1.0f, 1.0f), M1 = make_float2(-1.0f, -1.0f), M2 = make_float2(-2.0f, -2.0f);
     const float2 d3 = make_float2(act0 ? d3in.x : X.d1.x, act1 ? d3in.y : X.d1.x);
@@ -293,20 +300,20 @@ __device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 
     AtmbRow<NR> R0, R1; // the partners' rows at the x entry's type
     R0.load(yrow, k0);
     R1.load(yrow, k1);
-    const float2 ir3 = make_float2(rsqrtf(d3.x), rsqrtf(d3.y));
+    const float2 ir3 = make_float2(sfu_rsqrt(d3.x), sfu_rsqrt(d3.y));
     const float2 id3 = __fmul2_rn(ir3, ir3);
     // C6_xy = Y_y[t_x] . w_x, its derivatives dw_x and through D_y[t_x] = dw_y C
     const float2 c6 = make_float2(atmb_dot2<NR>(R0.Y, X.w), atmb_dot2<NR>(R1.Y, X.w));
     const float2 dcx = make_float2(atmb_dot2<NR>(R0.Y, X.dw), atmb_dot2<NR>(R1.Y, X.dw)); // dC6_xy/dCN_x
     const float2 dcy = make_float2(atmb_dot2<NR>(R0.D, X.w), atmb_dot2<NR>(R1.D, X.w));   // dC6_xy/dCN_y
-    const float2 is3 = make_float2(rsqrtf(c6.x), rsqrtf(c6.y));
+    const float2 is3 = make_float2(sfu_rsqrt(c6.x), sfu_rsqrt(c6.y));
     const float2 s3 = __fmul2_rn(c6, is3);
     const float2 is3q = __fmul2_rn(is3, is3);
     const float2 lam_xy = __fmul2_rn(dcx, is3q), lam_yx = __fmul2_rn(dcy, is3q);
     // (r0_xy^2 / d3)^(8/3)
-    const float2 lgu = __fmul2_rn(make_float2(__log2f(R0.r0sq * id3.x), __log2f(R1.r0sq * id3.y)),
+    const float2 lgu = __fmul2_rn(make_float2(sfu_log2(R0.r0sq * id3.x), sfu_log2(R1.r0sq * id3.y)),
                                   make_float2(8.0f / 3.0f, 8.0f / 3.0f));
-    const float2 g3 = make_float2(exp2f(lgu.x), exp2f(lgu.y));
+    const float2 g3 = make_float2(sfu_exp2(lgu.x), sfu_exp2(lgu.y));
     // reference scale factors (src/d3_kernel.cu:1282-1290) as pair weights; SIMPLE: no
     // atom appears twice in the list (cell heights > 2 rc_ATM), every weight is 1
     float2 nw, wf;
@@ -339,7 +346,7 @@ __device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 
     const float2 G3 = __ffma2_rn(__fmul2_rn(make_float2(-0.75f, -0.75f), d3), __ffma2_rn(M2, t23, T), base);
     const float2 x16 = __fmul2_rn(__fmul2_rn(X.gq, make_float2(Q1.z, Q1.w)), g3);
     const float2 den = __ffma2_rn(make_float2(6.0f, 6.0f), x16, ONE);
-    const float2 fd = make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y));
+    const float2 fd = make_float2(sfu_rcp(den.x), sfu_rcp(den.y));
     const float2 ndfd = __fmul2_rn(__fmul2_rn(__fmul2_rn(make_float2(-32.0f, -32.0f), x16), fd), fd);
     const float2 nC9 = __fmul2_rn(__fmul2_rn(X.sq, make_float2(Q1.x, Q1.y)), s3); // -C9
     const float2 nC9fd = __fmul2_rn(nC9, fd);
@@ -350,34 +357,33 @@ __device__ __forceinline__ void atmb_visit2(const AtmbX2<NR> &X, int k0, float2 
     const float2 f3 = __fmul2_rn(__ffma2_rn(Ap, G3, nBp), id3);
     const float2 wE = __fmul2_rn(nw, Em);
     const float2 wf3 = __fmul2_rn(wf, f3);
+    const float2 f13 = __fadd2_rn(f1, f3), f23 = __fadd2_rn(f2, f3);
     const float2 yx = make_float2(P0.x, P0.y), yy = make_float2(P0.z, P0.w), yz = make_float2(P1.x, P1.y);
     xt.SE = __fadd2_rn(xt.SE, wE);
     xt.SD = __ffma2_rn(wE, lam_xy, xt.SD);
-    xt.SA = __ffma2_rn(wf, f1, xt.SA);
-    xt.S3 = __fadd2_rn(xt.S3, wf3);
+    xt.SF = __ffma2_rn(wf, f13, xt.SF);
     xt.Wx = __ffma2_rn(wf3, yx, xt.Wx);
     xt.Wy = __ffma2_rn(wf3, yy, xt.Wy);
     xt.Wz = __ffma2_rn(wf3, yz, xt.Wz);
-    if (!SIMPLE) { // SIMPLE: U = W; here U accumulates -w f3 v_y
-        const float2 nw3 = __fmul2_rn(nw, f3);
-        xt.Ux = __ffma2_rn(nw3, yx, xt.Ux);
-        xt.Uy = __ffma2_rn(nw3, yy, xt.Uy);
-        xt.Uz = __ffma2_rn(nw3, yz, xt.Uz);
-    }
+    // minus the y entry's force: wf f3 v_x - wf (f2 + f3) v_y (SIMPLE: -wf = nw)
+    const float2 nwf23 = __fmul2_rn(SIMPLE ? nw : __fmul2_rn(wf, M1), f23);
     ys.SE = __fadd2_rn(ys.SE, wE);
     ys.SD = __ffma2_rn(wE, lam_yx, ys.SD);
-    ys.SA = __ffma2_rn(wf, f2, ys.SA);
-    ys.S3 = __fadd2_rn(ys.S3, wf3);
-    ys.Wx = __ffma2_rn(wf3, X.vx, ys.Wx);
-    ys.Wy = __ffma2_rn(wf3, X.vy, ys.Wy);
-    ys.Wz = __ffma2_rn(wf3, X.vz, ys.Wz);
+    ys.NFx = __ffma2_rn(wf3, X.vx, __ffma2_rn(nwf23, yx, ys.NFx));
+    ys.NFy = __ffma2_rn(wf3, X.vy, __ffma2_rn(nwf23, yy, ys.NFy));
+    ys.NFz = __ffma2_rn(wf3, X.vz, __ffma2_rn(nwf23, yz, ys.NFz));
     if (!SIMPLE) {
         // where the energy / virial weight w of a visit differs from its force weight wf
-        // (repeated indices) the apex virial needs (w - wf)(f_apex-side + f3) v (x) v for
-        // both entries: per entry coefficients, applied once per entry at the end
+        // (repeated indices) the apex virial needs (w - wf) times the visit's virial
+        // terms: (f_apex-side + f3) v (x) v per entry (coefficients SC, applied once per
+        // entry at the end) and the cross terms -f3 (v_x (x) v_y + v_y (x) v_x) (U)
         const float2 dwf = __ffma2_rn(nw, M1, __fmul2_rn(wf, M1)); // -nw - wf = w - wf
-        xt.SC = __ffma2_rn(dwf, __fadd2_rn(f1, f3), xt.SC);
-        ys.SC = __ffma2_rn(dwf, __fadd2_rn(f2, f3), ys.SC);
+        xt.SC = __ffma2_rn(dwf, f13, xt.SC);
+        ys.SC = __ffma2_rn(dwf, f23, ys.SC);
+        const float2 dwf3 = __fmul2_rn(dwf, f3);
+        xt.Ux = __ffma2_rn(dwf3, yx, xt.Ux);
+        xt.Uy = __ffma2_rn(dwf3, yy, xt.Uy);
+        xt.Uz = __ffma2_rn(dwf3, yz, xt.Uz);
     }
 }
 
@@ -448,7 +454,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         for (int k = tid; k < ne * NR; k += blockDim.x) yapex[k] = p.Y[(size_t)a * ne * NR + k];
         for (int k = tid; k < ATMB_CELLS; k += blockDim.x) cellpos[k] = 0;
         if (tid == 0) s_row = 0;
-        for (int q = 0; q < (SIMPLE ? 6 : 7); ++q)
+        for (int q = 0; q < (SIMPLE ? 5 : 6); ++q)
             for (int e = tid; e < m; e += blockDim.x) __stcg(&acc[q * mcap + e], 0.f);
         double dwa[NR];
 #pragma unroll
@@ -561,7 +567,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         // ---- 2./3. block pairs
         // apex force (3) and virial (6) of this lane, and the row sums of its x entry
         const AtmbCarry apx{reinterpret_cast<double *>(wbase + NBUF * bufq * sizeof(float4)) + lane};
-        const AtmbCarry xs{apx.p + 9 * 32}; // SE SD SF Wx Wy Wz SA Ux Uy Uz
+        const AtmbCarry xs{apx.p + 9 * 32}; // SE SD SF Wx Wy Wz, weighted form also Ux Uy Uz
         // positions (x, x', y, y'), (z, z', d2, d2') and constants (ir, ir', id2, id2'),
         // (s, s', g, g') of the current y block, entries k and k + 1 at slot k
         float4 *yP0 = reinterpret_cast<float4 *>(wbase + NBUF * bufq * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double));
@@ -627,7 +633,7 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             X.jx = jx;
             X.qa = qa;
 #pragma unroll
-            for (int q = 0; q < 10; ++q) xs[q] = 0.0;
+            for (int q = 0; q < (simple ? 6 : 9); ++q) xs[q] = 0.0;
             float xsc = 0.f; // weighted form: the x entry's virial coefficient over this row
             // block pairs (A, B) whose boxes are within rc_ATM, visited in order of B; the
             // y block of the next one is copied (cp.async) while the current one is visited
@@ -697,8 +703,8 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                     yQ1[lane] = make_float4(b0.z, b1z, b0.w, b1w);
                 }
                 __syncwarp();
-                AtmbSide2<simple> xt{};    // x side of this block pair (two partial sums)
-                AtmbSide2<simple> ys[2]{}; // y sides of steps s + 2p (x) and s + 2p + 1 (y), travelling with their y
+                AtmbXSums2<simple> xt{};    // x side of this block pair (two partial sums)
+                AtmbYSums2<simple> ys[2]{}; // y sides of steps s + 2p (x) and s + 2p + 1 (y), travelling with their y
                 const bool diag = (A == B);
                 const int s0 = diag ? 1 : 0, s1 = diag ? 17 : 32;
                 const float4 *yrow_x = yrow + tx * RQ * 32; // rows at the x entry's type
@@ -750,32 +756,17 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                 yg.add_from(ys[0].part(1), (lane - 1) & 31);
                 yg.add_from(ys[1].part(0), (lane - 2) & 31);
                 yg.add_from(ys[1].part(1), (lane - 3) & 31);
-                {
-                    const int ey = (lane + s1) & 31;
-                    yg.flush(acc, mcap, B * 32 + ey, m);
-                    // apex force of the a-y sides (padding partners carry zero sums)
-                    const float4 vyv = yA[ey];
-                    apx[0] -= (double)(yg.SA * vyv.x);
-                    apx[1] -= (double)(yg.SA * vyv.y);
-                    apx[2] -= (double)(yg.SA * vyv.z);
-                }
-                const float tSA = xt.SA.x + xt.SA.y, tS3 = xt.S3.x + xt.S3.y;
-                const float tWx = xt.Wx.x + xt.Wx.y, tWy = xt.Wy.x + xt.Wy.y, tWz = xt.Wz.x + xt.Wz.y;
+                yg.flush(acc, mcap, B * 32 + ((lane + s1) & 31), m); // padding partners carry zero sums
                 xs[0] += xt.SE.x + xt.SE.y;
                 xs[1] += xt.SD.x + xt.SD.y;
-                xs[2] += tSA + tS3;
-                xs[3] += tWx;
-                xs[4] += tWy;
-                xs[5] += tWz;
-                xs[6] += tSA;
-                if constexpr (simple) { // U = W
-                    xs[7] += tWx;
-                    xs[8] += tWy;
-                    xs[9] += tWz;
-                } else { // xt.U holds -U
-                    xs[7] -= xt.Ux.x + xt.Ux.y;
-                    xs[8] -= xt.Uy.x + xt.Uy.y;
-                    xs[9] -= xt.Uz.x + xt.Uz.y;
+                xs[2] += xt.SF.x + xt.SF.y;
+                xs[3] += xt.Wx.x + xt.Wx.y;
+                xs[4] += xt.Wy.x + xt.Wy.y;
+                xs[5] += xt.Wz.x + xt.Wz.y;
+                if constexpr (!simple) {
+                    xs[6] += xt.Ux.x + xt.Ux.y;
+                    xs[7] += xt.Uy.x + xt.Uy.y;
+                    xs[8] += xt.Uz.x + xt.Uz.y;
                     xsc += xt.SC.x + xt.SC.y;
                 }
                 B = Bn;
@@ -783,23 +774,23 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             }
             atmb_cp_wait<0>();
             if (xvalid) {
+                // the x entry's force over this row: SF v_x - W
+                const double SF = xs[2];
                 atomicAdd(&acc[0 * mcap + xe], (float)xs[0]);
                 atomicAdd(&acc[1 * mcap + xe], (float)xs[1]);
-                atomicAdd(&acc[2 * mcap + xe], (float)xs[2]);
-                atomicAdd(&acc[3 * mcap + xe], (float)xs[3]);
-                atomicAdd(&acc[4 * mcap + xe], (float)xs[4]);
-                atomicAdd(&acc[5 * mcap + xe], (float)xs[5]);
-                if (!simple && xsc != 0.f) atomicAdd(&acc[6 * mcap + xe], xsc);
-                // apex force of the a-x sides and the x-y cross terms of the virial
-                apx[0] -= xs[6] * vx;
-                apx[1] -= xs[6] * vy;
-                apx[2] -= xs[6] * vz;
-                apx[3] -= 2.0 * vx * xs[7];
-                apx[4] -= 2.0 * vy * xs[8];
-                apx[5] -= 2.0 * vz * xs[9];
-                apx[6] -= vx * xs[8] + vy * xs[7];
-                apx[7] -= vx * xs[9] + vz * xs[7];
-                apx[8] -= vy * xs[9] + vz * xs[8];
+                atomicAdd(&acc[2 * mcap + xe], (float)(SF * vx - xs[3]));
+                atomicAdd(&acc[3 * mcap + xe], (float)(SF * vy - xs[4]));
+                atomicAdd(&acc[4 * mcap + xe], (float)(SF * vz - xs[5]));
+                if constexpr (!simple) {
+                    if (xsc != 0.f) atomicAdd(&acc[5 * mcap + xe], xsc);
+                    // the x-y cross terms of the apex virial that the force weights miss
+                    apx[3] -= 2.0 * vx * xs[6];
+                    apx[4] -= 2.0 * vy * xs[7];
+                    apx[5] -= 2.0 * vz * xs[8];
+                    apx[6] -= vx * xs[7] + vy * xs[6];
+                    apx[7] -= vx * xs[8] + vz * xs[6];
+                    apx[8] -= vy * xs[8] + vz * xs[7];
+                }
             }
             __syncwarp();
         }
@@ -808,29 +799,33 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         double ea = 0, ga = 0;
         for (int e = tid; e < m; e += blockDim.x) {
             // accumulated at L2 by atomics: read past L1
-            const double SE = __ldcg(&acc[e]), SD = __ldcg(&acc[mcap + e]), SF = __ldcg(&acc[2 * mcap + e]);
-            const double Wx = __ldcg(&acc[3 * mcap + e]), Wy = __ldcg(&acc[4 * mcap + e]);
-            const double Wz = __ldcg(&acc[5 * mcap + e]);
+            const double SE = __ldcg(&acc[e]), SD = __ldcg(&acc[mcap + e]);
+            const double Fx = __ldcg(&acc[2 * mcap + e]), Fy = __ldcg(&acc[3 * mcap + e]);
+            const double Fz = __ldcg(&acc[4 * mcap + e]);
             const float4 qa4 = sA[e], qj4 = sJ[e];
             const int j = __float_as_int(qj4.x);
             const double lam_ea = qj4.z, lam_ae = qj4.w;
             const double vx = qa4.x, vy = qa4.y, vz = qa4.z;
             atomicAdd(&p.eb[j], SE * (1.0 / 3.0));
             atomicAdd(&p.gb[j], 0.5 * (lam_ea * SE + SD));
-            atomicAdd(&p.fb[3 * j], SF * vx - Wx);
-            atomicAdd(&p.fb[3 * j + 1], SF * vy - Wy);
-            atomicAdd(&p.fb[3 * j + 2], SF * vz - Wz);
+            atomicAdd(&p.fb[3 * j], Fx);
+            atomicAdd(&p.fb[3 * j + 1], Fy);
+            atomicAdd(&p.fb[3 * j + 2], Fz);
             ea += SE * (1.0 / 6.0);
             ga += 0.5 * lam_ae * SE;
-            // virial: the force scalar, plus in the weighted form the coefficient of the
-            // visits whose energy and force weights differ
-            const double SV = SIMPLE ? SF : SF + (double)__ldcg(&acc[6 * mcap + e]);
-            apx[3] += SV * vx * vx;
-            apx[4] += SV * vy * vy;
-            apx[5] += SV * vz * vz;
-            apx[6] += SV * vx * vy;
-            apx[7] += SV * vx * vz;
-            apx[8] += SV * vy * vz;
+            // the apex takes minus the entries' forces (each triplet term depends on relative
+            // positions only); the virial is sum v_e (x) F_e (symmetrised), plus in the
+            // weighted form SC v_e (x) v_e for the visits whose energy and force weights differ
+            apx[0] -= Fx;
+            apx[1] -= Fy;
+            apx[2] -= Fz;
+            const double SC = SIMPLE ? 0.0 : (double)__ldcg(&acc[5 * mcap + e]);
+            apx[3] += vx * fma(SC, vx, Fx);
+            apx[4] += vy * fma(SC, vy, Fy);
+            apx[5] += vz * fma(SC, vz, Fz);
+            apx[6] += 0.5 * (vx * Fy + vy * Fx) + SC * vx * vy;
+            apx[7] += 0.5 * (vx * Fz + vz * Fx) + SC * vx * vz;
+            apx[8] += 0.5 * (vy * Fz + vz * Fy) + SC * vy * vz;
         }
         const double vals[11] = {ea, ga, apx[0], apx[1], apx[2], apx[3], apx[4], apx[5], apx[6], apx[7], apx[8]};
 #pragma unroll

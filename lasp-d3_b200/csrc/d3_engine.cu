@@ -129,9 +129,10 @@ struct KP {
     int atm_min_m;  // k_atm32 takes only apexes with longer lists (the rest: k_atm32b)
     int atmb_mcap;  // longest list k_atm32b takes
     int atmb_split; // CTAs of k_atm32b sharing one apex (each a share of its block rows)
-    // sharded evaluation: this process computes the two-body and chain-rule terms of central
-    // atoms i = shard_rank + k shard_world (binned order) and the ATM apexes of work items
-    // shard_rank + k shard_world; CN and weights for every atom
+    // sharded evaluation: this process computes the two-body and chain-rule terms of the
+    // atom groups it owns (group_owner; without groups: central atoms i = shard_rank +
+    // k shard_world, binned order) and the ATM apexes of work items shard_rank +
+    // k shard_world; CN and weights for every atom
     int shard_rank, shard_world;
     // work counters: [0] ATM in-range visits (2 per triplet), [1] two-body in-range
     // ordered pairs, [2] CN in-range ordered pairs
@@ -646,6 +647,31 @@ __global__ void k_atm_list(KP p) {
 }
 
 __device__ __forceinline__ int sext8(int v) { return (v << 24) >> 24; }
+
+// Special-function-unit approximations in their subnormal-flushing PTX forms (.ftz): no
+// subnormal handling is wrapped around the operation. Relative error about 2^-22 (the
+// PTX ISA's bounds for the .approx forms). The FP32 triplet and pair terms stay far from
+// the subnormal range (their smallest intermediates are about 1e-25).
+__device__ __forceinline__ float sfu_rsqrt(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sfu_rcp(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sfu_log2(float x) {
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sfu_exp2(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 // ------------------------------------------------------------------------------------
 // precision form: CN, two-body and chain rule with FP32 pair arithmetic. Sums are kept
@@ -2004,7 +2030,7 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
             D3_CUDA(cudaMemsetAsync(p.f2, 0, sizeof(double) * 3 * n, s));
             D3_CUDA(cudaMemsetAsync(p.v2, 0, sizeof(double) * 6 * n, s));
         }
-        if (p.gslices > 0 && p.shard_world <= 1) {
+        if (p.gslices > 0) {
             const int grid = e->dev_sms * pairs_occupancy(e);
             if (p.precision)
                 k_twobody_g<NR, false><<<grid, PAIRS_WARPS * 32, pairs_smem(e), s>>>(p, e->gctl.p + 2);
@@ -2130,7 +2156,7 @@ static void launch_all(Engine *e, const KP &p0, cudaStream_t s, int stage = 0, d
         D3_CUDA(cudaMemsetAsync(p.fc, 0, sizeof(double) * 3 * n, s));
         D3_CUDA(cudaMemsetAsync(p.vc, 0, sizeof(double) * 6 * n, s));
     }
-    if (p.gslices > 0 && p.shard_world <= 1) {
+    if (p.gslices > 0) {
         const size_t sm = 64 + PAIRS_WARPS * 32 * ((p.precision ? sizeof(float4) : sizeof(double4)) + sizeof(double));
         if (p.precision)
             k_chain_g<false><<<e->dev_sms * 2, PAIRS_WARPS * 32, sm, s>>>(p, Gsum, e->gctl.p + 3);

@@ -171,7 +171,18 @@ struct GroupItem {
     int4 sr;         // the group's super-row
     int bx_lo, bx_hi;
     const SG *g;
+    bool own;        // sharded evaluation: this rank owns the group's two-body and
+                     // chain-rule sums (every rank still covers every group in CN and lists)
 };
+
+// Owner rank of a group in a sharded evaluation: a hash of the group's super-row, first
+// column and skip count (fields that k_groups writes the same way on every rank, unlike
+// the group's slot), so that the ranks partition the groups without talking.
+__device__ __forceinline__ int group_owner(int4 grp, int world) {
+    const unsigned h = (unsigned)grp.x * 0x9E3779B1u ^ (unsigned)(grp.y & 0xffff) * 0x85EBCA77u ^
+                       (unsigned)grp.z * 0xC2B2AE3Du;
+    return (int)((h ^ (h >> 15)) % (unsigned)world);
+}
 
 __device__ __forceinline__ bool next_item(const KP &p, int *work, GroupItem &it) {
     const int lane = threadIdx.x & 31;
@@ -188,6 +199,7 @@ __device__ __forceinline__ bool next_item(const KP &p, int *work, GroupItem &it)
     it.bx_lo = grp.y & 0xffff;
     it.bx_hi = grp.y >> 16;
     it.i = lane < grp.w ? group_atom(p, *it.g, it.sr, it.bx_lo, grp.z, lane) : -1;
+    it.own = p.shard_world <= 1 || group_owner(grp, p.shard_world) == p.shard_rank;
     return true;
 }
 
@@ -291,6 +303,7 @@ __global__ void __launch_bounds__(PAIRS_WARPS * 32, F64 ? 1 : 2) k_twobody_g(KP 
         const SG &g = *it.g;
         const bool box_pair = g.box_mode && p.anyshift[it.sr.x];
         double E = 0, Gd = 0, FX = 0, FY = 0, FZ = 0, V[6] = {0, 0, 0, 0, 0, 0};
+        if (it.own)
         group_ranges<R, R4>(p, it, p.stencils + g.st2b_off, g.st2b_n, box_pair, xi,
                             [&](int base, int m, R ox, R oy, R oz, int px, int Ty, int Tz) {
             __syncwarp();
@@ -455,6 +468,7 @@ __global__ void __launch_bounds__(PAIRS_WARPS * 32, 2) k_chain_g(KP p, const dou
         const SG &g = *it.g;
         const bool box_pair = g.box_mode && p.anyshift[it.sr.x];
         double F[3] = {0, 0, 0}, V[6] = {0, 0, 0, 0, 0, 0};
+        if (it.own)
         group_ranges<R, R4>(p, it, p.stencils + g.stcb_off, g.stcb_n, box_pair, xi,
                             [&](int base, int m, R ox, R oy, R oz, int px, int Ty, int Tz) {
             __syncwarp();
