@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
                         ++visits;
                         const float4 pb = pB[k];
                         const int2 pc = pC[k];
-                        const float ir3 = rsqrtf(d3);
+                        const float ir3 = sfu_rsqrt(d3);
                         const float id3 = ir3 * ir3;
                         const float4 *yr = ytile + ((size_t)k * ne + tq) * 2;
                         const float4 y0 = yr[0], y1 = yr[1];
@@ -225,11 +225,11 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
                             c6 = fmaf(y1.z, wq[6], c6);
                             dc6 = fmaf(y1.z, dwq[6], dc6);
                         }
-                        const float is3 = rsqrtf(c6);
+                        const float is3 = sfu_rsqrt(c6);
                         const float s3 = c6 * is3;
                         const float lam_xy = dc6 * is3 * is3;
                         const float u = r0sq[tq * ne + pc.y] * id3;
-                        const float g3 = u * u * u * exp2f(__log2f(u) * (-1.0f / 3.0f));
+                        const float g3 = u * u * u * sfu_exp2(sfu_log2(u) * (-1.0f / 3.0f));
                         // reference scale factors (src/d3_kernel.cu:1282-1290) as pair weights
                         const bool same = (jq == pc.x);
                         const bool apex_img = qa | (pc.x == a);
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(ATM_THREADS) k_atm32(KP p, int tile) {
                         const float dang1 = q52 * fmaf(-0.75f * d1, t23 + t13 - t12, base);
                         const float dang3 = q52 * fmaf(-0.75f * d3, t13 + t12 - t23, base);
                         const float x16 = x16c * gq * pb.w * g3;
-                        const float fd = __fdividef(1.0f, fmaf(6.0f, x16, 1.0f));
+                        const float fd = sfu_rcp(fmaf(6.0f, x16, 1.0f));
                         const float dfd = 32.0f * x16 * fd * fd;
                         const float C9 = -sq * pb.z * s3;
                         const float Et = C9 * A * fd;

@@ -681,9 +681,10 @@ __device__ __forceinline__ float sfu_exp2(float x) {
 // FP32 CN term: value and (d CN / d r) / r, with the optional tanh^3 smooth cutoff (the
 // reference's SMOOTH_CUTOFF_CN) as in the FP64 term
 __device__ __forceinline__ float cn_term32(const KP &p, float r2, float rsum, float *dcn_over_r) {
-    const float ir = rsqrtf(r2);
-    const float e = __expf(-16.0f * fmaf(rsum, ir, -1.0f));
-    const float inv = __fdividef(1.0f, 1.0f + e);
+    const float ir = sfu_rsqrt(r2);
+    // exp(-16 (rsum / r - 1)) as a power of two
+    const float e = sfu_exp2(-16.0f * 1.44269504f * fmaf(rsum, ir, -1.0f));
+    const float inv = sfu_rcp(1.0f + e);
     float d = -16.0f * e * rsum * ir * ir * ir * inv * inv;
     float v = inv;
     if (p.smooth_cn) {
@@ -786,19 +787,19 @@ __global__ void k_twobody32(KP p) {
             float E6, E8, Gt, fs;
             if (p.damping == 1) {
                 const float r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
-                const float i6 = __fdividef(1.0f, r6 + tp.x), i8 = __fdividef(1.0f, r8 + tp.y);
+                const float i6 = sfu_rcp(r6 + tp.x), i8 = sfu_rcp(r8 + tp.y);
                 E6 = s6 * c6 * i6;
                 E8 = s8 * c8 * i8;
                 Gt = s6 * dc6 * i6 + s8 * dc8 * i8;
                 fs = -6.0f * E6 * r4 * i6 - 8.0f * E8 * r6 * i8;
             } else {
-                const float ir = rsqrtf(r2), ir2 = ir * ir;
+                const float ir = sfu_rsqrt(r2), ir2 = ir * ir;
                 const float ir6 = ir2 * ir2 * ir2, ir8 = ir6 * ir2;
                 const float R0 = tp.x;
                 const float x6 = p1 * R0 * ir, x8 = p2 * R0 * ir;
                 const float x6_2 = x6 * x6, x6_4 = x6_2 * x6_2, x6_8 = x6_4 * x6_4, x6_14 = x6_8 * x6_4 * x6_2;
                 const float x8_2 = x8 * x8, x8_4 = x8_2 * x8_2, x8_8 = x8_4 * x8_4, x8_16 = x8_8 * x8_8;
-                const float f6 = __fdividef(1.0f, fmaf(6.0f, x6_14, 1.0f)), f8 = __fdividef(1.0f, fmaf(6.0f, x8_16, 1.0f));
+                const float f6 = sfu_rcp(fmaf(6.0f, x6_14, 1.0f)), f8 = sfu_rcp(fmaf(6.0f, x8_16, 1.0f));
                 const float df6 = 84.0f * f6 * f6 * x6_14 * ir, df8 = 96.0f * f8 * f8 * x8_16 * ir;
                 E6 = s6 * c6 * f6 * ir6;
                 E8 = s8 * c8 * f8 * ir8;

@@ -118,8 +118,8 @@ __device__ __forceinline__ void pair_term(const KP &p, R r2, const R *y, const R
         const R r4 = r2 * r2, r6 = r4 * r2, r8 = r4 * r4;
         R i6, i8;
         if constexpr (sizeof(R) == 4) {
-            i6 = __fdividef(1.0f, r6 + A6_or_R0);
-            i8 = __fdividef(1.0f, r8 + A8);
+            i6 = sfu_rcp(r6 + A6_or_R0);
+            i8 = sfu_rcp(r8 + A8);
         } else {
             i6 = 1.0 / (r6 + A6_or_R0);
             i8 = 1.0 / (r8 + A8);
@@ -131,7 +131,7 @@ __device__ __forceinline__ void pair_term(const KP &p, R r2, const R *y, const R
     } else {
         R ir;
         if constexpr (sizeof(R) == 4)
-            ir = rsqrtf(r2);
+            ir = sfu_rsqrt(r2);
         else
             ir = 1.0 / sqrt(r2);
         const R ir2 = ir * ir, ir6 = ir2 * ir2 * ir2, ir8 = ir6 * ir2;
@@ -141,8 +141,8 @@ __device__ __forceinline__ void pair_term(const KP &p, R r2, const R *y, const R
         const R x8_2 = x8 * x8, x8_4 = x8_2 * x8_2, x8_8 = x8_4 * x8_4, x8_16 = x8_8 * x8_8;
         R f6, f8;
         if constexpr (sizeof(R) == 4) {
-            f6 = __fdividef(1.0f, fmaf(6.0f, x6_14, 1.0f));
-            f8 = __fdividef(1.0f, fmaf(6.0f, x8_16, 1.0f));
+            f6 = sfu_rcp(fmaf(6.0f, x6_14, 1.0f));
+            f8 = sfu_rcp(fmaf(6.0f, x8_16, 1.0f));
         } else {
             f6 = 1.0 / (1.0 + 6.0 * x6_14);
             f8 = 1.0 / (1.0 + 6.0 * x8_16);
