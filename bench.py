@@ -336,7 +336,8 @@ def engine_arm(args, world, rank, local):
         algorithmic = "%d in-range triplets x %d FLOP per launch" % (triplets, ATM_FLOP_PER_TRIPLET)
     else:
         achieved = pairs * TWOBODY_FLOP_PER_PAIR / (ch["twobody_ms"] * 1e-3) / 1e12
-        kernel = "k_twobody (FP64)" if fp64 else "k_twobody32 (FP32 pair arithmetic)"
+        kernel = ("k_twobody_g (two-body pairs on atom groups, FP64)" if fp64 else
+                  "k_twobody_g (two-body pairs on atom groups, FP32 pair arithmetic)")
         algorithmic = "%d in-range ordered pairs x %d FLOP per launch" % (pairs, TWOBODY_FLOP_PER_PAIR)
     roofline = {"bound": "fp64" if fp64 else "fp32", "kernel": kernel,
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
@@ -509,7 +510,8 @@ def batch_mode(args):
            "data": "synthetic",
            "config": {"workload": "%d periodic structures, atom counts log-uniform in [8, 2000] (%d atoms in total), "
                                   "cubic cells at 0.1 atoms/A^3 sheared by +-10 %% tilts, Dirichlet(1) compositions over "
-                                  "H/C/N/O/Si/Cu; PBE-D3(BJ)+ATM, rc 95 / 40 / 40 bohr" % (len(sts), ntot)},
+                                  "H/C/N/O/Si/Cu; PBE-D3(BJ)+ATM, rc 95 / 40 / 40 bohr" % (len(sts), ntot),
+                      "l2": "not flushed: the ATM half lists of the batch (several GB) are far larger than L2"},
            "forms": {}}
     stream = torch.cuda.Stream()
     # the autotuner times candidates on a subset of the structures (same generator, so the
@@ -541,7 +543,30 @@ def batch_mode(args):
             e_ev.synchronize()
             ms.append(s_ev.elapsed_time(e_ev))
         pt, cnt = b.pass_times()
+        # the same evaluation captured once in a CUDA graph and replayed: one graph launch
+        # per evaluation of every structure (list capacity sized by the calls above)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            b.compute_async(stream.cuda_stream)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            graph.replay()
+        torch.cuda.synchronize()
+        gms = []
+        for _ in range(args.steps):
+            s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_ev.record(stream)
+            with torch.cuda.stream(stream):
+                graph.replay()
+            e_ev.record(stream)
+            e_ev.synchronize()
+            gms.append(s_ev.elapsed_time(e_ev))
+        del graph
         out["forms"][form] = {"value": ntot / (statistics.mean(ms) * 1e-3), "ms_per_step": statistics.mean(ms),
+                              "graph": {"value": ntot / (statistics.mean(gms) * 1e-3),
+                                        "ms_per_step": statistics.mean(gms),
+                                        "kernels_per_eval": b.launches_per_eval()},
+                              "atm_list_capacity_entries": b.atm_list_capacity(),
                               "passes_ms": pt, "autotuned": {k: v for k, v in tuned.items() if k != "trials"},
                               "tuned_on_structures": len(sub),
                               "energy_sum_ev": float(np.sum(e))}

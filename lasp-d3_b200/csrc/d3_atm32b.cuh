@@ -706,48 +706,61 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                 AtmbXSums2<simple> xt{};    // x side of this block pair (two partial sums)
                 AtmbYSums2<simple> ys[2]{}; // y sides of steps s + 2p (x) and s + 2p + 1 (y), travelling with their y
                 const bool diag = (A == B);
-                const int s0 = diag ? 1 : 0, s1 = diag ? 17 : 32;
+                const int s1 = diag ? 17 : 32;
                 const float4 *yrow_x = yrow + tx * RQ * 32; // rows at the x entry's type
                 const float2 M1 = make_float2(-1.0f, -1.0f);
                 int nv = 0;
-                for (int s = s0; s < s1; s += 4) {
-                    // four independent visits per iteration (steps s .. s + 3) as two packed pairs
-                    int kp[2];
-                    float4 P0q[2], P1q[2];
-                    float2 d3p[2];
-                    bool a0q[2], a1q[2];
-                    bool any = false;
+                // off-diagonal block pairs take steps 0..31 with one range limit per lane
+                // (rc_ATM^2, or -1 for a lane without entry); diagonal ones steps 1..16, where
+                // step 16 is taken by lanes 0..15 only (lanes 16..31 would repeat its pairs)
+                auto walk = [&](auto diag_c) {
+                    constexpr bool DG = decltype(diag_c)::value;
+                    const float lim = xvalid ? ratm2f : -1.0f;
+                    const float lim16 = DG && lane >= 16 ? -1.0f : lim;
+                    for (int s = DG ? 1 : 0; s < (DG ? 17 : 32); s += 4) {
+                        // four independent visits per iteration (steps s .. s + 3) as two packed pairs
+                        int kp[2];
+                        float4 P0q[2], P1q[2];
+                        float2 d3p[2];
+                        bool a0q[2], a1q[2];
+                        bool any = false;
 #pragma unroll
-                    for (int pq = 0; pq < 2; ++pq) {
-                        kp[pq] = (lane + s + 2 * pq) & 31;
-                        P0q[pq] = yP0[kp[pq]];
-                        P1q[pq] = yP1[kp[pq]];
-                        const float2 rx = __ffma2_rn(make_float2(P0q[pq].x, P0q[pq].y), M1, X.vx);
-                        const float2 ry = __ffma2_rn(make_float2(P0q[pq].z, P0q[pq].w), M1, X.vy);
-                        const float2 rz = __ffma2_rn(make_float2(P1q[pq].x, P1q[pq].y), M1, X.vz);
-                        d3p[pq] = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
-                        const int st = s + 2 * pq;
-                        a0q[pq] = xvalid && (!diag || st < 16 || lane < 16) && d3p[pq].x <= ratm2f && d3p[pq].x >= 1e-12f;
-                        a1q[pq] = xvalid && (!diag || st + 1 < 16 || lane < 16) && d3p[pq].y <= ratm2f && d3p[pq].y >= 1e-12f;
-                        any |= a0q[pq] | a1q[pq];
-                        nv += (a0q[pq] ? 2 : 0) + (a1q[pq] ? 2 : 0);
-                    }
-                    if constexpr (FINE) {
+                        for (int pq = 0; pq < 2; ++pq) {
+                            kp[pq] = (lane + s + 2 * pq) & 31;
+                            P0q[pq] = yP0[kp[pq]];
+                            P1q[pq] = yP1[kp[pq]];
+                            const float2 rx = __ffma2_rn(make_float2(P0q[pq].x, P0q[pq].y), M1, X.vx);
+                            const float2 ry = __ffma2_rn(make_float2(P0q[pq].z, P0q[pq].w), M1, X.vy);
+                            const float2 rz = __ffma2_rn(make_float2(P1q[pq].x, P1q[pq].y), M1, X.vz);
+                            d3p[pq] = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+                            const int st = s + 2 * pq;
+                            const float l0 = DG && st >= 16 ? lim16 : lim, l1 = DG && st + 1 >= 16 ? lim16 : lim;
+                            a0q[pq] = d3p[pq].x <= l0 && d3p[pq].x >= 1e-12f;
+                            a1q[pq] = d3p[pq].y <= l1 && d3p[pq].y >= 1e-12f;
+                            any |= a0q[pq] | a1q[pq];
+                            nv += (a0q[pq] ? 2 : 0) + (a1q[pq] ? 2 : 0);
+                        }
+                        if constexpr (FINE) {
 #pragma unroll
-                        for (int pq = 0; pq < 2; ++pq)
-                            if (__any_sync(0xffffffffu, a0q[pq] | a1q[pq]))
+                            for (int pq = 0; pq < 2; ++pq)
+                                if (__any_sync(0xffffffffu, a0q[pq] | a1q[pq]))
+                                    atmb_visit2<NR, simple>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0,
+                                                            yQ1, yrow_x, a, third, force_scaled, xt, ys[pq]);
+                        } else if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+                            for (int pq = 0; pq < 2; ++pq)
                                 atmb_visit2<NR, simple>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0,
                                                         yQ1, yrow_x, a, third, force_scaled, xt, ys[pq]);
-                    } else if (__any_sync(0xffffffffu, any)) {
-#pragma unroll
-                        for (int pq = 0; pq < 2; ++pq)
-                            atmb_visit2<NR, simple>(X, kp[pq], d3p[pq], a0q[pq], a1q[pq], P0q[pq], P1q[pq], yQ0, yQ1,
-                                                    yrow_x, a, third, force_scaled, xt, ys[pq]);
+                        }
+                        const int src = (lane + 4) & 31;
+                        ys[0].shift(src);
+                        ys[1].shift(src);
                     }
-                    const int src = (lane + 4) & 31;
-                    ys[0].shift(src);
-                    ys[1].shift(src);
-                }
+                };
+                if (diag)
+                    walk(std::true_type{});
+                else
+                    walk(std::false_type{});
                 visits += (unsigned long long)nv;
                 // lane L now holds the complete sums of y entry B[(L + s1 + q) mod 32] from the
                 // visits of steps = q (mod 4) (q = 0, 1 in ys[0].x, .y; 2, 3 in ys[1].x, .y):

@@ -397,6 +397,12 @@ class D3Batch(_Surrogate, _Shard):
     def compute_async(self, stream_ptr=None):
         return int(self.lib.d3_compute_async(self.h, ctypes.c_void_p(stream_ptr) if stream_ptr else None))
 
+    def launches_per_eval(self):
+        return int(self.lib.d3_launches_per_eval(self.h))
+
+    def atm_list_capacity(self):
+        return int(self.lib.d3_atm_list_capacity(self.h))
+
     def pass_times(self):
         ms = np.zeros(8, np.float32)
         cnt = np.zeros(4, np.uint64)
