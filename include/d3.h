@@ -138,8 +138,8 @@ enum {
                                     every S-th block row (0 = automatic: more than one only
                                     when the apexes are fewer than about 4 per CTA, e.g. the
                                     96-atom water box; 1..64) */
-    D3_OPT_ATMB_FINE_SKIP = 14   /* block-pair kernel: 1 skips out-of-range visits per two
-                                    steps, 0 (default) per four steps (more overlap of the
+    D3_OPT_ATMB_FINE_SKIP = 14   /* block-pair kernel: 1 (default) skips out-of-range visits
+                                    per two steps, 0 per four steps (more overlap of the
                                     packed pairs) */
 };
 int d3_set_option(d3_handle_t *handle, int option, int value);

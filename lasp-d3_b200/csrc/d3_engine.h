@@ -60,7 +60,7 @@ struct Options {
     int atmb_mcap = 0;             // block-pair ATM: longest list it takes (0: automatic)
     int atmb_split = 0;            // block-pair ATM: CTAs sharing one apex (0: automatic,
                                    // more than one only when apexes are fewer than CTAs)
-    int atmb_fine_skip = 0;        // block-pair ATM: skip out-of-range visits per packed pair
+    int atmb_fine_skip = 1;        // block-pair ATM: skip out-of-range visits per packed pair
                                    // of steps (1) or per four steps (0)
 };
 

@@ -105,7 +105,7 @@ def tune(handle, key, repeats=2, use_cache=True, atm=True, precision=None):
     if precision is None:
         precision = key.endswith("|p1")
     params = {"bin_divisor": 6, "pair_kernel": 0, "atm_tile": 0, "atm_ctas_per_sm": 0, "atmb_warps": 0,
-              "atmb_mcap": 0, "atmb_fine_skip": 0}
+              "atmb_mcap": 0, "atmb_fine_skip": 1}
     apply(handle, params)
     pair_passes = ("bin", "cn", "twobody", "atm_list", "chain")
     best = None
