@@ -69,10 +69,11 @@ __host__ __device__ inline size_t atmb_smem_fixed(int ne, int NR, int mcap) {
 // type as float4 [type][row quad][lane] (lanes read consecutive 16-byte words whatever the
 // x type, so the reads are free of bank conflicts) and positions / per-entry constants
 __host__ __device__ inline size_t atmb_buf_quads(int ne, int NR) { return 32 * ((size_t)ne * (atmb_row_floats(NR) / 4) + 2); }
-// plus the lanes' FP64 carries (apex force and virial, row sums of the x entry), [19][lane]
+// plus the lanes' FP64 carries (the weighted form's cross terms of the apex virial, row sums
+// of the x entry), [15][lane]
 // and the current block's positions / per-entry constants with entries k, k + 1 side by
 // side ([4][32] float4)
-constexpr int ATMB_NCARRY = 19;
+constexpr int ATMB_NCARRY = 15;
 __host__ __device__ inline size_t atmb_smem_warp(int ne, int NR, int nbuf = 2) {
     return nbuf * atmb_buf_quads(ne, NR) * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double) + 4 * 32 * sizeof(float4);
 }
@@ -566,14 +567,16 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
         __syncthreads();
         // ---- 2./3. block pairs
         // apex force (3) and virial (6) of this lane, and the row sums of its x entry
+        // carries: virial cross terms of the weighted form (xx yy zz xy xz yz), and the row
+        // sums of this lane's x entry
         const AtmbCarry apx{reinterpret_cast<double *>(wbase + NBUF * bufq * sizeof(float4)) + lane};
-        const AtmbCarry xs{apx.p + 9 * 32}; // SE SD SF Wx Wy Wz, weighted form also Ux Uy Uz
+        const AtmbCarry xs{apx.p + 6 * 32}; // SE SD SF Wx Wy Wz, weighted form also Ux Uy Uz
         // positions (x, x', y, y'), (z, z', d2, d2') and constants (ir, ir', id2, id2'),
         // (s, s', g, g') of the current y block, entries k and k + 1 at slot k
         float4 *yP0 = reinterpret_cast<float4 *>(wbase + NBUF * bufq * sizeof(float4) + ATMB_NCARRY * 32 * sizeof(double));
         float4 *yP1 = yP0 + 32, *yQ0 = yP1 + 32, *yQ1 = yQ0 + 32;
 #pragma unroll
-        for (int q = 0; q < 9; ++q) apx[q] = 0.0;
+        for (int q = 0; q < 6; ++q) apx[q] = 0.0;
         // rows are handed out in order (row A holds nb - A block pairs, so the dearest go
         // first and the cheapest close the apex, shortening the wait at its barrier)
         for (;;) {
@@ -797,19 +800,21 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
                 if constexpr (!simple) {
                     if (xsc != 0.f) atomicAdd(&acc[5 * mcap + xe], xsc);
                     // the x-y cross terms of the apex virial that the force weights miss
-                    apx[3] -= 2.0 * vx * xs[6];
-                    apx[4] -= 2.0 * vy * xs[7];
-                    apx[5] -= 2.0 * vz * xs[8];
-                    apx[6] -= vx * xs[7] + vy * xs[6];
-                    apx[7] -= vx * xs[8] + vz * xs[6];
-                    apx[8] -= vy * xs[8] + vz * xs[7];
+                    apx[0] -= 2.0 * vx * xs[6];
+                    apx[1] -= 2.0 * vy * xs[7];
+                    apx[2] -= 2.0 * vz * xs[8];
+                    apx[3] -= vx * xs[7] + vy * xs[6];
+                    apx[4] -= vx * xs[8] + vz * xs[6];
+                    apx[5] -= vy * xs[8] + vz * xs[7];
                 }
             }
             __syncwarp();
         }
         __syncthreads();
         // ---- 4. per entry: atom shares (FP64 atomics) and the apex's sums
-        double ea = 0, ga = 0;
+        double ea = 0, ga = 0, af[3] = {0.0, 0.0, 0.0}, av[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) av[k] = apx[k];
         for (int e = tid; e < m; e += blockDim.x) {
             // accumulated at L2 by atomics: read past L1
             const double SE = __ldcg(&acc[e]), SD = __ldcg(&acc[mcap + e]);
@@ -829,18 +834,18 @@ __global__ void __launch_bounds__((NBUF == 2 ? ATMB_MAXW : ATMB_MAXW1) * 32, 1) 
             // the apex takes minus the entries' forces (each triplet term depends on relative
             // positions only); the virial is sum v_e (x) F_e (symmetrised), plus in the
             // weighted form SC v_e (x) v_e for the visits whose energy and force weights differ
-            apx[0] -= Fx;
-            apx[1] -= Fy;
-            apx[2] -= Fz;
+            af[0] -= Fx;
+            af[1] -= Fy;
+            af[2] -= Fz;
             const double SC = SIMPLE ? 0.0 : (double)__ldcg(&acc[5 * mcap + e]);
-            apx[3] += vx * fma(SC, vx, Fx);
-            apx[4] += vy * fma(SC, vy, Fy);
-            apx[5] += vz * fma(SC, vz, Fz);
-            apx[6] += 0.5 * (vx * Fy + vy * Fx) + SC * vx * vy;
-            apx[7] += 0.5 * (vx * Fz + vz * Fx) + SC * vx * vz;
-            apx[8] += 0.5 * (vy * Fz + vz * Fy) + SC * vy * vz;
+            av[0] += vx * fma(SC, vx, Fx);
+            av[1] += vy * fma(SC, vy, Fy);
+            av[2] += vz * fma(SC, vz, Fz);
+            av[3] += 0.5 * (vx * Fy + vy * Fx) + SC * vx * vy;
+            av[4] += 0.5 * (vx * Fz + vz * Fx) + SC * vx * vz;
+            av[5] += 0.5 * (vy * Fz + vz * Fy) + SC * vy * vz;
         }
-        const double vals[11] = {ea, ga, apx[0], apx[1], apx[2], apx[3], apx[4], apx[5], apx[6], apx[7], apx[8]};
+        const double vals[11] = {ea, ga, af[0], af[1], af[2], av[0], av[1], av[2], av[3], av[4], av[5]};
 #pragma unroll
         for (int k = 0; k < 11; ++k) {
             const double v = warp_sum(vals[k]);
