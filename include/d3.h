@@ -136,7 +136,7 @@ enum {
                                     longer lists go to the mirror-symmetric kernel */
     D3_OPT_ATMB_SPLIT = 13,      /* CTAs of the block-pair kernel sharing one apex, each taking
                                     every S-th block row (0 = automatic: more than one only
-                                    when the apexes are fewer than about 4 per CTA, e.g. the
+                                    when the apexes are fewer than about 3 per CTA, e.g. the
                                     96-atom water box; 1..64) */
     D3_OPT_ATMB_FINE_SKIP = 14   /* block-pair kernel: 1 (default) skips out-of-range visits
                                     per two steps, 0 per four steps (more overlap of the
